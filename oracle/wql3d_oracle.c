@@ -1,0 +1,1309 @@
+/*
+ * CPU oracle for the WaveQLab3D per-step volume update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file restates, in plain C, the reference
+ * Fortran solver's hot path so that the CUDA product can be checked against
+ * it.  It is imported only by tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py.  Nothing in the product
+ * links it.
+ *
+ * Parity is pinned by the reference's own published 16-digit known answer
+ * (inputfile/test_elastic_traditional_o6.in ->
+ * "Elastic final state: max|field|=1.6623128367649574E+02",
+ * PHASE5_TRADITIONAL_CARTESIAN_RHS.md:35) and by the rupture truth files
+ * test_problems/truth/{1,2} (see tests/golden/).
+ *
+ * Every routine names the reference file:line it follows.  Floating-point
+ * expressions keep the reference's evaluation order (Fortran evaluates
+ * left to right within one precedence level), and the file is compiled with
+ * -ffp-contract=off so no fused multiply-add changes the rounding.
+ */
+#include "wql3d_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NB 3
+#define PI_WP 3.141592653589793
+
+/* ------------------------------------------------------------------------ */
+/* 6th-order SBP first-derivative operator (traditional-6).                  */
+/* Boundary rows 1..6 in the order their terms are written in                */
+/* src/JU_xJU_yJU_z6.f90:74-161 (left closure) and src/metrics.f90:29-86.    */
+/* Right rows are the negated mirror, src/JU_xJU_yJU_z6.f90:170-290.          */
+/* The row-4 coefficient 0.013435342414630 carries no _wp kind suffix in the */
+/* reference, so without -fdefault-real-8 it is a single-precision literal.  */
+/* ------------------------------------------------------------------------ */
+typedef struct { int n; int idx[8]; double c[8]; } sbp_row;
+
+static sbp_row g_left[6];
+static int g_f32lit_cached = -1;
+
+static void sbp_init(int f32lit) {
+  if (g_f32lit_cached == f32lit) return;
+  const double c4_7 = f32lit ? (double)0.013435342414630f : 0.013435342414630;
+  sbp_row r1 = {6, {6, 5, 4, 3, 2, 1}, {0.036577936277544, 0.104488069284042, -0.450398306578272,
+                                        -0.141512858744873, 2.033378678700676, -1.582533518939116}};
+  sbp_row r2 = {5, {6, 5, 4, 3, 1}, {-0.014903449191300, -0.069112065532624, 0.258816087376832,
+                                     0.287258622978251, -0.462059195631158}};
+  sbp_row r3 = {5, {6, 5, 4, 2, 1}, {-0.018129342917256, -0.022902190275815, 0.606235523609147,
+                                     -0.636451095137907, 0.071247104721830}};
+  sbp_row r4 = {6, {7, 6, 5, 3, 2, 1}, {c4_7, -0.051642265516119, 0.520262285050482,
+                                        -0.306681191361148, -0.290087484386815, 0.114713313798970}};
+  sbp_row r5 = {7, {8, 7, 6, 4, 3, 2, 1}, {0.018281071473911, -0.164529643265203, 0.769199413962647,
+                                           -0.707905442575989, 0.015764336127392, 0.105400944933782,
+                                           -0.036210680656541}};
+  sbp_row r6 = {8, {9, 8, 7, 5, 4, 3, 2, 1}, {0.016437980868017, -0.147941827812150, 0.739709139060752,
+                                              -0.691649024426814, 0.063183694641876, 0.011220896474665,
+                                              0.020437334208704, -0.011398193015050}};
+  g_left[0] = r1; g_left[1] = r2; g_left[2] = r3; g_left[3] = r4; g_left[4] = r5; g_left[5] = r6;
+  g_f32lit_cached = f32lit;
+}
+
+/* The stencil row used at 1-based position i of an axis with n points:
+   absolute 1-based indices and signed coefficients, in summation order. */
+static void sbp_stencil(int i, int n, int *cnt, int *idx, double *c) {
+  static const double cc[6] = {-1.0 / 60.0, 0.15, -0.75, 0.75, -0.15, 1.0 / 60.0};
+  static const int off[6] = {-3, -2, -1, 1, 2, 3};
+  if (i >= 7 && i <= n - 6) {
+    *cnt = 6;
+    for (int k = 0; k < 6; ++k) { idx[k] = i + off[k]; c[k] = cc[k]; }
+    return;
+  }
+  if (i >= n - 5) { /* right closure (mirror of left row n+1-i) */
+    const sbp_row *r = &g_left[n - i];
+    *cnt = r->n;
+    for (int k = 0; k < r->n; ++k) { idx[k] = n + 1 - r->idx[k]; c[k] = -r->c[k]; }
+    return;
+  }
+  const sbp_row *r = &g_left[i - 1];
+  *cnt = r->n;
+  for (int k = 0; k < r->n; ++k) { idx[k] = r->idx[k]; c[k] = r->c[k]; }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Block storage                                                             */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int x0, x1, y0, y1, z0, z1; /* inclusive 1-based box */
+  int active;
+} box_t;
+
+typedef struct {
+  orc_desc d;
+  int nx, ny, nz, NX, NY, NZ;
+  long np;                  /* padded point count */
+  double hq, hr, hs;
+  double *X[3];
+  double *mx[3], *my[3], *mz[3], *J;
+  double *M[3];
+  double *F[9], *DF[9];
+  /* PML slabs, faces 1..6 */
+  box_t pbox[6];
+  double *Q[6][9], *DQ[6][9];
+  /* anelastic */
+  int nmech;
+  double *qs, *qp;
+  double *eta[6][8], *deta[6][8];
+  /* boundary faces: normals n_l, n_m, n_n (3 comps each), face-local 2-D */
+  double *nl[6][3], *nm[6][3], *nn[6][3];
+  int fdim[6][2];
+  double *work[6][9];       /* SAT forcing u_bc per face */
+  /* sources */
+  int nsrc;
+  int *stype;
+  double *spar;
+  int *snear;               /* 3 per source */
+  double *sphys;            /* 3 per source */
+  /* receivers */
+  int nrec;
+  int *ridx;
+  /* interface face buffers (for 2-block runs) */
+  double *faceF[2][9];      /* own face (q-min: 0, q-max: 1) copied fields */
+  double *faceFopp[2][9];
+  double *faceM[2][3];
+  double *faceMopp[2][3];
+} oblk;
+
+typedef struct {
+  orc_iface_desc d;
+  int nr, ns;
+  double *S[4], *DS[4], *W, *DW, *Svel[3], *trup;
+  double *t0n, *t0m, *t0l, *fsm;
+} oiface;
+
+typedef struct {
+  int nb;
+  oblk *B[2];
+  oiface *I;
+  double t;
+} odom;
+
+static inline long ID(const oblk *b, int x, int y, int z) {
+  return (long)(x - 1 + NB) + (long)b->NX * ((long)(y - 1 + NB) + (long)b->NY * (long)(z - 1 + NB));
+}
+static inline long FID(const oblk *b, int face, int a, int c) {
+  /* face-local index: faces 1,2 -> (y,z); 3,4 -> (x,z); 5,6 -> (x,y), 1-based */
+  (void)b;
+  return (long)(a - 1) + (long)b->fdim[face][0] * (long)(c - 1);
+}
+static inline long PID(const oblk *b, int f, int x, int y, int z) {
+  const box_t *q = &b->pbox[f];
+  return (long)(x - q->x0) + (long)(q->x1 - q->x0 + 1) * ((long)(y - q->y0) + (long)(q->y1 - q->y0 + 1) * (long)(z - q->z0));
+}
+
+static double *zalloc(long n, double v) {
+  double *p = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  for (long i = 0; i < n; ++i) p[i] = v;
+  return p;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Grid and metrics: src/grid.f90:214-241 (cartesian_grid_3d),               */
+/* src/grid.f90:398-471 (derivatives), src/metrics.f90:16-491 (D6x/y/z)      */
+/* ------------------------------------------------------------------------ */
+static void d6_line(const oblk *b, int axis, int x, int y, int z, double h, double out[3]) {
+  int n = axis == 0 ? b->nx : axis == 1 ? b->ny : b->nz;
+  int i = axis == 0 ? x : axis == 1 ? y : z;
+  int cnt, idx[8];
+  double c[8];
+  sbp_stencil(i, n, &cnt, idx, c);
+  for (int comp = 0; comp < 3; ++comp) {
+    double s = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+      int xx = axis == 0 ? idx[k] : x, yy = axis == 1 ? idx[k] : y, zz = axis == 2 ? idx[k] : z;
+      double term = c[k] * b->X[comp][ID(b, xx, yy, zz)];
+      s = (k == 0) ? term : s + term;
+    }
+    out[comp] = (1.0 / h) * s;   /* src/metrics.f90:166 */
+  }
+}
+
+static void build_grid(oblk *b) {
+  const orc_desc *d = &b->d;
+  for (int c = 0; c < 3; ++c) b->X[c] = zalloc(b->np, 0.0);
+  if (d->coords) {
+    long n1 = (long)b->nx * b->ny * b->nz;
+    for (int z = 1; z <= b->nz; ++z)
+      for (int y = 1; y <= b->ny; ++y)
+        for (int x = 1; x <= b->nx; ++x)
+          for (int c = 0; c < 3; ++c)
+            b->X[c][ID(b, x, y, z)] = d->coords[c * n1 + (x - 1) + (long)b->nx * ((y - 1) + (long)b->ny * (z - 1))];
+  } else {
+    double bh[3];
+    int nn[3] = {b->nx, b->ny, b->nz};
+    for (int c = 0; c < 3; ++c) bh[c] = (d->bqrs[c] - d->aqrs[c]) / (double)(nn[c] - 1);
+    for (int z = 1; z <= b->nz; ++z)
+      for (int y = 1; y <= b->ny; ++y)
+        for (int x = 1; x <= b->nx; ++x) {
+          long p = ID(b, x, y, z);
+          b->X[0][p] = d->aqrs[0] + (double)(x - 1) * bh[0];
+          b->X[1][p] = d->aqrs[1] + (double)(y - 1) * bh[1];
+          b->X[2][p] = d->aqrs[2] + (double)(z - 1) * bh[2];
+        }
+  }
+  b->hq = 1.0 / (double)(b->nx - 1);
+  b->hr = 1.0 / (double)(b->ny - 1);
+  b->hs = 1.0 / (double)(b->nz - 1);
+  for (int c = 0; c < 3; ++c) { b->mx[c] = zalloc(b->np, 0.0); b->my[c] = zalloc(b->np, 0.0); b->mz[c] = zalloc(b->np, 0.0); }
+  b->J = zalloc(b->np, 0.0);
+  for (int s = 1; s <= b->nz; ++s)
+    for (int r = 1; r <= b->ny; ++r)
+      for (int q = 1; q <= b->nx; ++q) {
+        double Xq[3], Xr[3], Xs[3];
+        d6_line(b, 0, q, r, s, b->hq, Xq);
+        d6_line(b, 1, q, r, s, b->hr, Xr);
+        d6_line(b, 2, q, r, s, b->hs, Xs);
+        long p = ID(b, q, r, s);
+        double J = Xq[0] * (Xr[1] * Xs[2] - Xr[2] * Xs[1]) - Xq[1] * (Xr[0] * Xs[2] - Xr[2] * Xs[0]) +
+                   Xq[2] * (Xr[0] * Xs[1] - Xr[1] * Xs[0]);
+        b->J[p] = J;
+        double iJ = 1.0 / J;
+        b->mx[0][p] = iJ * (Xr[1] * Xs[2] - Xr[2] * Xs[1]);
+        b->mx[1][p] = iJ * (Xq[2] * Xs[1] - Xq[1] * Xs[2]);
+        b->mx[2][p] = iJ * (Xq[1] * Xr[2] - Xq[2] * Xr[1]);
+        b->my[0][p] = iJ * (Xr[2] * Xs[0] - Xr[0] * Xs[2]);
+        b->my[1][p] = iJ * (Xq[0] * Xs[2] - Xq[2] * Xs[0]);
+        b->my[2][p] = iJ * (Xq[2] * Xr[0] - Xq[0] * Xr[2]);
+        b->mz[0][p] = iJ * (Xr[0] * Xs[1] - Xr[1] * Xs[0]);
+        b->mz[1][p] = iJ * (Xq[1] * Xs[0] - Xq[0] * Xs[1]);
+        b->mz[2][p] = iJ * (Xq[0] * Xr[1] - Xq[1] * Xr[0]);
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Face normals: src/unit_normals.f90:8-266                                  */
+/* ------------------------------------------------------------------------ */
+static void gram_schmidt(const double y[3], double z[3]) { /* src/unit_normals.f90:252-264 */
+  double a = y[0] * z[0] + y[1] * z[1] + y[2] * z[2];
+  for (int i = 0; i < 3; ++i) z[i] = z[i] - a * y[i];
+  double s = 1.0 / sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2]);
+  for (int i = 0; i < 3; ++i) z[i] = s * z[i];
+}
+
+static void gen_orth(double l[3], double m[3], const double n[3]) { /* src/unit_normals.f90:217-249 */
+  const double tol = 1.0e-12;
+  m[0] = 0.0; m[1] = 1.0; m[2] = 0.0;
+  double d1 = sqrt((n[0] - m[0]) * (n[0] - m[0]) + (n[1] - m[1]) * (n[1] - m[1]) + (n[2] - m[2]) * (n[2] - m[2]));
+  double d2 = sqrt((n[0] + m[0]) * (n[0] + m[0]) + (n[1] + m[1]) * (n[1] + m[1]) + (n[2] + m[2]) * (n[2] + m[2]));
+  if (!(d1 >= tol && d2 >= tol)) { m[0] = 0.0; m[1] = 0.0; m[2] = 1.0; }
+  gram_schmidt(n, m);
+  l[0] = n[1] * m[2] - n[2] * m[1];
+  l[1] = n[2] * m[0] - n[0] * m[2];
+  l[2] = n[0] * m[1] - n[1] * m[0];
+}
+
+static void build_normals(oblk *b) {
+  for (int f = 0; f < 6; ++f) {
+    int axis = f / 2;
+    int d0 = axis == 0 ? b->ny : b->nx;
+    int d1 = axis == 2 ? b->ny : b->nz;
+    b->fdim[f][0] = d0; b->fdim[f][1] = d1;
+    long n = (long)d0 * d1;
+    for (int c = 0; c < 3; ++c) { b->nl[f][c] = zalloc(n, 0.0); b->nm[f][c] = zalloc(n, 0.0); b->nn[f][c] = zalloc(n, 0.0); }
+    for (int c = 0; c < 9; ++c) b->work[f][c] = zalloc(n, 0.0);
+    int fixed = (f % 2 == 0) ? 1 : (axis == 0 ? b->nx : axis == 1 ? b->ny : b->nz);
+    for (int c2 = 1; c2 <= d1; ++c2)
+      for (int c1 = 1; c1 <= d0; ++c1) {
+        int x, y, z;
+        if (axis == 0) { x = fixed; y = c1; z = c2; }
+        else if (axis == 1) { x = c1; y = fixed; z = c2; }
+        else { x = c1; y = c2; z = fixed; }
+        long p = ID(b, x, y, z);
+        double qx = b->mx[axis][p], qy = b->my[axis][p], qz = b->mz[axis][p];
+        double norm = sqrt(qx * qx + qy * qy + qz * qz);
+        double n3[3] = {qx / norm, qy / norm, qz / norm}, l3[3], m3[3];
+        gen_orth(l3, m3, n3);
+        long fp = FID(b, f, c1, c2);
+        for (int c = 0; c < 3; ++c) { b->nn[f][c][fp] = n3[c]; b->nm[f][c][fp] = m3[c]; b->nl[f][c][fp] = l3[c]; }
+      }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Moment-tensor source: src/moment_tensor.f90:813-1125                      */
+/* ------------------------------------------------------------------------ */
+static double source_time(int type, double t, double t0, double w) {
+  switch (type) {
+    case ORC_STF_GAUSSIAN: return (w / (sqrt(2.0 * PI_WP))) * exp((-(w * w) * ((t - t0) * (t - t0))) / 2.0);
+    case ORC_STF_LOH_DISC: return (t / (w * w)) * exp(-t / w);
+    case ORC_STF_BRUNE: return (w * w) * t * exp(-w * t);
+    case ORC_STF_COSBELL: return (t < t0) ? (1.0 - cos(2.0 * PI_WP * t / t0)) / t0 : 0.0;
+    case ORC_STF_COSINE: return ((t >= 0.0) && (t <= w)) ? 1.0 - cos(2.0 * PI_WP * t / w) : 0.0;
+    case ORC_STF_LOH_MOMENT: return (1.0 - (1.0 + t / w) * exp(-t / w));
+    case ORC_STF_SINE_MOMENT: return (t <= w) ? t - w / (2.0 * PI_WP) * sin(2.0 * PI_WP * t / w) : w;
+    case ORC_STF_RICKER: {
+      /* Ricker wavelet, an addition (the reference has none): f0 = w, delay t0 */
+      double a = PI_WP * w * (t - t0);
+      double a2 = a * a;
+      return (1.0 - 2.0 * a2) * exp(-a2);
+    }
+  }
+  return 0.0;
+}
+
+static double singular_source(int i, int i0, double h, double a, int order, int alpha) {
+  if (order == 2) { /* src/moment_tensor.f90:950-974 */
+    double beta = (1.0 - 2.0 * a) / 4.0 + 0.25;
+    double gam = (2.0 * a - 1.0) / 16.0;
+    double gap = (2.0 * a + 1.0) / 16.0;
+    if (i == i0 - 2) return (-gam) / h;
+    if (i == i0 - 1) return (beta + 3.0 * gam - gap) / h;
+    if (i == i0) return (1.0 - a - 2.0 * beta - 3.0 * gam + 3.0 * gap) / h;
+    if (i == i0 + 1) return (a + beta + gam - 3.0 * gap) / h;
+    if (i == i0 + 2) return gap / h;
+    return 0.0;
+  }
+  if (order == 4) { /* src/moment_tensor.f90:976-1121 */
+    static const double w0[9] = {-0.01171875, -0.03125, 0.046875, 0.28125, 0.4296875, 0.28125, 0.046875, -0.03125, -0.01171875};
+    static const double w25[9] = {-0.00246875, -0.02275, -0.014125, 0.16575, 0.4171875, 0.38675, 0.117875, -0.02975, -0.01846875};
+    static const double w50[9] = {-0.00728125, -0.028, 0.014875, 0.224, 0.4265625, 0.336, 0.081375, -0.032, -0.01553125};
+    static const double w100[9] = {-0.0095625, -0.02990625, 0.03053125, 0.25284375, 0.42890625, 0.30903125, 0.06384375, -0.03196875, -0.01371875};
+    const double *w = alpha == 0 ? w0 : alpha == 25 ? w25 : alpha == 50 ? w50 : alpha == 100 ? w100 : NULL;
+    int k = i - i0;
+    if (!w || k < -4 || k > 4) return 0.0;
+    return w[k + 4] / h;
+  }
+  return 0.0;
+}
+
+/* Find_Coordinates_moment, src/seismogram.f90:878-960: nearest node, ties to the last visited */
+static void nearest_node_moment(const oblk *b, double x1, double y1, double z1, int out[3]) {
+  double mn[3] = {1e300, 1e300, 1e300}, mxv[3] = {-1e300, -1e300, -1e300};
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x)
+        for (int c = 0; c < 3; ++c) {
+          double v = b->X[c][ID(b, x, y, z)];
+          if (v < mn[c]) mn[c] = v;
+          if (v > mxv[c]) mxv[c] = v;
+        }
+  double scale = 1.0;
+  for (int c = 0; c < 3; ++c) { if (fabs(mn[c]) > scale) scale = fabs(mn[c]); if (fabs(mxv[c]) > scale) scale = fabs(mxv[c]); }
+  double tol = 1000.0 * 2.220446049250313e-16 * scale;
+  out[0] = out[1] = out[2] = -9999;
+  if (!((mn[0] - tol <= x1 && x1 <= mxv[0] + tol) && (mn[1] - tol <= y1 && y1 <= mxv[1] + tol) &&
+        (mn[2] - tol <= z1 && z1 <= mxv[2] + tol)))
+    return;
+  double mindist = 1.0e8;
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) {
+        long p = ID(b, x, y, z);
+        double v0 = b->X[0][p] - x1, v1 = b->X[1][p] - y1, v2 = b->X[2][p] - z1;
+        double dist = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        if (dist <= mindist) { out[0] = x; out[1] = y; out[2] = z; mindist = dist; }
+      }
+}
+
+/* Find_Coordinates, src/seismogram.f90:767-876 (receivers) */
+static void nearest_node_receiver(const oblk *b, double x1, double y1, double z1, int out[3]) {
+  out[0] = out[1] = out[2] = -9999;
+  double mindist = 1.0e8;
+  int px = b->nx, py = b->ny, pz = b->nz;
+  for (int k = 1; k <= pz; ++k)
+    for (int j = 1; j <= py; ++j)
+      for (int i = 1; i <= px; ++i) {
+        double hx = b->X[0][ID(b, px, j, k)] - b->X[0][ID(b, px - 1, j, k)];
+        double hy = b->X[1][ID(b, i, py, k)] - b->X[1][ID(b, i, py - 1, k)];
+        double hz = b->X[2][ID(b, i, j, pz)] - b->X[2][ID(b, i, j, pz - 1)];
+        if (i < px) hx = b->X[0][ID(b, i + 1, j, k)] - b->X[0][ID(b, i, j, k)];
+        if (j < py) hy = b->X[1][ID(b, i, j + 1, k)] - b->X[1][ID(b, i, j, k)];
+        if (k < pz) hz = b->X[2][ID(b, i, j, k + 1)] - b->X[2][ID(b, i, j, k)];
+        long p = ID(b, i, j, k);
+        double v0 = b->X[0][p] - x1, v1 = b->X[1][p] - y1, v2 = b->X[2][p] - z1;
+        double dist = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        double dist0 = sqrt(hx * hx + hy * hy + hz * hz);
+        if ((dist <= mindist) && (dist <= 0.5 * dist0)) { out[0] = i; out[1] = j; out[2] = k; mindist = dist; }
+      }
+}
+
+/* set_moment_tensor, src/moment_tensor.f90:875-936.  The reference visits
+   every local point; the delta weights vanish outside the 5- or 9-point
+   support, so only the support is visited here (exact: DF - A*M*0 = DF). */
+static void set_moment_tensor(oblk *b, double t) {
+  const orc_desc *d = &b->d;
+  int half = d->src_order == 4 ? 4 : 2;
+  for (int i = 0; i < b->nsrc; ++i) {
+    const double *sp = &b->spar[i * 11];
+    int nx0 = b->snear[3 * i], ny0 = b->snear[3 * i + 1], nz0 = b->snear[3 * i + 2];
+    if (nx0 < 1) continue;
+    double A = source_time(b->stype[i], t, sp[1], sp[0]);
+    for (int n = nz0 - half; n <= nz0 + half; ++n) {
+      if (n < 1 || n > b->nz) continue;
+      for (int m = ny0 - half; m <= ny0 + half; ++m) {
+        if (m < 1 || m > b->ny) continue;
+        for (int l = nx0 - half; l <= nx0 + half; ++l) {
+          if (l < 1 || l > b->nx) continue;
+          long p = ID(b, l, m, n);
+          double hx = b->hq / b->mx[0][p];
+          double hy = b->hr / b->my[1][p];
+          double hz = b->hs / b->mz[2][p];
+          double ax = (sp[8] - b->sphys[3 * i]) / hx;
+          double ay = (sp[9] - b->sphys[3 * i + 1]) / hy;
+          double az = (sp[10] - b->sphys[3 * i + 2]) / hz;
+          double dx = singular_source(l, nx0, hx, ax, d->src_order, d->src_alpha);
+          double dy = singular_source(m, ny0, hy, ay, d->src_order, d->src_alpha);
+          double dz = singular_source(n, nz0, hz, az, d->src_order, d->src_alpha);
+          double delta = dx * dy * dz;
+          b->DF[3][p] = b->DF[3][p] - A * sp[2] * delta;
+          b->DF[4][p] = b->DF[4][p] - A * sp[3] * delta;
+          b->DF[5][p] = b->DF[5][p] - A * sp[4] * delta;
+          b->DF[6][p] = b->DF[6][p] - A * sp[5] * delta;
+          b->DF[7][p] = b->DF[7][p] - A * sp[6] * delta;
+          b->DF[8][p] = b->DF[8][p] - A * sp[7] * delta;
+        }
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Near-boundary derivative JJU_x6, src/JU_xJU_yJU_z6.f90:12-809             */
+/* X = metric row (metricx, metricy or metricz); components X[0..2] are the  */
+/* q-, r-, s-entries of that row.                                            */
+/* ------------------------------------------------------------------------ */
+static void jju6(const oblk *b, int x, int y, int z, double *const X[3], double Ju[9]) {
+  double Jq[9], Jr[9], Js[9];
+  int cnt, idx[8];
+  double c[8];
+  long p0 = ID(b, x, y, z);
+  /* q direction */
+  sbp_stencil(x, b->nx, &cnt, idx, c);
+  for (int f = 0; f < 9; ++f) {
+    double s = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+      long p = ID(b, idx[k], y, z);
+      double term = f < 3 ? c[k] * b->F[f][p] : c[k] * b->F[f][p] * b->J[p] * X[0][p];
+      s = (k == 0) ? term : s + term;
+    }
+    Jq[f] = f < 3 ? X[0][p0] * s : s;
+  }
+  sbp_stencil(y, b->ny, &cnt, idx, c);
+  for (int f = 0; f < 9; ++f) {
+    double s = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+      long p = ID(b, x, idx[k], z);
+      double term = f < 3 ? c[k] * b->F[f][p] : c[k] * b->F[f][p] * b->J[p] * X[1][p];
+      s = (k == 0) ? term : s + term;
+    }
+    Jr[f] = f < 3 ? X[1][p0] * s : s;
+  }
+  sbp_stencil(z, b->nz, &cnt, idx, c);
+  for (int f = 0; f < 9; ++f) {
+    double s = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+      long p = ID(b, x, y, idx[k]);
+      double term = f < 3 ? c[k] * b->F[f][p] : c[k] * b->F[f][p] * b->J[p] * X[2][p];
+      s = (k == 0) ? term : s + term;
+    }
+    Js[f] = f < 3 ? X[2][p0] * s : s;
+  }
+  for (int f = 0; f < 9; ++f) Ju[f] = (1.0 / b->hq) * Jq[f] + (1.0 / b->hr) * Jr[f] + (1.0 / b->hs) * Js[f];
+}
+
+/* ------------------------------------------------------------------------ */
+/* PML: src/RHS_Interior.f90:1846-2265, src/RHS_Interior.f90:2351-2451       */
+/* ------------------------------------------------------------------------ */
+static double pml_d0(void) { return 6.0 / (2.0 * 1.0) * log(1.0 / 1.0e-3); }
+
+static int in_slab(const oblk *b, int f, int x, int y, int z) {
+  const box_t *q = &b->pbox[f];
+  if (!q->active) return 0;
+  return x >= q->x0 && x <= q->x1 && y >= q->y0 && y <= q->y1 && z >= q->z0 && z <= q->z1;
+}
+
+/* damping for face f (0-based) at the point's coordinate */
+static double pml_damp(const oblk *b, int f, int x, int y, int z) {
+  int np = b->d.npml;
+  double d0 = pml_d0();
+  double v;
+  switch (f) {
+    case 0: v = (double)(x - (1 + np)); break;
+    case 1: v = (double)(x - (b->nx - np)); break;
+    case 2: v = (double)(y - (1 + np)); break;
+    case 3: v = (double)(y - (b->ny - np)); break;
+    case 4: v = (double)(z - np); break;        /* asymmetric offset, src/RHS_Interior.f90:1919 */
+    default: v = (double)(z - (b->nz - np)); break;
+  }
+  return d0 * fabs(v / (double)np);
+}
+
+static void pml_point(oblk *b, double DU[9], const double Ux[9], const double Uy[9], const double Uz[9],
+                      int x, int y, int z, double rhoJ_inv, double lambda2mu) {
+  static const int order[6] = {4, 5, 2, 3, 0, 1}; /* the reference applies z, y, x slabs in this order */
+  long p = ID(b, x, y, z);
+  double lam = b->M[0][p], mu = b->M[1][p];
+  double J = b->J[p];
+  const double cfs = 1.0;
+  for (int oi = 0; oi < 6; ++oi) {
+    int f = order[oi];
+    if (!b->d.pml[f] || !b->pbox[f].active) continue;
+    if (!in_slab(b, f, x, y, z)) continue;
+    double d = pml_damp(b, f, x, y, z);
+    long q = PID(b, f, x, y, z);
+    double *Qf[9], *DQf[9];
+    for (int c = 0; c < 9; ++c) { Qf[c] = b->Q[f][c]; DQf[c] = b->DQ[f][c]; }
+    DU[0] = DU[0] - d * J * Qf[0][q] * rhoJ_inv;
+    DU[1] = DU[1] - d * J * Qf[1][q] * rhoJ_inv;
+    DU[2] = DU[2] - d * J * Qf[2][q] * rhoJ_inv;
+    DU[3] = DU[3] - d * (lambda2mu * Qf[3][q] + lam * Qf[4][q] + lam * Qf[5][q]);
+    DU[4] = DU[4] - d * (lam * Qf[3][q] + lambda2mu * Qf[4][q] + lam * Qf[5][q]);
+    DU[5] = DU[5] - d * (lam * Qf[3][q] + lam * Qf[4][q] + lambda2mu * Qf[5][q]);
+    DU[6] = DU[6] - mu * d * Qf[6][q];
+    DU[7] = DU[7] - mu * d * Qf[7][q];
+    DU[8] = DU[8] - mu * d * Qf[8][q];
+    double src[9];
+    int axis = f / 2;
+    if (axis == 2) { /* z slabs, src/RHS_Interior.f90:1936-1962 */
+      src[0] = Uz[7] / J; src[1] = Uz[8] / J; src[2] = Uz[5] / J; src[3] = 0.0; src[4] = 0.0;
+      src[5] = Uz[2]; src[6] = 0.0; src[7] = Uz[0]; src[8] = Uz[1];
+    } else if (axis == 1) { /* y slabs */
+      src[0] = Uy[6] / J; src[1] = Uy[4] / J; src[2] = Uy[8] / J; src[3] = 0.0; src[4] = Uy[1];
+      src[5] = 0.0; src[6] = Uy[0]; src[7] = 0.0; src[8] = Uy[2];
+    } else { /* x slabs */
+      src[0] = Ux[3] / J; src[1] = Ux[6] / J; src[2] = Ux[7] / J; src[3] = Ux[0]; src[4] = 0.0;
+      src[5] = 0.0; src[6] = Ux[1]; src[7] = Ux[2]; src[8] = 0.0;
+    }
+    for (int c = 0; c < 9; ++c) DQf[c][q] = DQf[c][q] + src[c] - (d + cfs) * Qf[c][q];
+  }
+}
+
+/* pml_damping_and_q, src/RHS_Interior.f90:2351-2451 */
+static int pml_damping_and_q(const oblk *b, int x, int y, int z, double *dx, double *dy, double *dz,
+                             double Qx[9], double Qy[9], double Qz[9]) {
+  int inpml = 0;
+  *dx = *dy = *dz = 0.0;
+  for (int c = 0; c < 9; ++c) Qx[c] = Qy[c] = Qz[c] = 0.0;
+  for (int f = 0; f < 6; ++f) {
+    if (!b->d.pml[f] || !b->pbox[f].active || !in_slab(b, f, x, y, z)) continue;
+    inpml = 1;
+    double d = pml_damp(b, f, x, y, z);
+    long q = PID(b, f, x, y, z);
+    double *dd = f < 2 ? dx : f < 4 ? dy : dz;
+    double *QQ = f < 2 ? Qx : f < 4 ? Qy : Qz;
+    *dd = d;
+    for (int c = 0; c < 9; ++c) QQ[c] = b->Q[f][c][q];
+  }
+  return inpml;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Anelastic memory variables (Q4 / Q8 / fQ8):                               */
+/* src/RHS_Interior.f90:2599-2908 (Q4, Q8 point kernels + PML variants),     */
+/* src/RHS_Interior.f90:3361-3477 (fQ8), interior copies                     */
+/* src/JU_xJU_yJU_z6.f90:16263-16420.                                        */
+/* exx..gyz are the (PML-corrected) strain rates.                            */
+/* ------------------------------------------------------------------------ */
+static void anelastic_point(oblk *b, long p, int x, int y, int z, double exx, double eyy, double ezz,
+                            double gxy, double gxz, double gyz, double tr, double DU[9], int dfmode) {
+  int N = b->nmech;
+  double lam = b->M[0][p], mu = b->M[1][p];
+  double sum[6];
+  for (int c = 0; c < 6; ++c) {
+    double s = b->eta[c][0][p];
+    for (int i = 1; i < N; ++i) s = s + b->eta[c][i][p];
+    sum[c] = s;
+  }
+  if (dfmode) {
+    for (int c = 0; c < 6; ++c) b->DF[3 + c][p] = b->DF[3 + c][p] - sum[c];
+  } else {
+    for (int c = 0; c < 6; ++c) DU[3 + c] = DU[3 + c] - sum[c];
+  }
+  double e_n[3] = {exx, eyy, ezz};
+  double g_s[3] = {gxy, gxz, gyz};
+  if (b->d.response == ORC_FQ8) {
+    int active = 1 + ((x - 1) % 2) + 2 * ((y - 1) % 2) + 4 * ((z - 1) % 2);
+    for (int i = 0; i < N; ++i) {
+      if (b->d.coarse && (i + 1) != active) continue;
+      double ss = b->d.sstr[i], ps = b->d.pstr[i], tau = b->d.tau[i];
+      for (int c = 0; c < 3; ++c) {
+        double *De = &b->deta[c][i][p];
+        *De = *De + (((ss * 2.0 * mu) * e_n[c] + ((lam + 2.0 * mu) * ps - 2.0 * mu * ss) * tr) - b->eta[c][i][p]) / tau;
+      }
+      for (int c = 0; c < 3; ++c) {
+        double *De = &b->deta[3 + c][i][p];
+        *De = *De + ((ss * mu * g_s[c] - b->eta[3 + c][i][p]) / tau);
+      }
+    }
+  } else {
+    double qs = b->qs[p], qp = b->qp[p];
+    for (int i = 0; i < N; ++i) {
+      double w = b->d.weight[i], tau = b->d.tau[i];
+      for (int c = 0; c < 3; ++c) {
+        double *De = &b->deta[c][i][p];
+        *De = *De + (((w * 2.0 * mu * qs) * e_n[c] + (w * ((lam + 2.0 * mu) * qp - 2.0 * mu * qs)) * tr) - b->eta[c][i][p]) / tau;
+      }
+      for (int c = 0; c < 3; ++c) {
+        double *De = &b->deta[3 + c][i][p];
+        *De = *De + ((w * mu * qs * g_s[c] - b->eta[3 + c][i][p]) / tau);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* RHS_near_boundaries (traditional branch), src/RHS_Interior.f90:136-281    */
+/* ------------------------------------------------------------------------ */
+static void interior_bounds(const oblk *b, int lo[3], int hi[3]) {
+  /* src/RHS_Interior.f90:199-214, src/JU_xJU_yJU_z6.f90:16158-16173 */
+  int ix = 6, iy = 6, iz = 6, fx = 6, fy = 6, fz = 6;
+  const int *pm = b->d.pml;
+  int np = b->d.npml;
+  if (pm[4]) iz = np > 6 ? np : 6;
+  if (pm[5]) fz = np > 6 ? np : 6;
+  if (pm[2]) iy = np > 6 ? np : 6;
+  if (pm[3]) fy = np > 6 ? np : 6;
+  if (pm[0]) ix = np > 6 ? np : 6;
+  if (pm[1]) fx = np > 6 ? np : 6;
+  lo[0] = ix + 1; hi[0] = b->nx - fx;
+  lo[1] = iy + 1; hi[1] = b->ny - fy;
+  lo[2] = iz + 1; hi[2] = b->nz - fz;
+}
+
+static void rhs_near_boundaries(oblk *b) {
+  int lo[3], hi[3];
+  interior_bounds(b, lo, hi);
+#pragma omp parallel for schedule(static)
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) {
+        if ((lo[2] <= z && z <= hi[2]) && (lo[1] <= y && y <= hi[1]) && (lo[0] <= x && x <= hi[0])) continue;
+        double Ux[9], Uy[9], Uz[9], DU[9];
+        jju6(b, x, y, z, b->mx, Ux);
+        jju6(b, x, y, z, b->my, Uy);
+        jju6(b, x, y, z, b->mz, Uz);
+        long p = ID(b, x, y, z);
+        double rhoJ_inv = 1.0 / (b->M[2][p] * b->J[p]);
+        double lambda2mu = b->M[0][p] + 2.0 * b->M[1][p];
+        double lam = b->M[0][p], mu = b->M[1][p];
+        DU[0] = (Ux[3] + Uy[6] + Uz[7]) * rhoJ_inv;
+        DU[1] = (Ux[6] + Uy[4] + Uz[8]) * rhoJ_inv;
+        DU[2] = (Ux[7] + Uy[8] + Uz[5]) * rhoJ_inv;
+        DU[3] = lambda2mu * Ux[0] + lam * (Uy[1] + Uz[2]);
+        DU[4] = lambda2mu * Uy[1] + lam * (Ux[0] + Uz[2]);
+        DU[5] = lambda2mu * Uz[2] + lam * (Ux[0] + Uy[1]);
+        DU[6] = mu * (Uy[0] + Ux[1]);
+        DU[7] = mu * (Uz[0] + Ux[2]);
+        DU[8] = mu * (Uz[1] + Uy[2]);
+        if (b->d.response != ORC_ELASTIC) {
+          /* apply_anelastic_*_point_dispatch: PML variant corrects the strain rates */
+          double dxp, dyp, dzp, Qx[9], Qy[9], Qz[9];
+          double exx, eyy, ezz, gxy, gxz, gyz, tr;
+          if (pml_damping_and_q(b, x, y, z, &dxp, &dyp, &dzp, Qx, Qy, Qz)) {
+            exx = Ux[0] - dxp * Qx[3];
+            eyy = Uy[1] - dyp * Qy[4];
+            ezz = Uz[2] - dzp * Qz[5];
+            tr = exx + eyy + ezz;
+            gxy = (Uy[0] + Ux[1]) - dxp * Qx[6] - dyp * Qy[6];
+            gxz = (Uz[0] + Ux[2]) - dxp * Qx[7] - dzp * Qz[7];
+            gyz = (Uz[1] + Uy[2]) - dyp * Qy[8] - dzp * Qz[8];
+          } else {
+            exx = Ux[0]; eyy = Uy[1]; ezz = Uz[2];
+            tr = Ux[0] + Uy[1] + Uz[2];
+            gxy = Uy[0] + Ux[1]; gxz = Uz[0] + Ux[2]; gyz = Uz[1] + Uy[2];
+          }
+          anelastic_point(b, p, x, y, z, exx, eyy, ezz, gxy, gxz, gyz, tr, DU, 0);
+        }
+        pml_point(b, DU, Ux, Uy, Uz, x, y, z, rhoJ_inv, lambda2mu);
+        for (int f = 0; f < 9; ++f) b->DF[f][p] = b->DF[f][p] + DU[f];
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Strict interior JJU_x6_interior, src/JU_xJU_yJU_z6.f90:16088-16640        */
+/* ------------------------------------------------------------------------ */
+static void rhs_interior(oblk *b) {
+  int lo[3], hi[3];
+  interior_bounds(b, lo, hi);
+  static const double c[3] = {0.75, -0.15, 1.0 / 60.0};
+  double cx[3], cy[3], cz[3];
+  for (int s = 0; s < 3; ++s) { cx[s] = c[s] / b->hq; cy[s] = c[s] / b->hr; cz[s] = c[s] / b->hs; }
+  const long sx = 1, sy = b->NX, sz = (long)b->NX * b->NY;
+  int curv = b->d.mesh == 1;
+#pragma omp parallel for schedule(static)
+  for (int z = lo[2]; z <= hi[2]; ++z)
+    for (int y = lo[1]; y <= hi[1]; ++y)
+      for (int x = lo[0]; x <= hi[0]; ++x) {
+        long p = ID(b, x, y, z);
+        double DFx[9] = {0}, DFy[9] = {0}, DFz[9] = {0};
+        if (curv) { /* :16177-16424 */
+          for (int s = 1; s <= 3; ++s) {
+            double ccx = cx[s - 1], ccy = cy[s - 1], ccz = cz[s - 1];
+            long xp = p + s * sx, xm = p - s * sx, yp = p + s * sy, ym = p - s * sy, zp = p + s * sz, zm = p - s * sz;
+            for (int f = 0; f < 3; ++f) {
+              double ddx = b->F[f][xp] - b->F[f][xm], ddy = b->F[f][yp] - b->F[f][ym], ddz = b->F[f][zp] - b->F[f][zm];
+              DFx[f] = DFx[f] + b->mx[0][p] * ccx * ddx + b->mx[1][p] * ccy * ddy + b->mx[2][p] * ccz * ddz;
+              DFy[f] = DFy[f] + b->my[0][p] * ccx * ddx + b->my[1][p] * ccy * ddy + b->my[2][p] * ccz * ddz;
+              DFz[f] = DFz[f] + b->mz[0][p] * ccx * ddx + b->mz[1][p] * ccy * ddy + b->mz[2][p] * ccz * ddz;
+            }
+            for (int f = 3; f < 9; ++f) {
+              const double *Ff = b->F[f];
+              DFx[f] = DFx[f] + ccx * (Ff[xp] * (b->J[xp] * b->mx[0][xp]) - Ff[xm] * (b->J[xm] * b->mx[0][xm])) +
+                       ccy * (Ff[yp] * (b->J[yp] * b->mx[1][yp]) - Ff[ym] * (b->J[ym] * b->mx[1][ym])) +
+                       ccz * (Ff[zp] * (b->J[zp] * b->mx[2][zp]) - Ff[zm] * (b->J[zm] * b->mx[2][zm]));
+              DFy[f] = DFy[f] + ccx * (Ff[xp] * (b->J[xp] * b->my[0][xp]) - Ff[xm] * (b->J[xm] * b->my[0][xm])) +
+                       ccy * (Ff[yp] * (b->J[yp] * b->my[1][yp]) - Ff[ym] * (b->J[ym] * b->my[1][ym])) +
+                       ccz * (Ff[zp] * (b->J[zp] * b->my[2][zp]) - Ff[zm] * (b->J[zm] * b->my[2][zm]));
+              DFz[f] = DFz[f] + ccx * (Ff[xp] * (b->J[xp] * b->mz[0][xp]) - Ff[xm] * (b->J[xm] * b->mz[0][xm])) +
+                       ccy * (Ff[yp] * (b->J[yp] * b->mz[1][yp]) - Ff[ym] * (b->J[ym] * b->mz[1][ym])) +
+                       ccz * (Ff[zp] * (b->J[zp] * b->mz[2][zp]) - Ff[zm] * (b->J[zm] * b->mz[2][zm]));
+            }
+          }
+        } else { /* Cartesian, :16426-16450 */
+          for (int s = 1; s <= 3; ++s)
+            for (int f = 0; f < 9; ++f) {
+              DFx[f] = DFx[f] + b->mx[0][p] * cx[s - 1] * (b->F[f][p + s * sx] - b->F[f][p - s * sx]);
+              DFy[f] = DFy[f] + b->my[1][p] * cy[s - 1] * (b->F[f][p + s * sy] - b->F[f][p - s * sy]);
+              DFz[f] = DFz[f] + b->mz[2][p] * cz[s - 1] * (b->F[f][p + s * sz] - b->F[f][p - s * sz]);
+            }
+        }
+        double a1 = curv ? 1.0 / (b->M[2][p] * b->J[p]) : 1.0 / b->M[2][p];
+        double a2 = 2.0 * b->M[1][p] + b->M[0][p];
+        double a3 = b->M[0][p];
+        double a4 = b->M[1][p];
+        b->DF[0][p] = b->DF[0][p] + a1 * (DFx[3] + DFy[6] + DFz[7]);
+        b->DF[1][p] = b->DF[1][p] + a1 * (DFx[6] + DFy[4] + DFz[8]);
+        b->DF[2][p] = b->DF[2][p] + a1 * (DFx[7] + DFy[8] + DFz[5]);
+        b->DF[3][p] = b->DF[3][p] + a2 * DFx[0] + a3 * (DFy[1] + DFz[2]);
+        b->DF[4][p] = b->DF[4][p] + a2 * DFy[1] + a3 * (DFx[0] + DFz[2]);
+        b->DF[5][p] = b->DF[5][p] + a2 * DFz[2] + a3 * (DFx[0] + DFy[1]);
+        b->DF[6][p] = b->DF[6][p] + a4 * (DFy[0] + DFx[1]);
+        b->DF[7][p] = b->DF[7][p] + a4 * (DFz[0] + DFx[2]);
+        b->DF[8][p] = b->DF[8][p] + a4 * (DFz[1] + DFy[2]);
+        if (b->d.response != ORC_ELASTIC) {
+          double tr = DFx[0] + DFy[1] + DFz[2];
+          anelastic_point(b, p, x, y, z, DFx[0], DFy[1], DFz[2], DFy[0] + DFx[1], DFz[0] + DFx[2],
+                          DFz[1] + DFy[2], tr, NULL, 1);
+        }
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Physical-boundary SAT: src/BoundaryConditions.f90:50-924,                 */
+/* src/RHS_Interior.f90:1584-1768 (impose), :2267-2287 (structure)           */
+/* ------------------------------------------------------------------------ */
+static void bc_point(int plus, const double u[9], double rho, double mu, double lambda, const double l[3],
+                     const double m[3], const double n[3], double norm, double Zs, double Zp, double r,
+                     double ubc[9]) {
+  double T[3];
+  T[0] = n[0] * u[3] + n[1] * u[6] + n[2] * u[7];
+  T[1] = n[0] * u[6] + n[1] * u[4] + n[2] * u[8];
+  T[2] = n[0] * u[7] + n[1] * u[8] + n[2] * u[5];
+  double vl = l[0] * u[0] + l[1] * u[1] + l[2] * u[2];
+  double vm = m[0] * u[0] + m[1] * u[1] + m[2] * u[2];
+  double vn = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+  double Tl = l[0] * T[0] + l[1] * T[1] + l[2] * T[2];
+  double Tm = m[0] * T[0] + m[1] * T[1] + m[2] * T[2];
+  double Tn = n[0] * T[0] + n[1] * T[1] + n[2] * T[2];
+  double pl, pm, pn, ql, qm, qn;
+  if (plus) { /* BCp, :783-852 */
+    pl = 0.5 * ((1.0 - r) * Zs * vl + (1.0 + r) * Tl);
+    pm = 0.5 * ((1.0 - r) * Zs * vm + (1.0 + r) * Tm);
+    pn = 0.5 * ((1.0 - r) * Zp * vn + (1.0 + r) * Tn);
+    ql = 0.5 * ((1.0 - r) * vl + (1.0 + r) / Zs * Tl);
+    qm = 0.5 * ((1.0 - r) * vm + (1.0 + r) / Zs * Tm);
+    qn = 0.5 * ((1.0 - r) * vn + (1.0 + r) / Zp * Tn);
+  } else { /* BCm, :855-924 */
+    pl = 0.5 * ((1.0 - r) * Zs * vl - (1.0 + r) * Tl);
+    pm = 0.5 * ((1.0 - r) * Zs * vm - (1.0 + r) * Tm);
+    pn = 0.5 * ((1.0 - r) * Zp * vn - (1.0 + r) * Tn);
+    ql = 0.5 * ((1.0 - r) * vl - (1.0 + r) / Zs * Tl);
+    qm = 0.5 * ((1.0 - r) * vm - (1.0 + r) / Zs * Tm);
+    qn = 0.5 * ((1.0 - r) * vn - (1.0 + r) / Zp * Tn);
+  }
+  double Fx = l[0] * pl + m[0] * pm + n[0] * pn;
+  double Fy = l[1] * pl + m[1] * pm + n[1] * pn;
+  double Fz = l[2] * pl + m[2] * pm + n[2] * pn;
+  double F_x = l[0] * ql + m[0] * qm + n[0] * qn;
+  double F_y = l[1] * ql + m[1] * qm + n[1] * qn;
+  double F_z = l[2] * ql + m[2] * qm + n[2] * qn;
+  (void)rho; (void)mu; (void)lambda;
+  double sg = plus ? 1.0 : -1.0;
+  ubc[0] = norm * Fx;
+  ubc[1] = norm * Fy;
+  ubc[2] = norm * Fz;
+  ubc[3] = sg * (norm * n[0] * F_x);
+  ubc[4] = sg * (norm * n[1] * F_y);
+  ubc[5] = sg * (norm * n[2] * F_z);
+  ubc[6] = sg * (norm * (n[1] * F_x + n[0] * F_y));
+  ubc[7] = sg * (norm * (n[2] * F_x + n[0] * F_z));
+  ubc[8] = sg * (norm * (n[2] * F_y + n[1] * F_z));
+}
+
+static void structure(double Ux[9], const double Uq[9], double rho, double mu, double lam) {
+  Ux[0] = 1.0 / rho * Uq[0];
+  Ux[1] = 1.0 / rho * Uq[1];
+  Ux[2] = 1.0 / rho * Uq[2];
+  Ux[3] = (2.0 * mu + lam) * Uq[3] + lam * (Uq[4] + Uq[5]);
+  Ux[4] = (2.0 * mu + lam) * Uq[4] + lam * (Uq[3] + Uq[5]);
+  Ux[5] = (2.0 * mu + lam) * Uq[5] + lam * (Uq[3] + Uq[4]);
+  Ux[6] = mu * Uq[6];
+  Ux[7] = mu * Uq[7];
+  Ux[8] = mu * Uq[8];
+}
+
+static void impose_boundary_condition(oblk *b) {
+  const double tau0 = b->d.tau0;
+  const double hs_[3] = {b->hq, b->hr, b->hs};
+  for (int f = 0; f < 6; ++f) {
+    int type = b->d.bc[f];
+    if (type <= 0) continue;
+    int axis = f / 2, plus = f % 2;
+    double r = type == 1 ? 0.0 : type == 2 ? 1.0 : -1.0;
+    int fixed = plus ? (axis == 0 ? b->nx : axis == 1 ? b->ny : b->nz) : 1;
+    int d0 = b->fdim[f][0], d1 = b->fdim[f][1];
+    /* BC_* builds u_bc for the whole face first, then impose applies it */
+    for (int c2 = 1; c2 <= d1; ++c2)
+      for (int c1 = 1; c1 <= d0; ++c1) {
+        int x, y, z;
+        if (axis == 0) { x = fixed; y = c1; z = c2; }
+        else if (axis == 1) { x = c1; y = fixed; z = c2; }
+        else { x = c1; y = c2; z = fixed; }
+        long p = ID(b, x, y, z);
+        double rho = b->M[2][p], mu = b->M[1][p], lambda = b->M[0][p];
+        double c_p = sqrt((2.0 * mu + lambda) / rho);
+        double c_s = sqrt(mu / rho);
+        double Zp = rho * c_p, Zs = rho * c_s;
+        double qx = b->mx[axis][p], qy = b->my[axis][p], qz = b->mz[axis][p];
+        double norm = sqrt(qx * qx + qy * qy + qz * qz);
+        long fp = FID(b, f, c1, c2);
+        double l3[3], m3[3], n3[3], u[9], ubc[9];
+        for (int c = 0; c < 3; ++c) { l3[c] = b->nl[f][c][fp]; m3[c] = b->nm[f][c][fp]; n3[c] = b->nn[f][c][fp]; }
+        for (int c = 0; c < 9; ++c) u[c] = b->F[c][p];
+        bc_point(plus, u, rho, mu, lambda, l3, m3, n3, norm, Zs, Zp, r, ubc);
+        for (int c = 0; c < 9; ++c) b->work[f][c][fp] = ubc[c];
+      }
+    double h = hs_[axis];
+    for (int c2 = 1; c2 <= d1; ++c2)
+      for (int c1 = 1; c1 <= d0; ++c1) {
+        int x, y, z;
+        if (axis == 0) { x = fixed; y = c1; z = c2; }
+        else if (axis == 1) { x = c1; y = fixed; z = c2; }
+        else { x = c1; y = c2; z = fixed; }
+        long p = ID(b, x, y, z);
+        long fp = FID(b, f, c1, c2);
+        double Uq[9], Ux[9];
+        for (int c = 0; c < 9; ++c) Uq[c] = b->work[f][c][fp];
+        structure(Ux, Uq, b->M[2][p], b->M[1][p], b->M[0][p]);
+        for (int c = 0; c < 9; ++c) b->DF[c][p] = b->DF[c][p] - tau0 / h * Ux[c];
+        if (b->d.pml[f] && b->pbox[f].active && in_slab(b, f, x, y, z)) {
+          long q = PID(b, f, x, y, z);
+          for (int c = 0; c < 9; ++c) b->DQ[f][c][q] = b->DQ[f][c][q] - tau0 / h * Uq[c];
+        }
+      }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Block-interface coupling (q direction): src/CouplingForcing.f90:9-463,     */
+/* src/Interface_Condition.f90:12-916                                         */
+/* ------------------------------------------------------------------------ */
+void orc_iface_couple(odom *D, int ib, double t, int stage);
+
+/* ------------------------------------------------------------------------ */
+/* Block creation                                                            */
+/* ------------------------------------------------------------------------ */
+static oblk *block_create(const orc_desc *d) {
+  sbp_init(d->f32lit);
+  oblk *b = (oblk *)calloc(1, sizeof(oblk));
+  b->d = *d;
+  b->nx = d->nq; b->ny = d->nr; b->nz = d->ns;
+  b->NX = b->nx + 2 * NB; b->NY = b->ny + 2 * NB; b->NZ = b->nz + 2 * NB;
+  b->np = (long)b->NX * b->NY * b->NZ;
+  build_grid(b);
+  long n1 = (long)b->nx * b->ny * b->nz;
+  for (int c = 0; c < 3; ++c) b->M[c] = zalloc(b->np, 0.0);
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) {
+        long p = ID(b, x, y, z);
+        long q = (x - 1) + (long)b->nx * ((y - 1) + (long)b->ny * (z - 1));
+        if (d->material) {
+          for (int c = 0; c < 3; ++c) b->M[c][p] = d->material[c * n1 + q];
+        } else { /* src/material.f90:696-701 */
+          const double *r = d->rho_s_p;
+          b->M[0][p] = r[0] * (r[2] * r[2] - 2.0 * (r[1] * r[1]));
+          b->M[1][p] = r[0] * (r[1] * r[1]);
+          b->M[2][p] = r[0];
+        }
+      }
+  for (int c = 0; c < 9; ++c) { b->F[c] = zalloc(b->np, 0.0); b->DF[c] = zalloc(b->np, 1.0e40); } /* src/fields.f90:38-39 */
+  /* PML slabs, src/pml.f90:11-168 */
+  for (int f = 0; f < 6; ++f) {
+    box_t *q = &b->pbox[f];
+    q->x0 = 1; q->x1 = b->nx; q->y0 = 1; q->y1 = b->ny; q->z0 = 1; q->z1 = b->nz;
+    q->active = d->pml[f] && d->npml > 0;
+    if (!q->active) continue;
+    int np = d->npml;
+    switch (f) {
+      case 0: q->x1 = np; break;
+      case 1: q->x0 = b->nx - np + 1; break;
+      case 2: q->y1 = np; break;
+      case 3: q->y0 = b->ny - np + 1; break;
+      case 4: q->z1 = np; break;
+      default: q->z0 = b->nz - np + 1; break;
+    }
+    long n = (long)(q->x1 - q->x0 + 1) * (q->y1 - q->y0 + 1) * (q->z1 - q->z0 + 1);
+    for (int c = 0; c < 9; ++c) { b->Q[f][c] = zalloc(n, 0.0); b->DQ[f][c] = zalloc(n, 1.0e40); }
+  }
+  /* anelastic state */
+  if (d->response != ORC_ELASTIC) {
+    b->nmech = d->response == ORC_Q4 ? 4 : 8;
+    b->qs = zalloc(b->np, 0.0);
+    b->qp = zalloc(b->np, 0.0);
+    for (int z = 1; z <= b->nz; ++z)
+      for (int y = 1; y <= b->ny; ++y)
+        for (int x = 1; x <= b->nx; ++x) {
+          long p = ID(b, x, y, z);
+          long q = (x - 1) + (long)b->nx * ((y - 1) + (long)b->ny * (z - 1));
+          if (d->qsinv) b->qs[p] = d->qsinv[q];
+          if (d->qpinv) b->qp[p] = d->qpinv[q];
+        }
+    for (int c = 0; c < 6; ++c)
+      for (int i = 0; i < b->nmech; ++i) { b->eta[c][i] = zalloc(b->np, 0.0); b->deta[c][i] = zalloc(b->np, 0.0); }
+  }
+  build_normals(b);
+  /* sources */
+  b->nsrc = d->nsrc;
+  if (b->nsrc > 0) {
+    b->stype = (int *)malloc(sizeof(int) * b->nsrc);
+    b->spar = (double *)malloc(sizeof(double) * 11 * b->nsrc);
+    b->snear = (int *)malloc(sizeof(int) * 3 * b->nsrc);
+    b->sphys = (double *)malloc(sizeof(double) * 3 * b->nsrc);
+    memcpy(b->stype, d->src_type, sizeof(int) * b->nsrc);
+    memcpy(b->spar, d->src_par, sizeof(double) * 11 * b->nsrc);
+    for (int i = 0; i < b->nsrc; ++i) {
+      nearest_node_moment(b, b->spar[11 * i + 8], b->spar[11 * i + 9], b->spar[11 * i + 10], &b->snear[3 * i]);
+      if (b->snear[3 * i] > 0) {
+        long p = ID(b, b->snear[3 * i], b->snear[3 * i + 1], b->snear[3 * i + 2]);
+        for (int c = 0; c < 3; ++c) b->sphys[3 * i + c] = b->X[c][p];
+      } else {
+        for (int c = 0; c < 3; ++c) b->sphys[3 * i + c] = -1.0;
+      }
+    }
+  }
+  b->nrec = d->nrec;
+  if (b->nrec > 0) {
+    b->ridx = (int *)malloc(sizeof(int) * 3 * b->nrec);
+    for (int i = 0; i < b->nrec; ++i)
+      nearest_node_receiver(b, d->rec_xyz[3 * i], d->rec_xyz[3 * i + 1], d->rec_xyz[3 * i + 2], &b->ridx[3 * i]);
+  }
+  for (int s = 0; s < 2; ++s) {
+    long n = (long)b->ny * b->nz;
+    for (int c = 0; c < 9; ++c) { b->faceF[s][c] = zalloc(n, 0.0); b->faceFopp[s][c] = zalloc(n, 0.0); }
+    for (int c = 0; c < 3; ++c) { b->faceM[s][c] = zalloc(n, 0.0); b->faceMopp[s][c] = zalloc(n, 0.0); }
+  }
+  /* copy_materials_to_boundary, src/block.f90:484-495 */
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y) {
+      long fp = (y - 1) + (long)b->ny * (z - 1);
+      for (int c = 0; c < 3; ++c) {
+        b->faceM[0][c][fp] = b->M[c][ID(b, 1, y, z)];
+        b->faceM[1][c][fp] = b->M[c][ID(b, b->nx, y, z)];
+      }
+    }
+  return b;
+}
+
+static void block_free(oblk *b) {
+  if (!b) return;
+  for (int c = 0; c < 3; ++c) { free(b->X[c]); free(b->mx[c]); free(b->my[c]); free(b->mz[c]); free(b->M[c]); }
+  free(b->J);
+  for (int c = 0; c < 9; ++c) { free(b->F[c]); free(b->DF[c]); }
+  for (int f = 0; f < 6; ++f) {
+    for (int c = 0; c < 9; ++c) { free(b->Q[f][c]); free(b->DQ[f][c]); free(b->work[f][c]); }
+    for (int c = 0; c < 3; ++c) { free(b->nl[f][c]); free(b->nm[f][c]); free(b->nn[f][c]); }
+  }
+  free(b->qs); free(b->qp);
+  for (int c = 0; c < 6; ++c)
+    for (int i = 0; i < 8; ++i) { free(b->eta[c][i]); free(b->deta[c][i]); }
+  free(b->stype); free(b->spar); free(b->snear); free(b->sphys); free(b->ridx);
+  for (int s = 0; s < 2; ++s) {
+    for (int c = 0; c < 9; ++c) { free(b->faceF[s][c]); free(b->faceFopp[s][c]); }
+    for (int c = 0; c < 3; ++c) { free(b->faceM[s][c]); free(b->faceMopp[s][c]); }
+  }
+  free(b);
+}
+
+/* ------------------------------------------------------------------------ */
+/* RK vector operations: src/rk_vector_cpu.f90:7-18, fan-out                 */
+/* src/fields.f90:51-263                                                     */
+/* ------------------------------------------------------------------------ */
+static void scale_rates_block(oblk *b, double A) {
+  for (int c = 0; c < 9; ++c)
+    for (long i = 0; i < b->np; ++i) b->DF[c][i] = A * b->DF[c][i];
+  for (int c = 0; c < 6; ++c)
+    for (int k = 0; k < b->nmech; ++k)
+      for (long i = 0; i < b->np; ++i) b->deta[c][k][i] = A * b->deta[c][k][i];
+  for (int f = 0; f < 6; ++f) {
+    if (!b->pbox[f].active) continue;
+    const box_t *q = &b->pbox[f];
+    long n = (long)(q->x1 - q->x0 + 1) * (q->y1 - q->y0 + 1) * (q->z1 - q->z0 + 1);
+    for (int c = 0; c < 9; ++c)
+      for (long i = 0; i < n; ++i) b->DQ[f][c][i] = A * b->DQ[f][c][i];
+  }
+}
+
+static void update_fields_block(oblk *b, double dt) {
+  for (int c = 0; c < 9; ++c)
+    for (long i = 0; i < b->np; ++i) b->F[c][i] = b->F[c][i] + dt * b->DF[c][i];
+  for (int c = 0; c < 6; ++c)
+    for (int k = 0; k < b->nmech; ++k)
+      for (long i = 0; i < b->np; ++i) b->eta[c][k][i] = b->eta[c][k][i] + dt * b->deta[c][k][i];
+  for (int f = 0; f < 6; ++f) {
+    if (!b->pbox[f].active) continue;
+    const box_t *q = &b->pbox[f];
+    long n = (long)(q->x1 - q->x0 + 1) * (q->y1 - q->y0 + 1) * (q->z1 - q->z0 + 1);
+    for (int c = 0; c < 9; ++c)
+      for (long i = 0; i < n; ++i) b->Q[f][c][i] = b->Q[f][c][i] + dt * b->DQ[f][c][i];
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Low-storage RK: src/time_step.f90:20-150 (Kennedy-Carpenter (5,4))        */
+/* ------------------------------------------------------------------------ */
+static const double RK_A[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                               -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+static const double RK_B[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                               1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                               2277821191437.0 / 14882151754819.0};
+static const double RK_C[6] = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                               2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0, 1.0};
+
+static void iface_scale(oiface *I, double A) {
+  if (!I) return;
+  long n = (long)I->nr * I->ns;
+  for (int c = 0; c < 4; ++c)
+    for (long i = 0; i < n; ++i) I->DS[c][i] = A * I->DS[c][i];
+  for (long i = 0; i < n; ++i) I->DW[i] = A * I->DW[i];
+}
+
+static void iface_update(oiface *I, double dt) {
+  if (!I) return;
+  long n = (long)I->nr * I->ns;
+  for (int c = 0; c < 4; ++c)
+    for (long i = 0; i < n; ++i) I->S[c][i] = I->S[c][i] + dt * I->DS[c][i];
+  for (long i = 0; i < n; ++i) I->W[i] = I->W[i] + dt * I->DW[i];
+}
+
+static void copy_fields_to_boundary(oblk *b) { /* src/block.f90:466-482 */
+  for (int c = 0; c < 9; ++c)
+    for (int z = 1; z <= b->nz; ++z)
+      for (int y = 1; y <= b->ny; ++y) {
+        long fp = (y - 1) + (long)b->ny * (z - 1);
+        b->faceF[0][c][fp] = b->F[c][ID(b, 1, y, z)];
+        b->faceF[1][c][fp] = b->F[c][ID(b, b->nx, y, z)];
+      }
+}
+
+static void sample_receivers(oblk *b, double t, double *out) {
+  for (int r = 0; r < b->nrec; ++r) {
+    int i = b->ridx[3 * r], j = b->ridx[3 * r + 1], k = b->ridx[3 * r + 2];
+    out[4 * r] = t;
+    if (i > 0 && j > 0 && k > 0) {
+      long p = ID(b, i, j, k);
+      out[4 * r + 1] = b->F[0][p]; out[4 * r + 2] = b->F[1][p]; out[4 * r + 3] = b->F[2][p];
+    } else {
+      out[4 * r + 1] = out[4 * r + 2] = out[4 * r + 3] = 0.0;
+    }
+  }
+}
+
+static void do_stage(odom *D, int stage, double dt, double t0, int sample, double *seis0, double *seis1) {
+  /* exchange_fields: single rank, no-op */
+  for (int i = 0; i < D->nb; ++i) scale_rates_block(D->B[i], RK_A[stage - 1]);
+  iface_scale(D->I, RK_A[stage - 1]);
+  for (int i = 0; i < D->nb; ++i) {
+    oblk *b = D->B[i];
+    rhs_interior(b);
+    rhs_near_boundaries(b);
+    if (b->nsrc > 0) set_moment_tensor(b, D->t);
+  }
+  if (D->nb == 2) { /* exchange_fields_interface, src/domain.f90:696-726 (serial copy) */
+    copy_fields_to_boundary(D->B[0]);
+    copy_fields_to_boundary(D->B[1]);
+    long n = (long)D->B[0]->ny * D->B[0]->nz;
+    for (int c = 0; c < 9; ++c)
+      for (long k = 0; k < n; ++k) {
+        D->B[0]->faceFopp[1][c][k] = D->B[1]->faceF[0][c][k];
+        D->B[1]->faceFopp[0][c][k] = D->B[0]->faceF[1][c][k];
+      }
+  }
+  /* enforce_bound_iface_conditions, src/domain.f90:615-644 */
+  impose_boundary_condition(D->B[0]);
+  if (D->nb == 2) orc_iface_couple(D, 2, D->t, stage);
+  if (D->nb == 2) {
+    impose_boundary_condition(D->B[1]);
+    orc_iface_couple(D, 1, D->t, stage);
+  }
+  if (sample) {
+    if (seis0) sample_receivers(D->B[0], D->t, seis0);
+    if (seis1 && D->nb == 2) sample_receivers(D->B[1], D->t, seis1);
+  }
+  D->t = t0 + RK_C[stage] * dt;
+  for (int i = 0; i < D->nb; ++i) update_fields_block(D->B[i], RK_B[stage - 1] * dt);
+  iface_update(D->I, RK_B[stage - 1] * dt);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Public API                                                                */
+/* ------------------------------------------------------------------------ */
+void *orc_create(int nblocks, const orc_desc *blocks, const orc_iface_desc *iface) {
+  odom *D = (odom *)calloc(1, sizeof(odom));
+  D->nb = nblocks;
+  for (int i = 0; i < nblocks; ++i) D->B[i] = block_create(&blocks[i]);
+  if (nblocks == 2) {
+    oblk *b0 = D->B[0], *b1 = D->B[1];
+    long n = (long)b0->ny * b0->nz;
+    for (int c = 0; c < 3; ++c)
+      for (long k = 0; k < n; ++k) { /* exchange_materials_interface, src/domain.f90:728-754 */
+        b0->faceMopp[1][c][k] = b1->faceM[0][c][k];
+        b1->faceMopp[0][c][k] = b0->faceM[1][c][k];
+      }
+    oiface *I = (oiface *)calloc(1, sizeof(oiface));
+    if (iface) I->d = *iface;
+    I->nr = b0->ny; I->ns = b0->nz;
+    for (int c = 0; c < 4; ++c) { I->S[c] = zalloc(n, 0.0); I->DS[c] = zalloc(n, 0.0); }
+    I->W = zalloc(n, 0.0); I->DW = zalloc(n, 0.0);
+    for (int c = 0; c < 3; ++c) I->Svel[c] = zalloc(n, 0.0);
+    I->trup = zalloc(n, 1.0e9);
+    I->t0n = zalloc(n, 0.0); I->t0m = zalloc(n, 0.0); I->t0l = zalloc(n, 0.0); I->fsm = zalloc(n, iface ? iface->fs : 0.0);
+    if (iface) {
+      for (long k = 0; k < n; ++k) {
+        if (iface->tau0_n) I->t0n[k] = iface->tau0_n[k];
+        if (iface->tau0_m) I->t0m[k] = iface->tau0_m[k];
+        if (iface->tau0_l) I->t0l[k] = iface->tau0_l[k];
+        if (iface->fs_map) I->fsm[k] = iface->fs_map[k];
+      }
+    }
+    D->I = I;
+  }
+  D->t = 0.0;
+  return D;
+}
+
+void orc_destroy(void *dv) {
+  odom *D = (odom *)dv;
+  if (!D) return;
+  for (int i = 0; i < D->nb; ++i) block_free(D->B[i]);
+  if (D->I) {
+    for (int c = 0; c < 4; ++c) { free(D->I->S[c]); free(D->I->DS[c]); }
+    for (int c = 0; c < 3; ++c) free(D->I->Svel[c]);
+    free(D->I->W); free(D->I->DW); free(D->I->trup);
+    free(D->I->t0n); free(D->I->t0m); free(D->I->t0l); free(D->I->fsm);
+    free(D->I);
+  }
+  free(D);
+}
+
+double orc_time(void *dv) { return ((odom *)dv)->t; }
+void orc_set_time(void *dv, double t) { ((odom *)dv)->t = t; }
+
+int orc_run(void *dv, double dt, int nsteps, int w_stride, double *seis0, double *seis1) {
+  odom *D = (odom *)dv;
+  int nsamp = 0;
+  for (int n = 1; n <= nsteps; ++n) {
+    double t0 = D->t;
+    int sample = (w_stride > 0) && ((n - 1) % w_stride == 0);
+    double *s0 = (sample && seis0) ? seis0 + (long)nsamp * 4 * D->B[0]->nrec : NULL;
+    double *s1 = (sample && seis1 && D->nb == 2) ? seis1 + (long)nsamp * 4 * D->B[1]->nrec : NULL;
+    for (int stage = 1; stage <= 5; ++stage) do_stage(D, stage, dt, t0, stage == 1 && sample, s0, s1);
+    if (sample) ++nsamp;
+  }
+  return nsamp;
+}
+
+void orc_stage(void *dv, int stage, double dt) {
+  odom *D = (odom *)dv;
+  do_stage(D, stage, dt, D->t, 0, NULL, NULL);
+}
+
+static void get3(const oblk *b, double *const *src, int ncomp, double *out) {
+  long n1 = (long)b->nx * b->ny * b->nz;
+  for (int c = 0; c < ncomp; ++c)
+    for (int z = 1; z <= b->nz; ++z)
+      for (int y = 1; y <= b->ny; ++y)
+        for (int x = 1; x <= b->nx; ++x)
+          out[c * n1 + (x - 1) + (long)b->nx * ((y - 1) + (long)b->ny * (z - 1))] = src[c][ID(b, x, y, z)];
+}
+static void set3(oblk *b, double *const *dst, int ncomp, const double *in) {
+  long n1 = (long)b->nx * b->ny * b->nz;
+  for (int c = 0; c < ncomp; ++c)
+    for (int z = 1; z <= b->nz; ++z)
+      for (int y = 1; y <= b->ny; ++y)
+        for (int x = 1; x <= b->nx; ++x)
+          dst[c][ID(b, x, y, z)] = in[c * n1 + (x - 1) + (long)b->nx * ((y - 1) + (long)b->ny * (z - 1))];
+}
+
+void orc_get_fields(void *dv, int bi, double *out) { oblk *b = ((odom *)dv)->B[bi]; get3(b, b->F, 9, out); }
+void orc_set_fields(void *dv, int bi, const double *in) { oblk *b = ((odom *)dv)->B[bi]; set3(b, b->F, 9, in); }
+void orc_get_rates(void *dv, int bi, double *out) { oblk *b = ((odom *)dv)->B[bi]; get3(b, b->DF, 9, out); }
+void orc_set_rates(void *dv, int bi, const double *in) { oblk *b = ((odom *)dv)->B[bi]; set3(b, b->DF, 9, in); }
+void orc_get_material(void *dv, int bi, double *out) { oblk *b = ((odom *)dv)->B[bi]; get3(b, b->M, 3, out); }
+void orc_get_metrics(void *dv, int bi, double *out) {
+  oblk *b = ((odom *)dv)->B[bi];
+  double *arr[10] = {b->mx[0], b->mx[1], b->mx[2], b->my[0], b->my[1], b->my[2], b->mz[0], b->mz[1], b->mz[2], b->J};
+  get3(b, arr, 10, out);
+}
+int orc_get_eta(void *dv, int bi, double *out) {
+  oblk *b = ((odom *)dv)->B[bi];
+  long n1 = (long)b->nx * b->ny * b->nz;
+  for (int c = 0; c < 6; ++c) get3(b, b->eta[c], b->nmech, out + (long)c * b->nmech * n1);
+  return b->nmech;
+}
+void orc_set_eta(void *dv, int bi, const double *in) {
+  oblk *b = ((odom *)dv)->B[bi];
+  long n1 = (long)b->nx * b->ny * b->nz;
+  for (int c = 0; c < 6; ++c) set3(b, b->eta[c], b->nmech, in + (long)c * b->nmech * n1);
+}
+void orc_get_pml(void *dv, int bi, int face, double *out) {
+  oblk *b = ((odom *)dv)->B[bi];
+  const box_t *q = &b->pbox[face];
+  if (!q->active) return;
+  long n = (long)(q->x1 - q->x0 + 1) * (q->y1 - q->y0 + 1) * (q->z1 - q->z0 + 1);
+  for (int c = 0; c < 9; ++c) memcpy(out + c * n, b->Q[face][c], sizeof(double) * n);
+}
+void orc_get_normals(void *dv, int bi, int face, double *out) {
+  oblk *b = ((odom *)dv)->B[bi];
+  long n = (long)b->fdim[face][0] * b->fdim[face][1];
+  for (int c = 0; c < 3; ++c) {
+    memcpy(out + (0 + c) * n, b->nl[face][c], sizeof(double) * n);
+    memcpy(out + (3 + c) * n, b->nm[face][c], sizeof(double) * n);
+    memcpy(out + (6 + c) * n, b->nn[face][c], sizeof(double) * n);
+  }
+}
+void orc_get_iface(void *dv, double *out) {
+  odom *D = (odom *)dv;
+  if (!D->I) return;
+  long n = (long)D->I->nr * D->I->ns;
+  for (long k = 0; k < n; ++k) {
+    for (int c = 0; c < 4; ++c) out[7 * k + c] = D->I->S[c][k];
+    out[7 * k + 4] = D->I->W[k];
+    out[7 * k + 5] = sqrt(D->I->Svel[1][k] * D->I->Svel[1][k] + D->I->Svel[2][k] * D->I->Svel[2][k]);
+    out[7 * k + 6] = D->I->trup[k];
+  }
+}
+void orc_receiver_index(void *dv, int bi, int *idx) {
+  oblk *b = ((odom *)dv)->B[bi];
+  memcpy(idx, b->ridx, sizeof(int) * 3 * b->nrec);
+}
+
+/* close_domain diagnostics, src/domain.f90:505-613: max over the whole
+   allocated arrays (ghost layers included) */
+void orc_final_state(void *dv, double *maxF, double *maxEta, double *maxB) {
+  odom *D = (odom *)dv;
+  double mf = 0.0, me = 0.0;
+  for (int i = 0; i < D->nb; ++i) {
+    oblk *b = D->B[i];
+    double mb = 0.0;
+    for (int c = 0; c < 9; ++c)
+      for (long k = 0; k < b->np; ++k) { double v = fabs(b->F[c][k]); if (v > mb) mb = v; }
+    if (maxB) maxB[i] = mb;
+    if (mb > mf) mf = mb;
+    for (int c = 0; c < 6; ++c)
+      for (int m = 0; m < b->nmech; ++m)
+        for (long k = 0; k < b->np; ++k) { double v = fabs(b->eta[c][m][k]); if (v > me) me = v; }
+  }
+  *maxF = mf;
+  *maxEta = me;
+}
+
+/* Q4 / Q8 fixed coefficients */
+void orc_q4_coefficients(double fmin, double fmax, double *tau, double *weight) {
+  double taumin = 1.0 / (2.0 * PI_WP * fmax), taumax = 1.0 / (2.0 * PI_WP * fmin);
+  for (int k = 1; k <= 4; ++k) tau[k - 1] = exp(log(taumin) + (2.0 * k - 1.0) / (2.0 * 4) * log(taumax / taumin));
+  static const double w[4] = {1.549360, 0.804277, 0.887718, 1.464160};
+  memcpy(weight, w, sizeof(w));
+}
+void orc_q8_coefficients(double fmin, double fmax, double *tau, double *weight) {
+  double taumin = 1.0 / (2.0 * PI_WP * fmax), taumax = 1.0 / (2.0 * PI_WP * fmin);
+  for (int k = 1; k <= 8; ++k) tau[k - 1] = exp(log(taumin) + (2.0 * k - 1.0) / (2.0 * 8) * log(taumax / taumin));
+  static const double w[8] = {1.50589707, 0.0, 0.52793567, 0.53065494, 0.32862132, 0.64375916, 0.0, 1.32751442};
+  memcpy(weight, w, sizeof(w));
+}
+void orc_modulus_correction(int nmech, const double *tau, const double *weight, double fref, long n, double *lam,
+                            double *mu, const double *rho, const double *qsinv, const double *qpinv) {
+  double wref = 2.0 * PI_WP * fref;
+  for (long i = 0; i < n; ++i) {
+    double vS = 0.0, vP = 0.0;
+    for (int l = 0; l < nmech; ++l) {
+      double dS = ((wref * wref) * (tau[l] * tau[l]) + 1.0) * (1.0 / qsinv[i]);
+      double dP = ((wref * wref) * (tau[l] * tau[l]) + 1.0) * (1.0 / qpinv[i]);
+      vS = vS + weight[l] / dS;
+      vP = vP + weight[l] / dP;
+    }
+    double vs = sqrt(mu[i] / rho[i]);
+    double vp = sqrt((lam[i] + 2.0 * mu[i]) / rho[i]);
+    double muS = rho[i] * (vs * vs) / (1.0 - vS);
+    double muP = rho[i] * (vp * vp) / (1.0 - vP);
+    vs = sqrt(muS / rho[i]);
+    vp = sqrt(muP / rho[i]);
+    mu[i] = (vs * vs) * rho[i];
+    lam[i] = (vp * vp) * rho[i] - 2.0 * mu[i];
+  }
+}
+
+/* interface coupling: filled in by wql3d_oracle_iface.c */
+void orc_iface_couple(odom *D, int ib, double t, int stage) { (void)D; (void)ib; (void)t; (void)stage; }
