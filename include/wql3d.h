@@ -1,0 +1,182 @@
+/*
+ * wql3d.h -- C ABI of the B200-native WaveQLab3D per-step volume update.
+ *
+ * One library (libwql3d.so, sm_100a) advances one or two structured blocks of
+ * the elastic / anelastic wave equation with the 6th-order traditional SBP
+ * operator, SAT boundary and interface closures, compact ADE-PML, Q4 / Q8 /
+ * fQ8 memory variables, moment-tensor point sources and the
+ * Kennedy-Carpenter (5,4) low-storage Runge-Kutta scheme.
+ *
+ * The entry points are the seams of the reference Fortran driver
+ * (paths relative to the reference project root):
+ *   - domain stage ops   src/domain.f90:615-1017  (scale_rates, set_rates,
+ *                         enforce_bound_iface_conditions, update_fields)
+ *   - time step          src/time_step.f90:68-150 (time_step_RK)
+ *   - rk vector backend  src/rk_vector_cpu.f90:7-18, src/rk_vector_openacc.f90:8-75
+ *                         (scale_rate_array, update_state_array)
+ *   - RHS backend        src/traditional_cartesian_rhs_cpu.f90:8-15
+ *                         (try_traditional_cartesian_rhs)
+ *   - final diagnostics  src/domain.f90:505-613 (close_domain)
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative WQL3D_E* code and
+ *     never exits the process; wql3d_last_error() describes the last failure
+ *     of the calling thread.
+ *   - Host arrays are Fortran ordered (q/x fastest).  Each 3-D component
+ *     covers (1-host_nb : n+host_nb) per axis, so a Fortran array allocated by
+ *     allocate_array_body with ghost_nodes (nb = 3) is passed with host_nb = 3
+ *     and an interior-only array with host_nb = 0.  Components follow one
+ *     another (the 4th Fortran index is slowest).
+ *   - Field order is v_x, v_y, v_z, s_xx, s_yy, s_zz, s_xy, s_xz, s_yz
+ *     (src/JU_xJU_yJU_z6.f90:8-10).
+ *   - One domain owns one CUDA stream; calls on one domain are not
+ *     reentrant.  Domains are independent.
+ */
+#ifndef WQL3D_H
+#define WQL3D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WQL3D_ABI_VERSION 1
+
+/* status codes */
+#define WQL3D_OK 0
+#define WQL3D_EINVAL (-1)       /* bad argument or unsupported combination */
+#define WQL3D_ECUDA (-2)        /* CUDA runtime error */
+#define WQL3D_ENOMEM (-3)       /* device allocation failed */
+#define WQL3D_ENONFINITE (-4)   /* non-finite state detected (RUN-ELASTIC-001 family) */
+#define WQL3D_ESTATE (-5)       /* call out of order */
+
+/* mesh kinds (type_of_mesh) */
+#define WQL3D_MESH_CARTESIAN 0
+#define WQL3D_MESH_CURVILINEAR 1
+
+/* arithmetic */
+#define WQL3D_FP64 0
+#define WQL3D_FP32_COMPENSATED 1
+
+/* response */
+#define WQL3D_ELASTIC 0
+#define WQL3D_Q4 1
+#define WQL3D_Q8 2
+#define WQL3D_FQ8 3
+
+/* interface coupling (src/Interface_Condition.f90:348-378) */
+#define WQL3D_IFACE_LOCKED 0
+#define WQL3D_IFACE_SLIP_WEAKENING 1
+#define WQL3D_IFACE_LINEAR 2
+
+typedef struct wql3d_domain wql3d_domain;
+
+/* Per-block description, filled once from the resolved configuration
+   (src/block.f90:31-320 init_block). */
+typedef struct wql3d_block_desc {
+  int32_t nq, nr, ns;          /* grid points per axis */
+  int32_t mesh;                /* WQL3D_MESH_* */
+  int32_t f32_literal;         /* 1: SBP row-4 literal 0.013435342414630 in single precision
+                                  (reference built without -r8 / -fdefault-real-8) */
+  int32_t bc[6];               /* type_of_bc on faces Lx,Rx,Ly,Ry,Lz,Rz: 1 absorbing,
+                                  2 free surface, 3 clamped, 0 interface, -1 none */
+  int32_t pml[6];              /* PML slab per face (1..6 = Lx,Rx,Ly,Ry,Lz,Rz) */
+  int32_t npml;                /* PML thickness in points */
+  double aqrs[3], bqrs[3];     /* Cartesian block extents (mesh_source = 'compute') */
+  double tau0;                 /* SAT penalty, 1/0.315949074074074 for traditional-6 */
+  int32_t host_nb;             /* ghost width of the host arrays below */
+  const double *coords;        /* curvilinear: 3 components x, y, z; NULL for Cartesian */
+  const double *material;      /* 3 components lambda, mu, rho (already modulus-corrected) */
+  const double *qs_inv;        /* Q4/Q8: 1/Qs per point (NULL: use Qs0 below) */
+  const double *qp_inv;        /* Q4/Q8: 1/Qp per point */
+  /* moment-tensor sources, src/moment_tensor.f90:8-740 */
+  int32_t nsrc;
+  int32_t src_order;           /* 2: 5-point delta, 4: 9-point delta */
+  int32_t src_alpha;           /* 0, 25, 50 or 100 (order 4 weights) */
+  const int32_t *src_type;     /* per source: 0 gaussian, 1 LOH_discontinuity, 2 Brune, 3 Cos-Bell,
+                                  4 cosine, 5 LOH_moment_time_history, 6 sine_moment_time_history,
+                                  7 ricker (f0 = duration, delay = t_init) */
+  const double *src_par;       /* per source 11 values: duration t_init mxx myy mzz mxy mxz myz x y z */
+  /* receivers (stations), src/seismogram.f90:11-492 */
+  int32_t nrec;
+  const double *rec_xyz;       /* per receiver x y z; nearest node as Find_Coordinates */
+} wql3d_block_desc;
+
+/* Whole-run description (the &problem_list subset the hot path needs). */
+typedef struct wql3d_domain_desc {
+  int32_t abi_version;         /* WQL3D_ABI_VERSION */
+  int32_t nblocks;             /* 1 or 2 (two blocks share a q-direction interface) */
+  int32_t precision;           /* WQL3D_FP64 or WQL3D_FP32_COMPENSATED */
+  int32_t response;            /* WQL3D_ELASTIC / Q4 / Q8 / FQ8 */
+  int32_t coarse_grain;        /* fQ8: 1 when coarse_grain == 2 */
+  double Qs0, Qp0;             /* Q4/Q8 scalars when no per-point arrays are given */
+  double tau[8];               /* relaxation times */
+  double weight[8];            /* Q4/Q8 weights */
+  double strength_s[8];        /* fQ8 S strengths */
+  double strength_p[8];        /* fQ8 P strengths */
+  int32_t coupling;            /* WQL3D_IFACE_* (two blocks) */
+  int32_t serial_shared;       /* 1: interface slip rates accumulated once per block side,
+                                  like the reference's one-process two-block run */
+  double fs, fd, Dc;           /* slip-weakening parameters */
+  const double *iface_tau0;    /* optional (3, ns, nr): initial tractions n, m, l on the interface */
+  const double *iface_fs;      /* optional (ns, nr) static friction map */
+  int32_t max_samples;         /* receiver samples kept on the device */
+  wql3d_block_desc block[2];
+} wql3d_domain_desc;
+
+/* lifecycle (replaces init_domain's device side and enter_domain_device_data,
+   src/domain.f90:30-330, src/device_data_openacc.f90:37-87) */
+int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out);
+int wql3d_domain_destroy(wql3d_domain *d);
+
+/* explicit residency (src/device_data_openacc.f90): host <-> device copies */
+int wql3d_set_fields(wql3d_domain *d, int block, const double *F, int32_t host_nb);
+int wql3d_get_fields(wql3d_domain *d, int block, double *F, int32_t host_nb);
+int wql3d_set_rates(wql3d_domain *d, int block, const double *DF, int32_t host_nb);
+int wql3d_get_rates(wql3d_domain *d, int block, double *DF, int32_t host_nb);
+int wql3d_get_memory_variables(wql3d_domain *d, int block, double *eta);   /* 6 x nmech x n, host_nb 0 */
+int wql3d_get_metrics(wql3d_domain *d, int block, double *metrics);       /* 10 x n: metricx, metricy, metricz, J */
+int wql3d_get_interface(wql3d_domain *d, double *out);                    /* per point S(4) W Svel trup */
+
+/* time integration: one RK stage (time_step.f90:109-147 loop body),
+   one time step (time_step_RK) and a graph-captured run of many steps.
+   t is the domain time held on the device; wql3d_set_time sets it. */
+int wql3d_set_time(wql3d_domain *d, double t);
+int wql3d_get_time(wql3d_domain *d, double *t);
+int wql3d_stage(wql3d_domain *d, int stage, double dt);
+int wql3d_time_step(wql3d_domain *d, double dt, int n, int w_stride);
+int wql3d_run(wql3d_domain *d, double dt, int n_first, int nsteps, int w_stride);
+
+/* split stage operations (bring-up path, same arithmetic as wql3d_stage) */
+int wql3d_scale_rates(wql3d_domain *d, double A);                         /* domain.f90:922-949 */
+int wql3d_set_rates_rhs(wql3d_domain *d);                                 /* domain.f90:951-979 */
+int wql3d_enforce_bound_iface_conditions(wql3d_domain *d, int stage);     /* domain.f90:615-644 */
+int wql3d_update_fields(wql3d_domain *d, double dt);                      /* domain.f90:982-1017 */
+/* RHS backend seam: computes the traditional-6 RHS of every block into DF
+   and reports handled = 1 (traditional_cartesian_rhs_*.f90) */
+int wql3d_try_traditional_rhs(wql3d_domain *d, int *handled);
+
+/* rk_vector backend on raw device arrays (rk_vector_openacc.f90:22-75) */
+int wql3d_scale_rate_array(double *rate, int64_t n, double coefficient, void *stream);
+int wql3d_update_state_array(double *state, const double *rate, int64_t n, double increment, void *stream);
+
+/* receivers: samples taken at stage 1 before the update (time_step.f90:137),
+   out[(sample*nrec + r)*4 + {t, vx, vy, vz}] */
+int wql3d_get_seismograms(wql3d_domain *d, int block, double *out, int32_t *nsamples);
+int wql3d_receiver_index(wql3d_domain *d, int block, int32_t *idx);
+
+/* final diagnostics (close_domain): max|F| over all blocks, max|eta|,
+   per-block maxima; returns WQL3D_ENONFINITE for non-finite state */
+int wql3d_final_state(wql3d_domain *d, double *max_field, double *max_memory, double *block_max);
+
+int wql3d_synchronize(wql3d_domain *d);
+int wql3d_get_stream(wql3d_domain *d, void **stream);                    /* the domain's cudaStream_t */
+int wql3d_device_bytes(wql3d_domain *d, int64_t *bytes);
+int wql3d_kernel_launches(wql3d_domain *d, int64_t *launches);
+const char *wql3d_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WQL3D_H */

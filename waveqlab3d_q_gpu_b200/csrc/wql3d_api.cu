@@ -1,0 +1,1199 @@
+// C ABI of the B200-native WaveQLab3D per-step volume update (see include/wql3d.h).
+//
+// Host side: block setup (padded HBM layout, per-axis Cartesian metrics,
+// device-computed curvilinear metrics, face bases, PML slabs, memory
+// variables, source and receiver lookup), the RK stage sequence of
+// src/time_step.f90:68-150, CUDA-graph capture of the step loop, and the
+// host <-> device residency calls.
+#include "wql3d.h"
+#include "wql3d_device.cuh"
+#include "wql3d_iface.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace wql3d;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? WQL3D_ENOMEM : WQL3D_ECUDA,                   \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                            \
+  } while (0)
+
+const double kRkA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                        -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double kRkB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                        1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                        2277821191437.0 / 14882151754819.0};
+const double kRkC[6] = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                        2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0, 1.0};
+
+// SBP rows 1..6 of the traditional-6 first-derivative operator, in the
+// reference's summation order (src/JU_xJU_yJU_z6.f90:74-161, src/metrics.f90:29-86)
+const int kSbpCnt[6] = {6, 5, 5, 6, 7, 8};
+const int kSbpIdx[6][8] = {{6, 5, 4, 3, 2, 1, 0, 0}, {6, 5, 4, 3, 1, 0, 0, 0}, {6, 5, 4, 2, 1, 0, 0, 0},
+                           {7, 6, 5, 3, 2, 1, 0, 0}, {8, 7, 6, 4, 3, 2, 1, 0}, {9, 8, 7, 5, 4, 3, 2, 1}};
+double kSbpC[2][6][8];
+
+void sbp_tables() {
+  static bool done = false;
+  if (done) return;
+  const double rows[6][8] = {
+      {0.036577936277544, 0.104488069284042, -0.450398306578272, -0.141512858744873, 2.033378678700676, -1.582533518939116, 0, 0},
+      {-0.014903449191300, -0.069112065532624, 0.258816087376832, 0.287258622978251, -0.462059195631158, 0, 0, 0},
+      {-0.018129342917256, -0.022902190275815, 0.606235523609147, -0.636451095137907, 0.071247104721830, 0, 0, 0},
+      {0.013435342414630, -0.051642265516119, 0.520262285050482, -0.306681191361148, -0.290087484386815, 0.114713313798970, 0, 0},
+      {0.018281071473911, -0.164529643265203, 0.769199413962647, -0.707905442575989, 0.015764336127392, 0.105400944933782, -0.036210680656541, 0},
+      {0.016437980868017, -0.147941827812150, 0.739709139060752, -0.691649024426814, 0.063183694641876, 0.011220896474665, 0.020437334208704, -0.011398193015050}};
+  for (int lit = 0; lit < 2; ++lit)
+    for (int r = 0; r < 6; ++r)
+      for (int k = 0; k < 8; ++k) kSbpC[lit][r][k] = rows[r][k];
+  // row 4 coefficient of point 7 as a single-precision literal
+  kSbpC[1][3][0] = (double)0.013435342414630f;
+  done = true;
+}
+
+// host copy of the SBP stencil at 1-based i of an axis of n points
+void host_row(int i, int n, int lit, int &cnt, int idx[8], double c[8]) {
+  if (i >= 7 && i <= n - 6) {
+    const double cc[6] = {-1.0 / 60.0, 0.15, -0.75, 0.75, -0.15, 1.0 / 60.0};
+    const int off[6] = {-3, -2, -1, 1, 2, 3};
+    cnt = 6;
+    for (int k = 0; k < 6; ++k) { idx[k] = i + off[k]; c[k] = cc[k]; }
+    return;
+  }
+  if (i >= n - 5) {
+    int r = n - i;
+    cnt = kSbpCnt[r];
+    for (int k = 0; k < cnt; ++k) { idx[k] = n + 1 - kSbpIdx[r][k]; c[k] = -kSbpC[lit][r][k]; }
+    return;
+  }
+  int r = i - 1;
+  cnt = kSbpCnt[r];
+  for (int k = 0; k < cnt; ++k) { idx[k] = kSbpIdx[r][k]; c[k] = kSbpC[lit][r][k]; }
+}
+
+struct Alloc {
+  std::vector<void *> ptrs;
+  int64_t bytes = 0;
+  template <typename P>
+  cudaError_t get(P **p, size_t n, bool zero = true) {
+    void *v = nullptr;
+    size_t nb = n * sizeof(P);
+    if (nb == 0) nb = 16;
+    cudaError_t e = cudaMalloc(&v, nb);
+    if (e != cudaSuccess) return e;
+    if (zero) cudaMemset(v, 0, nb);
+    ptrs.push_back(v);
+    bytes += (int64_t)nb;
+    *p = (P *)v;
+    return cudaSuccess;
+  }
+  void release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+}  // namespace
+
+struct HostBlock {
+  int nq = 0, nr = 0, ns = 0;
+  int mesh = 0;
+  int PX = 0, PY = 0, PZ = 0;   // padded extents
+  int XOFF = 4;
+  long long vol = 0;
+  std::vector<double> coords;   // 3 * nq*nr*ns (host copy for source / receiver lookup)
+  std::vector<int> ridx;
+  int nrec = 0;
+  int nsrc = 0;
+  int iface_side[2] = {0, 0};
+};
+
+struct wql3d_domain {
+  wql3d_domain_desc desc;
+  int nblocks = 0;
+  int fp32 = 0;
+  int response = 0;
+  int nmech = 0;
+  cudaStream_t stream = nullptr;
+  Alloc mem;
+  HostBlock hb[2];
+  Blk<double> bd[2];
+  Blk<float> bf[2];
+  int cur = 0;
+  DevTime *time = nullptr;
+  // interface
+  bool has_iface = false;
+  IfaceDev iface;
+  // graph cache
+  cudaGraphExec_t graph = nullptr;
+  double g_dt = 0.0;
+  int g_w = -1, g_cur = -1;
+  int64_t launches = 0;
+  double *red = nullptr;
+  int *flag = nullptr;
+};
+
+namespace {
+
+template <typename T>
+Blk<T> &blk(wql3d_domain *d, int i);
+template <>
+Blk<double> &blk<double>(wql3d_domain *d, int i) { return d->bd[i]; }
+template <>
+Blk<float> &blk<float>(wql3d_domain *d, int i) { return d->bf[i]; }
+
+int upload_constants() {
+  sbp_tables();
+  int cnt[6], idx[6][8];
+  for (int r = 0; r < 6; ++r) {
+    cnt[r] = kSbpCnt[r];
+    for (int k = 0; k < 8; ++k) idx[r][k] = kSbpIdx[r][k];
+  }
+  CK(cudaMemcpyToSymbol(c_sbp_cnt, cnt, sizeof(cnt)));
+  CK(cudaMemcpyToSymbol(c_sbp_idx, idx, sizeof(idx)));
+  // c_sbp_c[0] = double literal, [1] = single literal
+  CK(cudaMemcpyToSymbol(c_sbp_c, kSbpC, sizeof(kSbpC)));
+  CK(cudaMemcpyToSymbol(c_rkA, kRkA, sizeof(kRkA)));
+  CK(cudaMemcpyToSymbol(c_rkB, kRkB, sizeof(kRkB)));
+  CK(cudaMemcpyToSymbol(c_rkC, kRkC, sizeof(kRkC)));
+  return WQL3D_OK;
+}
+
+// copy one padded device component <-> host component with ghost width hnb
+int copy_component(wql3d_domain *d, const HostBlock &h, void *dev, size_t esz, void *host, int hnb, bool to_dev) {
+  cudaMemcpy3DParms p;
+  memset(&p, 0, sizeof(p));
+  cudaPitchedPtr hp = make_cudaPitchedPtr(host, (size_t)(h.nq + 2 * hnb) * esz, h.nq + 2 * hnb, h.nr + 2 * hnb);
+  cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)h.PX * esz, h.PX, h.PY);
+  cudaPos hpos = make_cudaPos((size_t)hnb * esz, hnb, hnb);
+  cudaPos dpos = make_cudaPos((size_t)h.XOFF * esz, NB, NB);
+  if (to_dev) { p.srcPtr = hp; p.srcPos = hpos; p.dstPtr = dp; p.dstPos = dpos; p.kind = cudaMemcpyHostToDevice; }
+  else { p.srcPtr = dp; p.srcPos = dpos; p.dstPtr = hp; p.dstPos = hpos; p.kind = cudaMemcpyDeviceToHost; }
+  p.extent = make_cudaExtent((size_t)h.nq * esz, h.nr, h.ns);
+  CK(cudaMemcpy3DAsync(&p, d->stream));
+  return WQL3D_OK;
+}
+
+// double host data -> device storage type (FP32 path converts on the host)
+template <typename T>
+int put_array(wql3d_domain *d, const HostBlock &h, T *dev, int ncomp, const double *host, int hnb) {
+  long long hn = (long long)(h.nq + 2 * hnb) * (h.nr + 2 * hnb) * (h.ns + 2 * hnb);
+  for (int c = 0; c < ncomp; ++c) {
+    const double *src = host + (long long)c * hn;
+    if (sizeof(T) == sizeof(double)) {
+      int rc = copy_component(d, h, (void *)(dev + (long long)c * h.vol), sizeof(double), (void *)src, hnb, true);
+      if (rc) return rc;
+    } else {
+      std::vector<T> tmp((size_t)hn);
+      for (long long i = 0; i < hn; ++i) tmp[(size_t)i] = (T)src[i];
+      int rc = copy_component(d, h, (void *)(dev + (long long)c * h.vol), sizeof(T), tmp.data(), hnb, true);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(d->stream));
+    }
+  }
+  return WQL3D_OK;
+}
+
+template <typename T>
+int get_array(wql3d_domain *d, const HostBlock &h, const T *dev, int ncomp, double *host, int hnb) {
+  long long hn = (long long)(h.nq + 2 * hnb) * (h.nr + 2 * hnb) * (h.ns + 2 * hnb);
+  for (int c = 0; c < ncomp; ++c) {
+    double *dst = host + (long long)c * hn;
+    if (sizeof(T) == sizeof(double)) {
+      int rc = copy_component(d, h, (void *)(dev + (long long)c * h.vol), sizeof(double), (void *)dst, hnb, false);
+      if (rc) return rc;
+    } else {
+      std::vector<T> tmp((size_t)hn, (T)0);
+      int rc = copy_component(d, h, (void *)(dev + (long long)c * h.vol), sizeof(T), tmp.data(), hnb, false);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(d->stream));
+      for (long long i = 0; i < hn; ++i) dst[i] = (double)tmp[(size_t)i];
+    }
+  }
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+// curvilinear metrics from coordinates: src/grid.f90:398-471 with the SBP
+// operator of src/metrics.f90:16-491 (setup-time kernel)
+template <typename T>
+__global__ void k_metrics(Blk<T> b, const double *X, double *met, double *Jout) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int s = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (q > b.nx || r > b.ny || s > b.nz) return;
+  const long long p = pidx(b, q, r, s);
+  const long long V = b.vol;
+  const int pos[3] = {q, r, s};
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  const long long st[3] = {1, b.sy, b.sz};
+  double D[3][3];  // D[axis][comp]
+  for (int a = 0; a < 3; ++a) {
+    Row row;
+    sbp_row(pos[a], nn[a], b.lit, row);
+    double h = 1.0 / (double)(nn[a] - 1);
+    for (int c = 0; c < 3; ++c) {
+      double sum = 0.0;
+      for (int k = 0; k < row.cnt; ++k) sum = __dadd_rn(sum, __dmul_rn(row.c[k], X[c * V + p + row.off[k] * st[a]]));
+      D[a][c] = __dmul_rn(1.0 / h, sum);
+    }
+  }
+  const double *Xq = D[0], *Xr = D[1], *Xs = D[2];
+  double J = __dadd_rn(__dsub_rn(__dmul_rn(Xq[0], __dsub_rn(__dmul_rn(Xr[1], Xs[2]), __dmul_rn(Xr[2], Xs[1]))),
+                                 __dmul_rn(Xq[1], __dsub_rn(__dmul_rn(Xr[0], Xs[2]), __dmul_rn(Xr[2], Xs[0])))),
+                       __dmul_rn(Xq[2], __dsub_rn(__dmul_rn(Xr[0], Xs[1]), __dmul_rn(Xr[1], Xs[0]))));
+  double iJ = 1.0 / J;
+  double m[9];
+  m[0] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xr[1], Xs[2]), __dmul_rn(Xr[2], Xs[1])));
+  m[1] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xq[2], Xs[1]), __dmul_rn(Xq[1], Xs[2])));
+  m[2] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xq[1], Xr[2]), __dmul_rn(Xq[2], Xr[1])));
+  m[3] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xr[2], Xs[0]), __dmul_rn(Xr[0], Xs[2])));
+  m[4] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xq[0], Xs[2]), __dmul_rn(Xq[2], Xs[0])));
+  m[5] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xq[2], Xr[0]), __dmul_rn(Xq[0], Xr[2])));
+  m[6] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xr[0], Xs[1]), __dmul_rn(Xr[1], Xs[0])));
+  m[7] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xq[1], Xs[0]), __dmul_rn(Xq[0], Xs[1])));
+  m[8] = __dmul_rn(iJ, __dsub_rn(__dmul_rn(Xq[0], Xr[1]), __dmul_rn(Xq[1], Xr[0])));
+  for (int k = 0; k < 9; ++k) met[k * V + p] = m[k];
+  Jout[p] = J;
+}
+
+template <typename T>
+__global__ void k_convert(const double *src, T *dst, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long s = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += s) dst[i] = (T)src[i];
+}
+
+// unit_normals.f90 face bases from the metric of the face (host)
+void gen_orth(double l[3], double m[3], const double n[3]) {
+  const double tol = 1.0e-12;
+  m[0] = 0.0; m[1] = 1.0; m[2] = 0.0;
+  double d1 = sqrt((n[0] - m[0]) * (n[0] - m[0]) + (n[1] - m[1]) * (n[1] - m[1]) + (n[2] - m[2]) * (n[2] - m[2]));
+  double d2 = sqrt((n[0] + m[0]) * (n[0] + m[0]) + (n[1] + m[1]) * (n[1] + m[1]) + (n[2] + m[2]) * (n[2] + m[2]));
+  if (!(d1 >= tol && d2 >= tol)) { m[0] = 0.0; m[1] = 0.0; m[2] = 1.0; }
+  double a = n[0] * m[0] + n[1] * m[1] + n[2] * m[2];
+  for (int i = 0; i < 3; ++i) m[i] = m[i] - a * n[i];
+  double s = 1.0 / sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  for (int i = 0; i < 3; ++i) m[i] = s * m[i];
+  l[0] = n[1] * m[2] - n[2] * m[1];
+  l[1] = n[2] * m[0] - n[0] * m[2];
+  l[2] = n[0] * m[1] - n[1] * m[0];
+}
+
+void nearest_moment(const HostBlock &h, double x1, double y1, double z1, int out[3]) {
+  long long n1 = (long long)h.nq * h.nr * h.ns;
+  const double *X = h.coords.data();
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (long long i = 0; i < n1; ++i)
+    for (int c = 0; c < 3; ++c) {
+      double v = X[c * n1 + i];
+      if (v < mn[c]) mn[c] = v;
+      if (v > mx[c]) mx[c] = v;
+    }
+  double scale = 1.0;
+  for (int c = 0; c < 3; ++c) scale = fmax(scale, fmax(fabs(mn[c]), fabs(mx[c])));
+  double tol = 1000.0 * 2.220446049250313e-16 * scale;
+  out[0] = out[1] = out[2] = -9999;
+  if (!((mn[0] - tol <= x1 && x1 <= mx[0] + tol) && (mn[1] - tol <= y1 && y1 <= mx[1] + tol) &&
+        (mn[2] - tol <= z1 && z1 <= mx[2] + tol)))
+    return;
+  double best = 1.0e8;
+  for (int z = 1; z <= h.ns; ++z)
+    for (int y = 1; y <= h.nr; ++y)
+      for (int x = 1; x <= h.nq; ++x) {
+        long long i = (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1));
+        double a = X[i] - x1, b = X[n1 + i] - y1, c = X[2 * n1 + i] - z1;
+        double dist = sqrt(a * a + b * b + c * c);
+        if (dist <= best) { out[0] = x; out[1] = y; out[2] = z; best = dist; }
+      }
+}
+
+// Find_Coordinates, src/seismogram.f90:767-876
+void nearest_receiver(const HostBlock &h, double x1, double y1, double z1, int out[3]) {
+  long long n1 = (long long)h.nq * h.nr * h.ns;
+  const double *X = h.coords.data();
+  auto at = [&](int c, int x, int y, int z) { return X[c * n1 + (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1))]; };
+  out[0] = out[1] = out[2] = -9999;
+  double best = 1.0e8;
+  int px = h.nq, py = h.nr, pz = h.ns;
+  for (int k = 1; k <= pz; ++k)
+    for (int j = 1; j <= py; ++j)
+      for (int i = 1; i <= px; ++i) {
+        double hx = at(0, px, j, k) - at(0, px - 1, j, k);
+        double hy = at(1, i, py, k) - at(1, i, py - 1, k);
+        double hz = at(2, i, j, pz) - at(2, i, j, pz - 1);
+        if (i < px) hx = at(0, i + 1, j, k) - at(0, i, j, k);
+        if (j < py) hy = at(1, i, j + 1, k) - at(1, i, j, k);
+        if (k < pz) hz = at(2, i, j, k + 1) - at(2, i, j, k);
+        double a = at(0, i, j, k) - x1, b = at(1, i, j, k) - y1, c = at(2, i, j, k) - z1;
+        double dist = sqrt(a * a + b * b + c * c);
+        double dist0 = sqrt(hx * hx + hy * hy + hz * hz);
+        if (dist <= best && dist <= 0.5 * dist0) { out[0] = i; out[1] = j; out[2] = k; best = dist; }
+      }
+}
+
+template <typename T>
+int setup_block(wql3d_domain *d, int bi) {
+  const wql3d_block_desc &bd = d->desc.block[bi];
+  HostBlock &h = d->hb[bi];
+  Blk<T> &b = blk<T>(d, bi);
+  memset(&b, 0, sizeof(b));
+  if (bd.nq < 13 || bd.nr < 13 || bd.ns < 13) return fail(WQL3D_EINVAL, "each axis needs at least 13 points for the traditional-6 operator");
+  if (bd.mesh != WQL3D_MESH_CARTESIAN && bd.mesh != WQL3D_MESH_CURVILINEAR) return fail(WQL3D_EINVAL, "unknown mesh kind");
+  if (bd.mesh == WQL3D_MESH_CURVILINEAR && !bd.coords) return fail(WQL3D_EINVAL, "curvilinear block needs coordinates");
+  if (!bd.material) return fail(WQL3D_EINVAL, "block material (lambda, mu, rho) is required");
+  h.nq = bd.nq; h.nr = bd.nr; h.ns = bd.ns;
+  h.mesh = bd.mesh;
+  const int esz = (int)sizeof(T);
+  h.XOFF = 32 / esz;  // first interior point of a row on a 32-byte boundary
+  int row_elems = 128 / esz;
+  h.PX = ((h.XOFF + h.nq + NB + row_elems - 1) / row_elems) * row_elems;
+  h.PY = h.nr + 2 * NB;
+  h.PZ = h.ns + 2 * NB;
+  long long vol = (long long)h.PX * h.PY * h.PZ;
+  vol = (vol + 63) / 64 * 64;
+  h.vol = vol;
+  b.nx = h.nq; b.ny = h.nr; b.nz = h.ns;
+  b.sy = h.PX;
+  b.sz = (long long)h.PX * h.PY;
+  b.o1 = h.XOFF + b.sy * NB + b.sz * NB;
+  b.vol = vol;
+  b.lit = bd.f32_literal ? 1 : 0;
+  b.hq = (T)(1.0 / (double)(h.nq - 1));
+  b.hr = (T)(1.0 / (double)(h.nr - 1));
+  b.hs = (T)(1.0 / (double)(h.ns - 1));
+  b.ihq = (T)(1.0 / (1.0 / (double)(h.nq - 1)));
+  b.ihr = (T)(1.0 / (1.0 / (double)(h.nr - 1)));
+  b.ihs = (T)(1.0 / (1.0 / (double)(h.ns - 1)));
+  const double cc[3] = {0.75, -0.15, 1.0 / 60.0};
+  for (int s = 0; s < 3; ++s) {
+    b.cx[s] = (T)(cc[s] / (1.0 / (double)(h.nq - 1)));
+    b.cy[s] = (T)(cc[s] / (1.0 / (double)(h.nr - 1)));
+    b.cz[s] = (T)(cc[s] / (1.0 / (double)(h.ns - 1)));
+  }
+  b.tau0 = (T)bd.tau0;
+  for (int f = 0; f < 6; ++f) b.bc[f] = bd.bc[f];
+  // strict interior bounds, src/JU_xJU_yJU_z6.f90:16158-16173
+  int np = bd.npml;
+  int ix = bd.pml[0] ? std::max(np, 6) : 6, fx = bd.pml[1] ? std::max(np, 6) : 6;
+  int iy = bd.pml[2] ? std::max(np, 6) : 6, fy = bd.pml[3] ? std::max(np, 6) : 6;
+  int iz = bd.pml[4] ? std::max(np, 6) : 6, fz = bd.pml[5] ? std::max(np, 6) : 6;
+  b.lo[0] = ix + 1; b.hi[0] = h.nq - fx;
+  b.lo[1] = iy + 1; b.hi[1] = h.nr - fy;
+  b.lo[2] = iz + 1; b.hi[2] = h.ns - fz;
+
+  Alloc &M = d->mem;
+  CK(M.get(&b.F0, 9 * vol));
+  CK(M.get(&b.F1, 9 * vol));
+  CK(M.get(&b.DF, 9 * vol));
+  CK(M.get(&b.M, 3 * vol));
+  if (d->fp32) CK(M.get(&b.FC, 9 * vol));
+  {
+    // rates start at the reference's 1e40 sentinel (src/fields.f90:39) in FP64;
+    // the first stage scales them by A(1) = 0.  FP32 cannot hold 1e40: zero.
+    std::vector<T> init((size_t)9 * vol, (T)0);
+    if (!d->fp32) {
+      for (int c = 0; c < 9; ++c)
+        for (int z = 1; z <= h.ns; ++z)
+          for (int y = 1; y <= h.nr; ++y)
+            for (int x = 1; x <= h.nq; ++x)
+              init[(size_t)(c * vol + b.o1 + (x - 1) + b.sy * (y - 1) + b.sz * (z - 1))] = (T)1.0e40;
+    }
+    CK(cudaMemcpyAsync(b.DF, init.data(), sizeof(T) * 9 * vol, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  int rc = put_array<T>(d, h, b.M, 3, bd.material, bd.host_nb);
+  if (rc) return rc;
+
+  // coordinates (host copy for lookups)
+  long long n1 = (long long)h.nq * h.nr * h.ns;
+  h.coords.assign((size_t)(3 * n1), 0.0);
+  if (bd.mesh == WQL3D_MESH_CARTESIAN) {
+    double bh[3];
+    int nn[3] = {h.nq, h.nr, h.ns};
+    for (int c = 0; c < 3; ++c) bh[c] = (bd.bqrs[c] - bd.aqrs[c]) / (double)(nn[c] - 1);
+    for (int z = 1; z <= h.ns; ++z)
+      for (int y = 1; y <= h.nr; ++y)
+        for (int x = 1; x <= h.nq; ++x) {
+          long long i = (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1));
+          h.coords[i] = bd.aqrs[0] + (double)(x - 1) * bh[0];
+          h.coords[n1 + i] = bd.aqrs[1] + (double)(y - 1) * bh[1];
+          h.coords[2 * n1 + i] = bd.aqrs[2] + (double)(z - 1) * bh[2];
+        }
+    // per-axis metric of the separable Cartesian mesh: 1 / (D6 x)(i), with
+    // the SBP operator applied to the coordinate line exactly as
+    // src/grid.f90:398-471 does (row-4 literal included)
+    for (int a = 0; a < 3; ++a) {
+      std::vector<T> m((size_t)nn[a] + 1, (T)0);
+      double hh = 1.0 / (double)(nn[a] - 1);
+      for (int i = 1; i <= nn[a]; ++i) {
+        int cnt, idx[8];
+        double c[8];
+        host_row(i, nn[a], b.lit, cnt, idx, c);
+        double s = 0.0;
+        for (int k = 0; k < cnt; ++k) s = s + c[k] * (bd.aqrs[a] + (double)(idx[k] - 1) * bh[a]);
+        double Xa = (1.0 / hh) * s;
+        m[(size_t)i] = (T)(1.0 / Xa);
+      }
+      T *dm;
+      CK(M.get(&dm, m.size()));
+      CK(cudaMemcpyAsync(dm, m.data(), sizeof(T) * m.size(), cudaMemcpyHostToDevice, d->stream));
+      if (a == 0) b.mq = dm; else if (a == 1) b.mr = dm; else b.ms = dm;
+    }
+  } else {
+    long long hn = (long long)(h.nq + 2 * bd.host_nb) * (h.nr + 2 * bd.host_nb) * (h.ns + 2 * bd.host_nb);
+    for (int c = 0; c < 3; ++c)
+      for (int z = 1; z <= h.ns; ++z)
+        for (int y = 1; y <= h.nr; ++y)
+          for (int x = 1; x <= h.nq; ++x) {
+            int H = bd.host_nb;
+            long long hi = (x - 1 + H) + (long long)(h.nq + 2 * H) * ((y - 1 + H) + (long long)(h.nr + 2 * H) * (z - 1 + H));
+            h.coords[c * n1 + (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1))] = bd.coords[c * hn + hi];
+          }
+  }
+  {
+    // full metric and Jacobian of both mesh kinds from the coordinates
+    // (the near-boundary operator and the face SATs use all nine entries)
+    double *Xd, *metd, *Jd;
+    CK(M.get(&Xd, 3 * vol));
+    CK(M.get(&metd, 9 * vol));
+    CK(M.get(&Jd, vol));
+    rc = put_array<double>(d, h, Xd, 3, h.coords.data(), 0);
+    if (rc) return rc;
+    dim3 th(32, 4, 2), gr((h.nq + 31) / 32, (h.nr + 3) / 4, (h.ns + 1) / 2);
+    k_metrics<T><<<gr, th, 0, d->stream>>>(b, Xd, metd, Jd);
+    CK(cudaGetLastError());
+    if (sizeof(T) == sizeof(double)) {
+      b.met = (const T *)metd;
+      b.J = (const T *)Jd;
+    } else {
+      T *mt, *jt;
+      CK(M.get(&mt, 9 * vol));
+      CK(M.get(&jt, vol));
+      k_convert<T><<<1024, 256, 0, d->stream>>>(metd, mt, 9 * vol);
+      k_convert<T><<<1024, 256, 0, d->stream>>>(Jd, jt, vol);
+      b.met = mt;
+      b.J = jt;
+    }
+    // face bases from the device metrics (src/unit_normals.f90:8-160)
+    std::vector<double> met9((size_t)9 * vol);
+    CK(cudaMemcpyAsync(met9.data(), metd, sizeof(double) * 9 * vol, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    for (int f = 0; f < 6; ++f) {
+      int axis = f / 2;
+      int d0 = axis == 0 ? h.nr : h.nq, d1 = axis == 2 ? h.nr : h.ns;
+      long long fn = (long long)d0 * d1;
+      std::vector<T> basis((size_t)(9 * fn));
+      int fixed = (f % 2 == 0) ? 1 : (axis == 0 ? h.nq : axis == 1 ? h.nr : h.ns);
+      for (int c2 = 1; c2 <= d1; ++c2)
+        for (int c1 = 1; c1 <= d0; ++c1) {
+          int x, y, z;
+          if (axis == 0) { x = fixed; y = c1; z = c2; }
+          else if (axis == 1) { x = c1; y = fixed; z = c2; }
+          else { x = c1; y = c2; z = fixed; }
+          long long p = b.o1 + (x - 1) + b.sy * (y - 1) + b.sz * (z - 1);
+          double qx = met9[(size_t)((0 + axis) * vol + p)], qy = met9[(size_t)((3 + axis) * vol + p)],
+                 qz = met9[(size_t)((6 + axis) * vol + p)];
+          double norm = sqrt(qx * qx + qy * qy + qz * qz);
+          double n3[3] = {qx / norm, qy / norm, qz / norm}, l3[3], m3[3];
+          gen_orth(l3, m3, n3);
+          long long fp = (c1 - 1) + (long long)d0 * (c2 - 1);
+          for (int c = 0; c < 3; ++c) {
+            basis[(size_t)((0 + c) * fn + fp)] = (T)l3[c];
+            basis[(size_t)((3 + c) * fn + fp)] = (T)m3[c];
+            basis[(size_t)((6 + c) * fn + fp)] = (T)n3[c];
+          }
+        }
+      T *dbase;
+      CK(M.get(&dbase, basis.size()));
+      CK(cudaMemcpyAsync(dbase, basis.data(), sizeof(T) * basis.size(), cudaMemcpyHostToDevice, d->stream));
+      CK(cudaStreamSynchronize(d->stream));
+      b.nrm[f] = dbase;
+    }
+  }
+
+  // PML slabs, src/pml.f90:11-168
+  b.npml = np;
+  b.d0 = (T)(6.0 / (2.0 * 1.0) * log(1.0 / 1.0e-3));
+  for (int f = 0; f < 6; ++f) {
+    b.pml_on[f] = (bd.pml[f] && np > 0) ? 1 : 0;
+    int *B = b.pb[f];
+    B[0] = 1; B[1] = h.nq; B[2] = 1; B[3] = h.nr; B[4] = 1; B[5] = h.ns;
+    if (!b.pml_on[f]) continue;
+    switch (f) {
+      case 0: B[1] = np; break;
+      case 1: B[0] = h.nq - np + 1; break;
+      case 2: B[3] = np; break;
+      case 3: B[2] = h.nr - np + 1; break;
+      case 4: B[5] = np; break;
+      default: B[4] = h.ns - np + 1; break;
+    }
+    long long pv = (long long)(B[1] - B[0] + 1) * (B[3] - B[2] + 1) * (B[5] - B[4] + 1);
+    b.pvol[f] = pv;
+    CK(M.get(&b.Q[f], 9 * pv));
+    CK(M.get(&b.DQ[f], 9 * pv));
+    std::vector<T> init((size_t)(9 * pv), d->fp32 ? (T)0 : (T)1.0e40);  // DQ = 1e40, src/pml.f90
+    CK(cudaMemcpyAsync(b.DQ[f], init.data(), sizeof(T) * init.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+
+  // anelastic memory variables
+  b.nmech = d->nmech;
+  if (d->nmech) {
+    CK(M.get(&b.eta, (size_t)6 * d->nmech * vol));
+    CK(M.get(&b.deta, (size_t)6 * d->nmech * vol));
+    for (int i = 0; i < 8; ++i) {
+      b.tau[i] = (T)d->desc.tau[i];
+      b.w[i] = (T)d->desc.weight[i];
+      b.ss[i] = (T)d->desc.strength_s[i];
+      b.ps[i] = (T)d->desc.strength_p[i];
+    }
+    b.coarse = d->desc.coarse_grain;
+    if (d->response != WQL3D_FQ8) {
+      T *qs, *qp;
+      CK(M.get(&qs, vol));
+      CK(M.get(&qp, vol));
+      std::vector<double> tmp;
+      const double *qsh = bd.qs_inv, *qph = bd.qp_inv;
+      int hnb = bd.host_nb;
+      long long hn = (long long)(h.nq + 2 * hnb) * (h.nr + 2 * hnb) * (h.ns + 2 * hnb);
+      std::vector<double> cs, cp;
+      if (!qsh) { cs.assign((size_t)hn, 1.0 / d->desc.Qs0); qsh = cs.data(); }
+      if (!qph) { cp.assign((size_t)hn, 1.0 / d->desc.Qp0); qph = cp.data(); }
+      rc = put_array<T>(d, h, qs, 1, qsh, hnb);
+      if (rc) return rc;
+      rc = put_array<T>(d, h, qp, 1, qph, hnb);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(d->stream));
+      b.qs = qs;
+      b.qp = qp;
+    }
+  }
+
+  // sources: nearest node (Find_Coordinates_moment) and support box
+  h.nsrc = bd.nsrc;
+  b.nsrc = bd.nsrc;
+  b.src_order = bd.src_order;
+  b.src_alpha = bd.src_alpha;
+  b.src_half = bd.src_order == 4 ? 4 : 2;
+  b.sbox[0] = b.sbox[2] = b.sbox[4] = 1 << 30;
+  b.sbox[1] = b.sbox[3] = b.sbox[5] = -(1 << 30);
+  if (bd.nsrc > 0) {
+    if (!bd.src_type || !bd.src_par) return fail(WQL3D_EINVAL, "sources need src_type and src_par");
+    std::vector<DevSource> ss((size_t)bd.nsrc);
+    for (int i = 0; i < bd.nsrc; ++i) {
+      DevSource &s = ss[(size_t)i];
+      s.type = bd.src_type[i];
+      for (int k = 0; k < 11; ++k) s.par[k] = bd.src_par[11 * i + k];
+      nearest_moment(h, s.par[8], s.par[9], s.par[10], s.near);
+      if (s.near[0] > 0) {
+        long long ii = (s.near[0] - 1) + (long long)h.nq * ((s.near[1] - 1) + (long long)h.nr * (s.near[2] - 1));
+        for (int c = 0; c < 3; ++c) s.phys[c] = h.coords[(size_t)(c * n1 + ii)];
+        for (int c = 0; c < 3; ++c) {
+          b.sbox[2 * c] = std::min(b.sbox[2 * c], s.near[c] - b.src_half);
+          b.sbox[2 * c + 1] = std::max(b.sbox[2 * c + 1], s.near[c] + b.src_half);
+        }
+      } else {
+        for (int c = 0; c < 3; ++c) s.phys[c] = -1.0;
+      }
+    }
+    DevSource *ds;
+    CK(M.get(&ds, ss.size()));
+    CK(cudaMemcpyAsync(ds, ss.data(), sizeof(DevSource) * ss.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    b.src = ds;
+  }
+  // receivers (Find_Coordinates)
+  h.nrec = bd.nrec;
+  b.nrec = bd.nrec;
+  b.max_samples = d->desc.max_samples;
+  if (bd.nrec > 0) {
+    h.ridx.assign((size_t)3 * bd.nrec, -9999);
+    for (int r = 0; r < bd.nrec; ++r)
+      nearest_receiver(h, bd.rec_xyz[3 * r], bd.rec_xyz[3 * r + 1], bd.rec_xyz[3 * r + 2], &h.ridx[(size_t)3 * r]);
+    int *ri;
+    CK(M.get(&ri, h.ridx.size()));
+    CK(cudaMemcpyAsync(ri, h.ridx.data(), sizeof(int) * h.ridx.size(), cudaMemcpyHostToDevice, d->stream));
+    b.ridx = ri;
+    CK(M.get(&b.seis, (size_t)std::max(1, b.max_samples) * bd.nrec * 4));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  return WQL3D_OK;
+}
+
+template <typename T>
+void launch_stage(wql3d_domain *d, int bi, const StageArgs &a) {
+  Blk<T> &b = blk<T>(d, bi);
+  dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
+  int mesh = d->hb[bi].mesh;
+  switch (d->response * 2 + mesh) {
+    case 0: k_stage<T, MESH_CART, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 1: k_stage<T, MESH_CURV, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 2: k_stage<T, MESH_CART, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 3: k_stage<T, MESH_CURV, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 4: k_stage<T, MESH_CART, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 5: k_stage<T, MESH_CURV, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 6: k_stage<T, MESH_CART, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
+    default: k_stage<T, MESH_CURV, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
+  }
+  d->launches++;
+}
+
+template <typename T>
+int enqueue_stage(wql3d_domain *d, int stage, double dt, int flags) {
+  StageArgs a;
+  a.cur = d->cur;
+  a.flags = flags;
+  a.stage = stage;
+  a.A = kRkA[stage - 1];
+  a.Bdt = kRkB[stage - 1] * dt;
+  a.dt = dt;
+  a.time = d->time;
+  if (d->has_iface && (flags & F_ISAT)) {
+    launch_iface<T>(d->iface, blk<T>(d, 0), blk<T>(d, 1), a, d->stream);
+    d->launches++;
+  }
+  for (int i = 0; i < d->nblocks; ++i) launch_stage<T>(d, i, a);
+  if (flags & F_UPDATE) {
+    if (d->has_iface) {
+      launch_iface_update<T>(d->iface, a, d->stream);
+      d->launches++;
+    }
+    d->cur ^= 1;
+  }
+  return WQL3D_OK;
+}
+
+template <typename T>
+int enqueue_sample(wql3d_domain *d, int w_stride) {
+  int last = -1;
+  for (int i = 0; i < d->nblocks; ++i)
+    if (d->hb[i].nrec > 0) last = i;
+  for (int i = 0; i < d->nblocks; ++i) {
+    if (d->hb[i].nrec <= 0) continue;
+    k_sample<T><<<1, 256, 0, d->stream>>>(blk<T>(d, i), d->cur, d->time, w_stride, i == last ? 1 : 0);
+    d->launches++;
+  }
+  return WQL3D_OK;
+}
+
+template <typename T>
+int enqueue_step(wql3d_domain *d, double dt, int w_stride) {
+  enqueue_sample<T>(d, w_stride);
+  for (int s = 1; s <= 5; ++s) {
+    int rc = enqueue_stage<T>(d, s, dt, F_ALL);
+    if (rc) return rc;
+  }
+  k_advance<<<1, 32, 0, d->stream>>>(d->time, dt);
+  d->launches++;
+  return WQL3D_OK;
+}
+
+template <typename T>
+int run_steps(wql3d_domain *d, double dt, int nsteps, int w_stride) {
+  // CUDA graph of two steps (five stages each, so the field-buffer parity
+  // returns to its start) replayed nsteps/2 times
+  int pairs = nsteps / 2;
+  if (pairs > 0) {
+    if (!d->graph || d->g_dt != dt || d->g_w != w_stride || d->g_cur != d->cur) {
+      if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+      int cur0 = d->cur;
+      int64_t l0 = d->launches;
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_step<T>(d, dt, w_stride);
+      enqueue_step<T>(d, dt, w_stride);
+      CK(cudaStreamEndCapture(d->stream, &g));
+      CK(cudaGraphInstantiate(&d->graph, g, 0));
+      cudaGraphDestroy(g);
+      d->cur = cur0;
+      d->g_dt = dt;
+      d->g_w = w_stride;
+      d->g_cur = cur0;
+      d->launches = l0;
+    }
+    // launches per replay: count by re-enqueue size
+    int64_t per_pair = 0;
+    {
+      int64_t l0 = d->launches;
+      int cur0 = d->cur;
+      // counting pass without launching: mirror enqueue_step's structure
+      for (int k = 0; k < 2; ++k) {
+        for (int i = 0; i < d->nblocks; ++i) per_pair += d->hb[i].nrec > 0 ? 1 : 0;
+        per_pair += 5 * (d->nblocks + (d->has_iface ? 2 : 0)) + 1;
+      }
+      d->launches = l0;
+      d->cur = cur0;
+    }
+    for (int k = 0; k < pairs; ++k) {
+      CK(cudaGraphLaunch(d->graph, d->stream));
+      d->launches += per_pair;
+    }
+  }
+  if (nsteps % 2) {
+    int rc = enqueue_step<T>(d, dt, w_stride);
+    if (rc) return rc;
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+template <typename T>
+int final_state(wql3d_domain *d, double *maxF, double *maxEta, double *bmax) {
+  double mf = 0.0, me = 0.0;
+  int nonfinite = 0;
+  for (int i = 0; i < d->nblocks; ++i) {
+    Blk<T> &b = blk<T>(d, i);
+    const T *F = d->cur ? b.F1 : b.F0;
+    CK(cudaMemsetAsync(d->flag, 0, sizeof(int), d->stream));
+    k_maxabs<T><<<592, 256, 0, d->stream>>>(F, 9 * b.vol, d->red, d->flag);
+    d->launches++;
+    std::vector<double> part(592);
+    int fl = 0;
+    CK(cudaMemcpyAsync(part.data(), d->red, sizeof(double) * 592, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaMemcpyAsync(&fl, d->flag, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    double m = 0.0;
+    for (double v : part) m = std::max(m, v);
+    nonfinite |= fl;
+    if (bmax) bmax[i] = m;
+    mf = std::max(mf, m);
+    if (b.nmech) {
+      CK(cudaMemsetAsync(d->flag, 0, sizeof(int), d->stream));
+      k_maxabs<T><<<592, 256, 0, d->stream>>>(b.eta, (long long)6 * b.nmech * b.vol, d->red, d->flag);
+      d->launches++;
+      CK(cudaMemcpyAsync(part.data(), d->red, sizeof(double) * 592, cudaMemcpyDeviceToHost, d->stream));
+      CK(cudaMemcpyAsync(&fl, d->flag, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+      CK(cudaStreamSynchronize(d->stream));
+      for (double v : part) me = std::max(me, v);
+      nonfinite |= fl;
+    }
+  }
+  if (maxF) *maxF = mf;
+  if (maxEta) *maxEta = me;
+  if (nonfinite) return fail(WQL3D_ENONFINITE, "non-finite field or memory state (RUN-ELASTIC-001 / RUN-Q*-001)");
+  return WQL3D_OK;
+}
+
+wql3d_domain *checked(wql3d_domain *d) { return d; }
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *wql3d_last_error(void) { return g_err.c_str(); }
+
+int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
+  if (!desc || !out) return fail(WQL3D_EINVAL, "null argument");
+  *out = nullptr;
+  if (desc->abi_version != WQL3D_ABI_VERSION) return fail(WQL3D_EINVAL, "ABI version mismatch");
+  if (desc->nblocks < 1 || desc->nblocks > 2) return fail(WQL3D_EINVAL, "nblocks must be 1 or 2");
+  if (desc->precision != WQL3D_FP64 && desc->precision != WQL3D_FP32_COMPENSATED) return fail(WQL3D_EINVAL, "precision");
+  if (desc->response < 0 || desc->response > 3) return fail(WQL3D_EINVAL, "response");
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return fail(WQL3D_ECUDA, "no CUDA device");
+  int rc = upload_constants();
+  if (rc) return rc;
+  wql3d_domain *d = new wql3d_domain();
+  d->desc = *desc;
+  d->nblocks = desc->nblocks;
+  d->fp32 = desc->precision == WQL3D_FP32_COMPENSATED;
+  d->response = desc->response;
+  d->nmech = desc->response == WQL3D_ELASTIC ? 0 : desc->response == WQL3D_Q4 ? 4 : 8;
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete d;
+    return fail(WQL3D_ECUDA, "stream creation failed");
+  }
+  auto cleanup = [&](int code) {
+    cudaStreamSynchronize(d->stream);
+    d->mem.release();
+    cudaStreamDestroy(d->stream);
+    delete d;
+    return code;
+  };
+  if (d->mem.get(&d->time, 1) != cudaSuccess) return cleanup(fail(WQL3D_ENOMEM, "time"));
+  DevTime t0 = {0.0, 1, 0};
+  cudaMemcpy(d->time, &t0, sizeof(t0), cudaMemcpyHostToDevice);
+  if (d->mem.get(&d->red, 592) != cudaSuccess || d->mem.get(&d->flag, 1) != cudaSuccess)
+    return cleanup(fail(WQL3D_ENOMEM, "reduction scratch"));
+  for (int i = 0; i < d->nblocks; ++i) {
+    rc = d->fp32 ? setup_block<float>(d, i) : setup_block<double>(d, i);
+    if (rc) return cleanup(rc);
+  }
+  if (d->nblocks == 2) {
+    rc = d->fp32 ? setup_iface<float>(d->iface, d->desc, d->bf[0], d->bf[1], d->mem.ptrs, d->mem.bytes, d->stream)
+                 : setup_iface<double>(d->iface, d->desc, d->bd[0], d->bd[1], d->mem.ptrs, d->mem.bytes, d->stream);
+    if (rc) return cleanup(fail(rc, "interface setup failed"));
+    d->has_iface = true;
+    if (d->fp32) { d->bf[0].isat[1] = (float *)d->iface.sat_m; d->bf[1].isat[0] = (float *)d->iface.sat_p; }
+    else { d->bd[0].isat[1] = (double *)d->iface.sat_m; d->bd[1].isat[0] = (double *)d->iface.sat_p; }
+  }
+  if (cudaStreamSynchronize(d->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+    return cleanup(fail(WQL3D_ECUDA, "setup kernels failed"));
+  *out = d;
+  return WQL3D_OK;
+}
+
+int wql3d_domain_destroy(wql3d_domain *d) {
+  if (!d) return WQL3D_OK;
+  cudaStreamSynchronize(d->stream);
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  d->mem.release();
+  cudaStreamDestroy(d->stream);
+  delete d;
+  return WQL3D_OK;
+}
+
+#define DOM_CHECK(d, bi)                                                         \
+  if (!(d)) return fail(WQL3D_EINVAL, "null domain");                            \
+  if ((bi) < 0 || (bi) >= (d)->nblocks) return fail(WQL3D_EINVAL, "block index");
+
+int wql3d_set_fields(wql3d_domain *d, int bi, const double *F, int32_t host_nb) {
+  DOM_CHECK(d, bi);
+  if (!F || host_nb < 0) return fail(WQL3D_EINVAL, "fields");
+  int rc = d->fp32 ? put_array<float>(d, d->hb[bi], d->cur ? d->bf[bi].F1 : d->bf[bi].F0, 9, F, host_nb)
+                   : put_array<double>(d, d->hb[bi], d->cur ? d->bd[bi].F1 : d->bd[bi].F0, 9, F, host_nb);
+  if (rc) return rc;
+  if (d->fp32) CK(cudaMemsetAsync(d->bf[bi].FC, 0, sizeof(float) * 9 * d->bf[bi].vol, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_get_fields(wql3d_domain *d, int bi, double *F, int32_t host_nb) {
+  DOM_CHECK(d, bi);
+  if (!F || host_nb < 0) return fail(WQL3D_EINVAL, "fields");
+  if (host_nb > 0) {
+    long long hn = (long long)(d->hb[bi].nq + 2 * host_nb) * (d->hb[bi].nr + 2 * host_nb) * (d->hb[bi].ns + 2 * host_nb);
+    memset(F, 0, sizeof(double) * 9 * hn);
+  }
+  return d->fp32 ? get_array<float>(d, d->hb[bi], d->cur ? d->bf[bi].F1 : d->bf[bi].F0, 9, F, host_nb)
+                 : get_array<double>(d, d->hb[bi], d->cur ? d->bd[bi].F1 : d->bd[bi].F0, 9, F, host_nb);
+}
+
+int wql3d_set_rates(wql3d_domain *d, int bi, const double *DF, int32_t host_nb) {
+  DOM_CHECK(d, bi);
+  if (!DF || host_nb < 0) return fail(WQL3D_EINVAL, "rates");
+  int rc = d->fp32 ? put_array<float>(d, d->hb[bi], d->bf[bi].DF, 9, DF, host_nb)
+                   : put_array<double>(d, d->hb[bi], d->bd[bi].DF, 9, DF, host_nb);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_get_rates(wql3d_domain *d, int bi, double *DF, int32_t host_nb) {
+  DOM_CHECK(d, bi);
+  if (!DF || host_nb < 0) return fail(WQL3D_EINVAL, "rates");
+  if (host_nb > 0) {
+    long long hn = (long long)(d->hb[bi].nq + 2 * host_nb) * (d->hb[bi].nr + 2 * host_nb) * (d->hb[bi].ns + 2 * host_nb);
+    memset(DF, 0, sizeof(double) * 9 * hn);
+  }
+  return d->fp32 ? get_array<float>(d, d->hb[bi], d->bf[bi].DF, 9, DF, 0 + host_nb)
+                 : get_array<double>(d, d->hb[bi], d->bd[bi].DF, 9, DF, host_nb);
+}
+
+int wql3d_get_memory_variables(wql3d_domain *d, int bi, double *eta) {
+  DOM_CHECK(d, bi);
+  if (!d->nmech) return fail(WQL3D_EINVAL, "elastic domain has no memory variables");
+  return d->fp32 ? get_array<float>(d, d->hb[bi], d->bf[bi].eta, 6 * d->nmech, eta, 0)
+                 : get_array<double>(d, d->hb[bi], d->bd[bi].eta, 6 * d->nmech, eta, 0);
+}
+
+int wql3d_get_metrics(wql3d_domain *d, int bi, double *out) {
+  DOM_CHECK(d, bi);
+  const HostBlock &h = d->hb[bi];
+  long long n1 = (long long)h.nq * h.nr * h.ns;
+  if (h.mesh == WQL3D_MESH_CARTESIAN) {
+    // diagonal metric and J of the separable mesh, off-diagonals zero
+    int nn[3] = {h.nq, h.nr, h.ns};
+    std::vector<double> m[3];
+    for (int a = 0; a < 3; ++a) {
+      m[a].resize((size_t)nn[a] + 1);
+      const void *src = a == 0 ? (d->fp32 ? (const void *)d->bf[bi].mq : (const void *)d->bd[bi].mq)
+                        : a == 1 ? (d->fp32 ? (const void *)d->bf[bi].mr : (const void *)d->bd[bi].mr)
+                                 : (d->fp32 ? (const void *)d->bf[bi].ms : (const void *)d->bd[bi].ms);
+      if (d->fp32) {
+        std::vector<float> tmp((size_t)nn[a] + 1);
+        CK(cudaMemcpy(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < tmp.size(); ++i) m[a][i] = tmp[i];
+      } else {
+        CK(cudaMemcpy(m[a].data(), src, sizeof(double) * m[a].size(), cudaMemcpyDeviceToHost));
+      }
+    }
+    memset(out, 0, sizeof(double) * 10 * n1);
+    for (int z = 1; z <= h.ns; ++z)
+      for (int y = 1; y <= h.nr; ++y)
+        for (int x = 1; x <= h.nq; ++x) {
+          long long i = (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1));
+          out[0 * n1 + i] = m[0][x];
+          out[4 * n1 + i] = m[1][y];
+          out[8 * n1 + i] = m[2][z];
+          out[9 * n1 + i] = 1.0 / (m[0][x] * m[1][y] * m[2][z]);
+        }
+    return WQL3D_OK;
+  }
+  int rc = d->fp32 ? get_array<float>(d, h, d->bf[bi].met, 9, out, 0) : get_array<double>(d, h, d->bd[bi].met, 9, out, 0);
+  if (rc) return rc;
+  return d->fp32 ? get_array<float>(d, h, d->bf[bi].J, 1, out + 9 * n1, 0) : get_array<double>(d, h, d->bd[bi].J, 1, out + 9 * n1, 0);
+}
+
+int wql3d_get_interface(wql3d_domain *d, double *out) {
+  if (!d || !d->has_iface) return fail(WQL3D_EINVAL, "no interface");
+  return iface_download(d->iface, out, d->stream);
+}
+
+int wql3d_set_time(wql3d_domain *d, double t) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  h.t = t;
+  CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_get_time(wql3d_domain *d, double *t) {
+  if (!d || !t) return fail(WQL3D_EINVAL, "null argument");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  *t = h.t;
+  return WQL3D_OK;
+}
+
+int wql3d_stage(wql3d_domain *d, int stage, double dt) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  if (stage < 1 || stage > 5) return fail(WQL3D_EINVAL, "stage must be 1..5");
+  int rc = d->fp32 ? enqueue_stage<float>(d, stage, dt, F_ALL) : enqueue_stage<double>(d, stage, dt, F_ALL);
+  if (rc) return rc;
+  if (stage == 5) {
+    k_advance<<<1, 32, 0, d->stream>>>(d->time, dt);
+    d->launches++;
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_time_step(wql3d_domain *d, double dt, int n, int w_stride) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  h.n = n;
+  CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
+  int rc = d->fp32 ? enqueue_step<float>(d, dt, w_stride) : enqueue_step<double>(d, dt, w_stride);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_run(wql3d_domain *d, double dt, int n_first, int nsteps, int w_stride) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  if (nsteps < 0) return fail(WQL3D_EINVAL, "nsteps");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  h.n = n_first;
+  CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
+  return d->fp32 ? run_steps<float>(d, dt, nsteps, w_stride) : run_steps<double>(d, dt, nsteps, w_stride);
+}
+
+int wql3d_scale_rates(wql3d_domain *d, double A) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  // A*DF and the point-local memory-variable / PML rates, whole arrays
+  for (int i = 0; i < d->nblocks; ++i) {
+    if (d->fp32) {
+      Blk<float> &b = d->bf[i];
+      k_scale_T<float><<<1184, 256, 0, d->stream>>>(b.DF, 9 * b.vol, A);
+      if (b.nmech) k_scale_T<float><<<1184, 256, 0, d->stream>>>(b.deta, (long long)6 * b.nmech * b.vol, A);
+      for (int f = 0; f < 6; ++f)
+        if (b.pml_on[f]) k_scale_T<float><<<1184, 256, 0, d->stream>>>(b.DQ[f], 9 * b.pvol[f], A);
+    } else {
+      Blk<double> &b = d->bd[i];
+      k_scale_T<double><<<1184, 256, 0, d->stream>>>(b.DF, 9 * b.vol, A);
+      if (b.nmech) k_scale_T<double><<<1184, 256, 0, d->stream>>>(b.deta, (long long)6 * b.nmech * b.vol, A);
+      for (int f = 0; f < 6; ++f)
+        if (b.pml_on[f]) k_scale_T<double><<<1184, 256, 0, d->stream>>>(b.DQ[f], 9 * b.pvol[f], A);
+    }
+    d->launches++;
+  }
+  if (d->has_iface) {
+    iface_scale(d->iface, A, d->stream);
+    d->launches++;
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_set_rates_rhs(wql3d_domain *d) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  // stage index 1 makes the source evaluate at the current domain time
+  StageArgs a;
+  a.cur = d->cur;
+  a.flags = F_RHS | F_SOURCE;
+  a.stage = 1;
+  a.A = 1.0;
+  a.Bdt = 0.0;
+  a.dt = 0.0;
+  a.time = d->time;
+  for (int i = 0; i < d->nblocks; ++i) {
+    if (d->fp32) launch_stage<float>(d, i, a);
+    else launch_stage<double>(d, i, a);
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_try_traditional_rhs(wql3d_domain *d, int *handled) {
+  if (handled) *handled = 0;
+  int rc = wql3d_set_rates_rhs(d);
+  if (rc) return rc;
+  if (handled) *handled = 1;
+  return WQL3D_OK;
+}
+
+int wql3d_enforce_bound_iface_conditions(wql3d_domain *d, int stage) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  StageArgs a;
+  a.cur = d->cur;
+  a.flags = F_SAT | (d->has_iface ? F_ISAT : 0);
+  a.stage = stage < 1 ? 1 : stage;
+  a.A = 1.0;
+  a.Bdt = 0.0;
+  a.dt = 0.0;
+  a.time = d->time;
+  if (d->has_iface) {
+    if (d->fp32) launch_iface<float>(d->iface, d->bf[0], d->bf[1], a, d->stream);
+    else launch_iface<double>(d->iface, d->bd[0], d->bd[1], a, d->stream);
+    d->launches++;
+  }
+  for (int i = 0; i < d->nblocks; ++i) {
+    if (d->fp32) launch_stage<float>(d, i, a);
+    else launch_stage<double>(d, i, a);
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_update_fields(wql3d_domain *d, double dt) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  for (int i = 0; i < d->nblocks; ++i) {
+    if (d->fp32) {
+      Blk<float> &b = d->bf[i];
+      dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
+      k_update_inplace<float><<<gr, th, 0, d->stream>>>(b, d->cur, dt);
+      if (b.nmech) k_axpy_T<float><<<1184, 256, 0, d->stream>>>(b.eta, b.deta, (long long)6 * b.nmech * b.vol, dt);
+      for (int f = 0; f < 6; ++f)
+        if (b.pml_on[f]) k_axpy_T<float><<<1184, 256, 0, d->stream>>>(b.Q[f], b.DQ[f], 9 * b.pvol[f], dt);
+    } else {
+      Blk<double> &b = d->bd[i];
+      dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
+      k_update_inplace<double><<<gr, th, 0, d->stream>>>(b, d->cur, dt);
+      if (b.nmech) k_axpy_T<double><<<1184, 256, 0, d->stream>>>(b.eta, b.deta, (long long)6 * b.nmech * b.vol, dt);
+      for (int f = 0; f < 6; ++f)
+        if (b.pml_on[f]) k_axpy_T<double><<<1184, 256, 0, d->stream>>>(b.Q[f], b.DQ[f], 9 * b.pvol[f], dt);
+    }
+    d->launches++;
+  }
+  if (d->has_iface) {
+    StageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.Bdt = dt;
+    launch_iface_update<double>(d->iface, a, d->stream);
+    d->launches++;
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_scale_rate_array(double *rate, int64_t n, double coefficient, void *stream) {
+  if (n < 0 || (n > 0 && !rate)) return fail(WQL3D_EINVAL, "rate array");
+  if (n == 0) return WQL3D_OK;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_scale_array<<<blocks, 256, 0, (cudaStream_t)stream>>>(rate, n, coefficient);
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_update_state_array(double *state, const double *rate, int64_t n, double increment, void *stream) {
+  if (n < 0 || (n > 0 && (!state || !rate))) return fail(WQL3D_EINVAL, "state/rate array");
+  if (n == 0) return WQL3D_OK;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_axpy_array<<<blocks, 256, 0, (cudaStream_t)stream>>>(state, rate, n, increment);
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_get_seismograms(wql3d_domain *d, int bi, double *out, int32_t *nsamples) {
+  DOM_CHECK(d, bi);
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  int ns = std::min(h.nsamp, d->desc.max_samples);
+  if (nsamples) *nsamples = ns;
+  int nrec = d->hb[bi].nrec;
+  if (out && ns > 0 && nrec > 0) {
+    const double *src = d->fp32 ? d->bf[bi].seis : d->bd[bi].seis;
+    CK(cudaMemcpyAsync(out, src, sizeof(double) * (size_t)ns * nrec * 4, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  return WQL3D_OK;
+}
+
+int wql3d_receiver_index(wql3d_domain *d, int bi, int32_t *idx) {
+  DOM_CHECK(d, bi);
+  if (d->hb[bi].nrec > 0) memcpy(idx, d->hb[bi].ridx.data(), sizeof(int32_t) * 3 * d->hb[bi].nrec);
+  return WQL3D_OK;
+}
+
+int wql3d_final_state(wql3d_domain *d, double *max_field, double *max_memory, double *block_max) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  return d->fp32 ? final_state<float>(d, max_field, max_memory, block_max)
+                 : final_state<double>(d, max_field, max_memory, block_max);
+}
+
+int wql3d_synchronize(wql3d_domain *d) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  CK(cudaStreamSynchronize(d->stream));
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_get_stream(wql3d_domain *d, void **stream) {
+  if (!d || !stream) return fail(WQL3D_EINVAL, "null argument");
+  *stream = (void *)d->stream;
+  return WQL3D_OK;
+}
+
+int wql3d_device_bytes(wql3d_domain *d, int64_t *bytes) {
+  if (!d || !bytes) return fail(WQL3D_EINVAL, "null argument");
+  *bytes = d->mem.bytes;
+  return WQL3D_OK;
+}
+
+int wql3d_kernel_launches(wql3d_domain *d, int64_t *launches) {
+  if (!d || !launches) return fail(WQL3D_EINVAL, "null argument");
+  *launches = d->launches;
+  return WQL3D_OK;
+}
+
+}  // extern "C"

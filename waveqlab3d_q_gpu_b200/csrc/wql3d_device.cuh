@@ -1,0 +1,846 @@
+// Device-side data model and kernels of the WaveQLab3D per-step volume update.
+//
+// Layout (HBM): every 3-D component is a padded x-fastest array with XOFF
+// leading pad points in x (so the first interior point of every row starts on
+// a 32-byte sector), a row pitch rounded up to 128 bytes, and 3 ghost planes
+// in y and z.  Components of one logical array follow one another at a fixed
+// component stride.  Two field buffers alternate between RK stages (the
+// stencil reads buffer `cur` and the fused update writes buffer `cur^1`), so
+// one stage is a single pass over F, DF and the material.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace wql3d {
+
+constexpr int NB = 3;               // ghost width of the traditional-6 operator
+constexpr int MESH_CART = 0;
+constexpr int MESH_CURV = 1;
+constexpr int RESP_EL = 0, RESP_Q4 = 1, RESP_Q8 = 2, RESP_FQ8 = 3;
+
+// stage flags
+constexpr int F_SCALE = 1;     // DF <- A*DF (and memory-variable / PML rates)
+constexpr int F_RHS = 2;       // DF += L(F) (interior and near-boundary, anelastic, PML)
+constexpr int F_SOURCE = 4;    // moment-tensor sources
+constexpr int F_SAT = 8;       // physical-boundary SAT
+constexpr int F_ISAT = 16;     // interface SAT (precomputed face vector)
+constexpr int F_UPDATE = 32;   // F <- F + B*dt*DF (+ memory variables, PML)
+constexpr int F_ALL = 63;
+
+// Kennedy-Carpenter (5,4) coefficients, src/time_step.f90:53-62
+__constant__ double c_rkA[5];
+__constant__ double c_rkB[5];
+__constant__ double c_rkC[6];
+
+// SBP first-derivative rows 1..6 in the order the reference sums their terms
+// (src/JU_xJU_yJU_z6.f90:74-161); [lit] selects the row-4 literal precision.
+__constant__ int c_sbp_cnt[6];
+__constant__ int c_sbp_idx[6][8];
+__constant__ double c_sbp_c[2][6][8];
+
+struct DevSource {
+  int type;
+  int near[3];
+  double phys[3];
+  double par[11];  // duration t_init mxx myy mzz mxy mxz myz x y z
+};
+
+struct DevTime {
+  double t;        // domain time at the start of the current step (D%t)
+  int n;           // current step number (1-based)
+  int nsamp;       // receiver samples taken
+};
+
+template <typename T>
+struct Blk {
+  int nx, ny, nz;
+  long long sy, sz;     // y and z strides in elements
+  long long o1;         // element offset of point (1,1,1)
+  long long vol;        // component stride
+  T *F0, *F1;           // field buffers (9 components each)
+  T *DF;                // rates (9 components)
+  T *FC;                // FP32 path: Kahan compensation for F (9 components)
+  T *M;                 // lambda, mu, rho
+  // Cartesian: per-axis diagonal metric 1/X_a(i) (index 1..n)
+  const T *mq, *mr, *ms;
+  // curvilinear: metricx(1..3), metricy(1..3), metricz(1..3), then J
+  const T *met;
+  const T *J;
+  int lo[3], hi[3];     // strict-interior bounds (1-based, inclusive)
+  T hq, hr, hs;         // unit-cube spacing
+  T ihq, ihr, ihs;      // 1/h
+  T cx[3], cy[3], cz[3];// interior coefficients c/h
+  int lit;              // SBP literal precision (index into c_sbp_c)
+  // PML slabs (faces 0..5): box and Q / DQ (9 components each, slab-local)
+  int npml;
+  int pml_on[6];
+  int pb[6][6];         // x0 x1 y0 y1 z0 z1
+  long long pvol[6];
+  T *Q[6], *DQ[6];
+  T d0;                 // PML damping strength
+  // anelastic memory variables: 6 components x nmech, stride vol
+  int nmech;
+  T *eta, *deta;
+  const T *qs, *qp;
+  T tau[8], w[8], ss[8], ps[8];
+  int coarse;
+  // physical boundaries
+  int bc[6];
+  T tau0;
+  const T *nrm[6];      // curvilinear face bases n_l(3) n_m(3) n_n(3), face-local
+  // interface SAT vectors (q-min face: isat[0], q-max face: isat[1]), 9 x ny*nz
+  T *isat[2];
+  // sources
+  int nsrc, src_order, src_alpha, src_half;
+  const DevSource *src;
+  int sbox[6];          // union box of all source supports (x0 x1 y0 y1 z0 z1)
+  // receivers
+  int nrec;
+  const int *ridx;
+  double *seis;
+  int max_samples;
+};
+
+struct StageArgs {
+  int cur;              // field buffer read by the stencil
+  int flags;
+  int stage;            // 1..5
+  double A, Bdt, dt;
+  const DevTime *time;
+};
+
+template <typename T>
+__device__ __forceinline__ long long pidx(const Blk<T> &b, int x, int y, int z) {
+  return b.o1 + (long long)(x - 1) + b.sy * (long long)(y - 1) + b.sz * (long long)(z - 1);
+}
+
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// SBP stencil row at 1-based index i of an axis with n points: taps as
+// relative offsets and signed coefficients, in the reference's summation
+// order.  Interior rows (7 <= i <= n-6) use the central operator
+// -1/60, 3/20, -3/4, 3/4, -3/20, 1/60 (src/JU_xJU_yJU_z6.f90:52-68).
+// ---------------------------------------------------------------------------
+struct Row {
+  int cnt;
+  int off[8];
+  double c[8];
+};
+
+__device__ __forceinline__ void sbp_row(int i, int n, int lit, Row &r) {
+  if (i >= 7 && i <= n - 6) {
+    r.cnt = 6;
+    r.off[0] = -3; r.off[1] = -2; r.off[2] = -1; r.off[3] = 1; r.off[4] = 2; r.off[5] = 3;
+    r.c[0] = -1.0 / 60.0; r.c[1] = 0.15; r.c[2] = -0.75; r.c[3] = 0.75; r.c[4] = -0.15; r.c[5] = 1.0 / 60.0;
+    return;
+  }
+  if (i >= n - 5) {  // right closure: negated mirror of left row n+1-i
+    int row = n - i;
+    r.cnt = c_sbp_cnt[row];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      r.off[k] = (n + 1 - c_sbp_idx[row][k]) - i;
+      r.c[k] = -c_sbp_c[lit][row][k];
+    }
+    return;
+  }
+  int row = i - 1;
+  r.cnt = c_sbp_cnt[row];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    r.off[k] = c_sbp_idx[row][k] - i;
+    r.c[k] = c_sbp_c[lit][row][k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Moment-tensor source: src/moment_tensor.f90:813-1125
+// ---------------------------------------------------------------------------
+__device__ inline double source_time(int type, double t, double t0, double w) {
+  const double pi = 3.141592653589793;
+  switch (type) {
+    case 0: return (w / (sqrt(2.0 * pi))) * exp((-(w * w) * ((t - t0) * (t - t0))) / 2.0);
+    case 1: return (t / (w * w)) * exp(-t / w);
+    case 2: return (w * w) * t * exp(-w * t);
+    case 3: return (t < t0) ? (1.0 - cos(2.0 * pi * t / t0)) / t0 : 0.0;
+    case 4: return ((t >= 0.0) && (t <= w)) ? 1.0 - cos(2.0 * pi * t / w) : 0.0;
+    case 5: return (1.0 - (1.0 + t / w) * exp(-t / w));
+    case 6: return (t <= w) ? t - w / (2.0 * pi) * sin(2.0 * pi * t / w) : w;
+    case 7: {
+      double a = pi * w * (t - t0);
+      double a2 = a * a;
+      return (1.0 - 2.0 * a2) * exp(-a2);
+    }
+  }
+  return 0.0;
+}
+
+__device__ inline double singular_source(int i, int i0, double h, double a, int order, int alpha) {
+  if (order == 2) {
+    double beta = (1.0 - 2.0 * a) / 4.0 + 0.25;
+    double gam = (2.0 * a - 1.0) / 16.0;
+    double gap = (2.0 * a + 1.0) / 16.0;
+    if (i == i0 - 2) return (-gam) / h;
+    if (i == i0 - 1) return (beta + 3.0 * gam - gap) / h;
+    if (i == i0) return (1.0 - a - 2.0 * beta - 3.0 * gam + 3.0 * gap) / h;
+    if (i == i0 + 1) return (a + beta + gam - 3.0 * gap) / h;
+    if (i == i0 + 2) return gap / h;
+    return 0.0;
+  }
+  const double w0[9] = {-0.01171875, -0.03125, 0.046875, 0.28125, 0.4296875, 0.28125, 0.046875, -0.03125, -0.01171875};
+  const double w25[9] = {-0.00246875, -0.02275, -0.014125, 0.16575, 0.4171875, 0.38675, 0.117875, -0.02975, -0.01846875};
+  const double w50[9] = {-0.00728125, -0.028, 0.014875, 0.224, 0.4265625, 0.336, 0.081375, -0.032, -0.01553125};
+  const double w100[9] = {-0.0095625, -0.02990625, 0.03053125, 0.25284375, 0.42890625, 0.30903125, 0.06384375, -0.03196875, -0.01371875};
+  int k = i - i0;
+  if (k < -4 || k > 4) return 0.0;
+  const double *w = alpha == 0 ? w0 : alpha == 25 ? w25 : alpha == 50 ? w50 : alpha == 100 ? w100 : nullptr;
+  if (!w) return 0.0;
+  return w[k + 4] / h;
+}
+
+// diagonal metric at a point (Cartesian: per-axis table; curvilinear: array)
+template <typename T, int MESH>
+__device__ __forceinline__ T diag_metric(const Blk<T> &b, int axis, int x, int y, int z, long long p) {
+  return ld(b.met + (long long)(axis * 3 + axis) * b.vol + p);
+}
+
+template <typename T, int MESH>
+__device__ void add_sources(const Blk<T> &b, double t, int x, int y, int z, long long p, T df[9]) {
+  for (int i = 0; i < b.nsrc; ++i) {
+    const DevSource &s = b.src[i];
+    if (s.near[0] < 1) continue;
+    if (abs(x - s.near[0]) > b.src_half || abs(y - s.near[1]) > b.src_half || abs(z - s.near[2]) > b.src_half) continue;
+    double A = source_time(s.type, t, s.par[1], s.par[0]);
+    double hx = (double)b.hq / (double)diag_metric<T, MESH>(b, 0, x, y, z, p);
+    double hy = (double)b.hr / (double)diag_metric<T, MESH>(b, 1, x, y, z, p);
+    double hz = (double)b.hs / (double)diag_metric<T, MESH>(b, 2, x, y, z, p);
+    double ax = (s.par[8] - s.phys[0]) / hx;
+    double ay = (s.par[9] - s.phys[1]) / hy;
+    double az = (s.par[10] - s.phys[2]) / hz;
+    double dx = singular_source(x, s.near[0], hx, ax, b.src_order, b.src_alpha);
+    double dy = singular_source(y, s.near[1], hy, ay, b.src_order, b.src_alpha);
+    double dz = singular_source(z, s.near[2], hz, az, b.src_order, b.src_alpha);
+    double delta = dx * dy * dz;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) df[3 + c] = (T)((double)df[3 + c] - A * s.par[2 + c] * delta);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Physical-boundary SAT at one face point: BC_* + BCm/BCp + structure,
+// src/BoundaryConditions.f90:50-924, src/RHS_Interior.f90:1584-1768, :2267-2287
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ void bc_vector(int plus, const T u[9], T Zs, T Zp, T r, const T l[3], const T m[3], const T n[3], T norm,
+                          T ubc[9]) {
+  T T0 = n[0] * u[3] + n[1] * u[6] + n[2] * u[7];
+  T T1 = n[0] * u[6] + n[1] * u[4] + n[2] * u[8];
+  T T2 = n[0] * u[7] + n[1] * u[8] + n[2] * u[5];
+  T vl = l[0] * u[0] + l[1] * u[1] + l[2] * u[2];
+  T vm = m[0] * u[0] + m[1] * u[1] + m[2] * u[2];
+  T vn = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+  T Tl = l[0] * T0 + l[1] * T1 + l[2] * T2;
+  T Tm = m[0] * T0 + m[1] * T1 + m[2] * T2;
+  T Tn = n[0] * T0 + n[1] * T1 + n[2] * T2;
+  const T one = (T)1, half = (T)0.5;
+  T sg = plus ? one : -one;
+  T pl = half * ((one - r) * Zs * vl + sg * ((one + r) * Tl));
+  T pm = half * ((one - r) * Zs * vm + sg * ((one + r) * Tm));
+  T pn = half * ((one - r) * Zp * vn + sg * ((one + r) * Tn));
+  T ql = half * ((one - r) * vl + sg * ((one + r) / Zs * Tl));
+  T qm = half * ((one - r) * vm + sg * ((one + r) / Zs * Tm));
+  T qn = half * ((one - r) * vn + sg * ((one + r) / Zp * Tn));
+  T Fx = l[0] * pl + m[0] * pm + n[0] * pn;
+  T Fy = l[1] * pl + m[1] * pm + n[1] * pn;
+  T Fz = l[2] * pl + m[2] * pm + n[2] * pn;
+  T F_x = l[0] * ql + m[0] * qm + n[0] * qn;
+  T F_y = l[1] * ql + m[1] * qm + n[1] * qn;
+  T F_z = l[2] * ql + m[2] * qm + n[2] * qn;
+  ubc[0] = norm * Fx;
+  ubc[1] = norm * Fy;
+  ubc[2] = norm * Fz;
+  ubc[3] = sg * (norm * n[0] * F_x);
+  ubc[4] = sg * (norm * n[1] * F_y);
+  ubc[5] = sg * (norm * n[2] * F_z);
+  ubc[6] = sg * (norm * (n[1] * F_x + n[0] * F_y));
+  ubc[7] = sg * (norm * (n[2] * F_x + n[0] * F_z));
+  ubc[8] = sg * (norm * (n[2] * F_y + n[1] * F_z));
+}
+
+template <typename T, int MESH>
+__device__ void add_face_sats(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T df[9], bool pml_point) {
+  const int pos[3] = {x, y, z};
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  T u[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) u[c] = F[c * b.vol + p];
+  const T lam = b.M[p], mu = b.M[b.vol + p], rho = b.M[2 * b.vol + p];
+  for (int f = 0; f < 6; ++f) {
+    int type = b.bc[f];
+    if (type <= 0) continue;
+    int axis = f >> 1, plus = f & 1;
+    if (pos[axis] != (plus ? nn[axis] : 1)) continue;
+    T r = type == 1 ? (T)0 : type == 2 ? (T)1 : (T)-1;
+    T c_p = sqrt(((T)2 * mu + lam) / rho);
+    T c_s = sqrt(mu / rho);
+    T Zp = rho * c_p, Zs = rho * c_s;
+    T l[3], m[3], n[3], norm;
+    {
+      T qx = ld(b.met + (long long)(0 + axis) * b.vol + p);
+      T qy = ld(b.met + (long long)(3 + axis) * b.vol + p);
+      T qz = ld(b.met + (long long)(6 + axis) * b.vol + p);
+      norm = sqrt(qx * qx + qy * qy + qz * qz);
+      int a0 = axis == 0 ? y : x, a1 = axis == 2 ? y : z;
+      int d0 = axis == 0 ? b.ny : b.nx;
+      long long fp = (long long)(a0 - 1) + (long long)d0 * (a1 - 1);
+      long long fn = (long long)d0 * (axis == 2 ? b.ny : b.nz);
+      const T *B = b.nrm[f];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        l[c] = ld(B + (0 + c) * fn + fp);
+        m[c] = ld(B + (3 + c) * fn + fp);
+        n[c] = ld(B + (6 + c) * fn + fp);
+      }
+    }
+    T ubc[9], Ux[9];
+    bc_vector<T>(plus, u, Zs, Zp, r, l, m, n, norm, ubc);
+    // structure(), src/RHS_Interior.f90:2267-2287
+    const T irho = (T)1 / rho;
+    Ux[0] = irho * ubc[0];
+    Ux[1] = irho * ubc[1];
+    Ux[2] = irho * ubc[2];
+    Ux[3] = ((T)2 * mu + lam) * ubc[3] + lam * (ubc[4] + ubc[5]);
+    Ux[4] = ((T)2 * mu + lam) * ubc[4] + lam * (ubc[3] + ubc[5]);
+    Ux[5] = ((T)2 * mu + lam) * ubc[5] + lam * (ubc[3] + ubc[4]);
+    Ux[6] = mu * ubc[6];
+    Ux[7] = mu * ubc[7];
+    Ux[8] = mu * ubc[8];
+    T h = axis == 0 ? b.hq : axis == 1 ? b.hr : b.hs;
+    T pen = b.tau0 / h;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) df[c] = df[c] - pen * Ux[c];
+    if (pml_point && b.pml_on[f]) {
+      const int *B = b.pb[f];
+      long long q = (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+      T *DQ = b.DQ[f];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) DQ[c * b.pvol[f] + q] = DQ[c * b.pvol[f] + q] - pen * ubc[c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Anelastic memory variables at one point, src/RHS_Interior.f90:2599-2908,
+// :3361-3477 and the interior copies src/JU_xJU_yJU_z6.f90:16263-16420.
+// e = (exx, eyy, ezz, gxy, gxz, gyz) strain rates (PML-corrected in slabs).
+// The eta sums are subtracted from s (df in the interior form, DU near
+// boundaries).  Memory-variable rates are scaled, accumulated and (with
+// F_UPDATE) integrated here because they are point-local.
+// ---------------------------------------------------------------------------
+template <typename T, int RESP>
+__device__ void anelastic_point(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p, const T e[6], T tr,
+                                T s[9], bool do_rhs) {
+  constexpr int N = RESP == RESP_Q4 ? 4 : 8;
+  const long long V = b.vol;
+  const T lam = b.M[p], mu = b.M[V + p];
+  T qs = 0, qp = 0;
+  if (RESP != RESP_FQ8) { qs = ld(b.qs + p); qp = ld(b.qp + p); }
+  int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    T eta[N], de[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      eta[i] = b.eta[(long long)(c * N + i) * V + p];
+      de[i] = b.deta[(long long)(c * N + i) * V + p];
+      if (a.flags & F_SCALE) de[i] = (T)a.A * de[i];
+    }
+    if (do_rhs) {
+      T sum = eta[0];
+#pragma unroll
+      for (int i = 1; i < N; ++i) sum = sum + eta[i];
+      s[3 + c] = s[3 + c] - sum;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        if (RESP == RESP_FQ8) {
+          if (b.coarse && (i + 1) != active) continue;
+          T ss = b.ss[i], ps = b.ps[i];
+          if (c < 3)
+            de[i] = de[i] + (((ss * (T)2 * mu) * e[c] + ((lam + (T)2 * mu) * ps - (T)2 * mu * ss) * tr) - eta[i]) / b.tau[i];
+          else
+            de[i] = de[i] + ((ss * mu * e[c] - eta[i]) / b.tau[i]);
+        } else {
+          T w = b.w[i];
+          if (c < 3)
+            de[i] = de[i] + (((w * (T)2 * mu * qs) * e[c] + (w * ((lam + (T)2 * mu) * qp - (T)2 * mu * qs)) * tr) - eta[i]) / b.tau[i];
+          else
+            de[i] = de[i] + ((w * mu * qs * e[c] - eta[i]) / b.tau[i]);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      b.deta[(long long)(c * N + i) * V + p] = de[i];
+      if (a.flags & F_UPDATE) b.eta[(long long)(c * N + i) * V + p] = eta[i] + (T)a.Bdt * de[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PML at one point, src/RHS_Interior.f90:1846-2265.  Slabs are visited in the
+// reference order z-, z+, y-, y+, x-, x+.  Ux(4:9) carry J (JJU_x6), so the
+// DQ(1:3) sources divide by J.
+// ---------------------------------------------------------------------------
+template <typename T, bool JFORM>
+__device__ void pml_point(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p, const T Ux[9], const T Uy[9],
+                          const T Uz[9], T rhoJ_inv, T lambda2mu, T J, T DU[9]) {
+  const int order[6] = {4, 5, 2, 3, 0, 1};
+  const long long V = b.vol;
+  const T lam = b.M[p], mu = b.M[V + p];
+  const T cfs = (T)1;
+  const int pos[3] = {x, y, z};
+  for (int oi = 0; oi < 6; ++oi) {
+    int f = order[oi];
+    if (!b.pml_on[f]) continue;
+    const int *B = b.pb[f];
+    if (x < B[0] || x > B[1] || y < B[2] || y > B[3] || z < B[4] || z > B[5]) continue;
+    int axis = f >> 1;
+    int n = axis == 0 ? b.nx : axis == 1 ? b.ny : b.nz;
+    int i = pos[axis];
+    T v = (f == 4) ? (T)(i - b.npml) : ((f & 1) ? (T)(i - (n - b.npml)) : (T)(i - (1 + b.npml)));
+    T d = b.d0 * fabs(v / (T)b.npml);
+    long long q = (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+    T *Qp = b.Q[f];
+    T *DQp = b.DQ[f];
+    const long long PV = b.pvol[f];
+    T Q[9], DQ[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      Q[c] = Qp[c * PV + q];
+      DQ[c] = DQp[c * PV + q];
+    }
+    if (JFORM) {
+      DU[0] = DU[0] - d * J * Q[0] * rhoJ_inv;
+      DU[1] = DU[1] - d * J * Q[1] * rhoJ_inv;
+      DU[2] = DU[2] - d * J * Q[2] * rhoJ_inv;
+    } else {
+      DU[0] = DU[0] - d * Q[0] * rhoJ_inv;
+      DU[1] = DU[1] - d * Q[1] * rhoJ_inv;
+      DU[2] = DU[2] - d * Q[2] * rhoJ_inv;
+    }
+    DU[3] = DU[3] - d * (lambda2mu * Q[3] + lam * Q[4] + lam * Q[5]);
+    DU[4] = DU[4] - d * (lam * Q[3] + lambda2mu * Q[4] + lam * Q[5]);
+    DU[5] = DU[5] - d * (lam * Q[3] + lam * Q[4] + lambda2mu * Q[5]);
+    DU[6] = DU[6] - mu * d * Q[6];
+    DU[7] = DU[7] - mu * d * Q[7];
+    DU[8] = DU[8] - mu * d * Q[8];
+    T src[9];
+    const T iJ = JFORM ? J : (T)1;
+    if (axis == 2) {
+      src[0] = Uz[7] / iJ; src[1] = Uz[8] / iJ; src[2] = Uz[5] / iJ; src[3] = 0; src[4] = 0;
+      src[5] = Uz[2]; src[6] = 0; src[7] = Uz[0]; src[8] = Uz[1];
+    } else if (axis == 1) {
+      src[0] = Uy[6] / iJ; src[1] = Uy[4] / iJ; src[2] = Uy[8] / iJ; src[3] = 0; src[4] = Uy[1];
+      src[5] = 0; src[6] = Uy[0]; src[7] = 0; src[8] = Uy[2];
+    } else {
+      src[0] = Ux[3] / iJ; src[1] = Ux[6] / iJ; src[2] = Ux[7] / iJ; src[3] = Ux[0]; src[4] = 0;
+      src[5] = 0; src[6] = Ux[1]; src[7] = Ux[2]; src[8] = 0;
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) DQ[c] = DQ[c] + src[c] - (d + cfs) * Q[c];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) DQp[c * PV + q] = DQ[c];
+  }
+}
+
+// PML damping and auxiliary fields for the anelastic strain correction,
+// src/RHS_Interior.f90:2351-2451
+template <typename T>
+__device__ bool pml_strain_correction(const Blk<T> &b, int x, int y, int z, T e[6]) {
+  bool in = false;
+  T dd[3] = {0, 0, 0};
+  T Qd[3][9];
+  for (int k = 0; k < 3; ++k)
+    for (int c = 0; c < 9; ++c) Qd[k][c] = 0;
+  const int pos[3] = {x, y, z};
+  for (int f = 0; f < 6; ++f) {
+    if (!b.pml_on[f]) continue;
+    const int *B = b.pb[f];
+    if (x < B[0] || x > B[1] || y < B[2] || y > B[3] || z < B[4] || z > B[5]) continue;
+    in = true;
+    int axis = f >> 1;
+    int n = axis == 0 ? b.nx : axis == 1 ? b.ny : b.nz;
+    int i = pos[axis];
+    T v = (f == 4) ? (T)(i - b.npml) : ((f & 1) ? (T)(i - (n - b.npml)) : (T)(i - (1 + b.npml)));
+    dd[axis] = b.d0 * fabs(v / (T)b.npml);
+    long long q = (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+    for (int c = 0; c < 9; ++c) Qd[axis][c] = b.Q[f][c * b.pvol[f] + q];
+  }
+  if (!in) return false;
+  // exx = Ux(1) - dx*Qx(4), ..., gxy = (Uy(1)+Ux(2)) - dx*Qx(7) - dy*Qy(7), ...
+  e[0] = e[0] - dd[0] * Qd[0][3];
+  e[1] = e[1] - dd[1] * Qd[1][4];
+  e[2] = e[2] - dd[2] * Qd[2][5];
+  e[3] = e[3] - dd[0] * Qd[0][6] - dd[1] * Qd[1][6];
+  e[4] = e[4] - dd[0] * Qd[0][7] - dd[2] * Qd[2][7];
+  e[5] = e[5] - dd[1] * Qd[1][8] - dd[2] * Qd[2][8];
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Near-boundary derivatives, both mesh kinds: JJU_x6
+// (src/JU_xJU_yJU_z6.f90:12-809) for one metric row: velocities
+// X_a(p) * D_a(u), stresses D_a(F * J * X_a), summed over the three axes.
+// A Cartesian grid keeps its full metric here: without -r8 the row-4
+// literal leaves off-diagonal metric terms of order 1e-10.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ void jju6_row(const Blk<T> &b, const T *F, int x, int y, int z, long long p, int mrow, T Ju[9]) {
+  const int pos[3] = {x, y, z};
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  const long long st[3] = {1, b.sy, b.sz};
+  const T ih[3] = {b.ihq, b.ihr, b.ihs};
+  for (int f = 0; f < 9; ++f) Ju[f] = 0;
+  for (int a = 0; a < 3; ++a) {
+    Row r;
+    sbp_row(pos[a], nn[a], b.lit, r);
+    const T *X = b.met + (long long)(mrow * 3 + a) * b.vol;
+    T sv[3] = {0, 0, 0};
+    T ss[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < r.cnt; ++k) {
+      long long q = p + (long long)r.off[k] * st[a];
+      T c = (T)r.c[k];
+      T JX = ld(b.J + q);
+      T Xq = ld(X + q);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) sv[f] = sv[f] + c * ld(F + f * b.vol + q);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) ss[f] = ss[f] + c * ld(F + (3 + f) * b.vol + q) * JX * Xq;
+    }
+    T Xp = ld(X + p);
+#pragma unroll
+    for (int f = 0; f < 3; ++f) Ju[f] = Ju[f] + ih[a] * (Xp * sv[f]);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) Ju[3 + f] = Ju[3 + f] + ih[a] * ss[f];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage kernel: one thread per grid point.
+// ---------------------------------------------------------------------------
+template <typename T, int MESH, int RESP>
+__global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (x > b.nx || y > b.ny || z > b.nz) return;
+  const long long p = pidx(b, x, y, z);
+  const long long V = b.vol;
+  const T *F = a.cur ? b.F1 : b.F0;
+  T *Fn = a.cur ? b.F0 : b.F1;
+  const double t0 = a.time ? a.time->t : 0.0;
+  const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
+
+  T df[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    T v = b.DF[c * V + p];
+    df[c] = (a.flags & F_SCALE) ? (T)a.A * v : v;
+  }
+  const bool interior = x >= b.lo[0] && x <= b.hi[0] && y >= b.lo[1] && y <= b.hi[1] && z >= b.lo[2] && z <= b.hi[2];
+  bool in_pml = false;
+  if (b.npml > 0) {
+    for (int f = 0; f < 6; ++f) {
+      if (!b.pml_on[f]) continue;
+      const int *B = b.pb[f];
+      if (x >= B[0] && x <= B[1] && y >= B[2] && y <= B[3] && z >= B[4] && z <= B[5]) in_pml = true;
+    }
+  }
+  // scale / integrate PML rates of points not reached by the RHS path
+  const bool rhs = (a.flags & F_RHS) != 0;
+
+  if (rhs && interior) {
+    // strict interior, src/JU_xJU_yJU_z6.f90:16177-16636
+    T DFx[9], DFy[9], DFz[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) { DFx[c] = 0; DFy[c] = 0; DFz[c] = 0; }
+    if (MESH == MESH_CART) {
+      const T mx = ld(b.mq + x), my = ld(b.mr + y), mz = ld(b.ms + z);
+#pragma unroll
+      for (int s = 1; s <= 3; ++s) {
+        const T ax = mx * b.cx[s - 1], ay = my * b.cy[s - 1], az = mz * b.cz[s - 1];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          const T *Fc = F + c * V;
+          DFx[c] = DFx[c] + ax * (ld(Fc + p + s) - ld(Fc + p - s));
+          DFy[c] = DFy[c] + ay * (ld(Fc + p + s * b.sy) - ld(Fc + p - s * b.sy));
+          DFz[c] = DFz[c] + az * (ld(Fc + p + s * b.sz) - ld(Fc + p - s * b.sz));
+        }
+      }
+    } else {
+      const T *met = b.met;
+      T mp[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) mp[k] = ld(met + k * V + p);
+#pragma unroll
+      for (int s = 1; s <= 3; ++s) {
+        const long long off[3] = {s, s * b.sy, s * b.sz};
+        const T cc[3] = {b.cx[s - 1], b.cy[s - 1], b.cz[s - 1]};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T *Fc = F + c * V;
+          T d0 = ld(Fc + p + off[0]) - ld(Fc + p - off[0]);
+          T d1 = ld(Fc + p + off[1]) - ld(Fc + p - off[1]);
+          T d2 = ld(Fc + p + off[2]) - ld(Fc + p - off[2]);
+          DFx[c] = DFx[c] + mp[0] * cc[0] * d0 + mp[1] * cc[1] * d1 + mp[2] * cc[2] * d2;
+          DFy[c] = DFy[c] + mp[3] * cc[0] * d0 + mp[4] * cc[1] * d1 + mp[5] * cc[2] * d2;
+          DFz[c] = DFz[c] + mp[6] * cc[0] * d0 + mp[7] * cc[1] * d1 + mp[8] * cc[2] * d2;
+        }
+        // conservative stress derivatives, J * metric at the neighbours
+        T jm[3][3][2];  // [row][axis][+/-]
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          long long qp_ = p + off[ax], qm_ = p - off[ax];
+          T Jp = ld(b.J + qp_), Jm = ld(b.J + qm_);
+#pragma unroll
+          for (int row = 0; row < 3; ++row) {
+            jm[row][ax][0] = Jp * ld(met + (row * 3 + ax) * V + qp_);
+            jm[row][ax][1] = Jm * ld(met + (row * 3 + ax) * V + qm_);
+          }
+        }
+#pragma unroll
+        for (int c = 3; c < 9; ++c) {
+          const T *Fc = F + c * V;
+          T fp0 = ld(Fc + p + off[0]), fm0 = ld(Fc + p - off[0]);
+          T fp1 = ld(Fc + p + off[1]), fm1 = ld(Fc + p - off[1]);
+          T fp2 = ld(Fc + p + off[2]), fm2 = ld(Fc + p - off[2]);
+          DFx[c] = DFx[c] + cc[0] * (fp0 * jm[0][0][0] - fm0 * jm[0][0][1]) + cc[1] * (fp1 * jm[0][1][0] - fm1 * jm[0][1][1]) +
+                   cc[2] * (fp2 * jm[0][2][0] - fm2 * jm[0][2][1]);
+          DFy[c] = DFy[c] + cc[0] * (fp0 * jm[1][0][0] - fm0 * jm[1][0][1]) + cc[1] * (fp1 * jm[1][1][0] - fm1 * jm[1][1][1]) +
+                   cc[2] * (fp2 * jm[1][2][0] - fm2 * jm[1][2][1]);
+          DFz[c] = DFz[c] + cc[0] * (fp0 * jm[2][0][0] - fm0 * jm[2][0][1]) + cc[1] * (fp1 * jm[2][1][0] - fm1 * jm[2][1][1]) +
+                   cc[2] * (fp2 * jm[2][2][0] - fm2 * jm[2][2][1]);
+        }
+      }
+    }
+    const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
+    const T a1 = MESH == MESH_CART ? (T)1 / rho : (T)1 / (rho * ld(b.J + p));
+    const T a2 = (T)2 * mu + lam, a3 = lam, a4 = mu;
+    df[0] = df[0] + a1 * (DFx[3] + DFy[6] + DFz[7]);
+    df[1] = df[1] + a1 * (DFx[6] + DFy[4] + DFz[8]);
+    df[2] = df[2] + a1 * (DFx[7] + DFy[8] + DFz[5]);
+    df[3] = df[3] + a2 * DFx[0] + a3 * (DFy[1] + DFz[2]);
+    df[4] = df[4] + a2 * DFy[1] + a3 * (DFx[0] + DFz[2]);
+    df[5] = df[5] + a2 * DFz[2] + a3 * (DFx[0] + DFy[1]);
+    df[6] = df[6] + a4 * (DFy[0] + DFx[1]);
+    df[7] = df[7] + a4 * (DFz[0] + DFx[2]);
+    df[8] = df[8] + a4 * (DFz[1] + DFy[2]);
+    if (RESP != RESP_EL) {
+      T e[6] = {DFx[0], DFy[1], DFz[2], DFy[0] + DFx[1], DFz[0] + DFx[2], DFz[1] + DFy[2]};
+      T tr = DFx[0] + DFy[1] + DFz[2];
+      anelastic_point<T, RESP>(b, a, x, y, z, p, e, tr, df, true);
+    }
+  } else if (rhs) {
+    // near boundaries and PML slabs, src/RHS_Interior.f90:136-281
+    T Ux[9], Uy[9], Uz[9];
+    const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
+    jju6_row<T>(b, F, x, y, z, p, 0, Ux);
+    jju6_row<T>(b, F, x, y, z, p, 1, Uy);
+    jju6_row<T>(b, F, x, y, z, p, 2, Uz);
+    const T J = ld(b.J + p);
+    const T rhoJ_inv = (T)1 / (rho * J);
+    const T lambda2mu = lam + (T)2 * mu;
+    T DU[9];
+    DU[0] = (Ux[3] + Uy[6] + Uz[7]) * rhoJ_inv;
+    DU[1] = (Ux[6] + Uy[4] + Uz[8]) * rhoJ_inv;
+    DU[2] = (Ux[7] + Uy[8] + Uz[5]) * rhoJ_inv;
+    DU[3] = lambda2mu * Ux[0] + lam * (Uy[1] + Uz[2]);
+    DU[4] = lambda2mu * Uy[1] + lam * (Ux[0] + Uz[2]);
+    DU[5] = lambda2mu * Uz[2] + lam * (Ux[0] + Uy[1]);
+    DU[6] = mu * (Uy[0] + Ux[1]);
+    DU[7] = mu * (Uz[0] + Ux[2]);
+    DU[8] = mu * (Uz[1] + Uy[2]);
+    if (RESP != RESP_EL) {
+      T e[6] = {Ux[0], Uy[1], Uz[2], Uy[0] + Ux[1], Uz[0] + Ux[2], Uz[1] + Uy[2]};
+      T tr;
+      if (in_pml && pml_strain_correction<T>(b, x, y, z, e)) tr = e[0] + e[1] + e[2];
+      else tr = Ux[0] + Uy[1] + Uz[2];
+      anelastic_point<T, RESP>(b, a, x, y, z, p, e, tr, DU, true);
+    }
+    if (in_pml) {
+      // scale the slab rates first (scale_rates runs before set_rates)
+      if (a.flags & F_SCALE) {
+        for (int f = 0; f < 6; ++f) {
+          if (!b.pml_on[f]) continue;
+          const int *B = b.pb[f];
+          if (x < B[0] || x > B[1] || y < B[2] || y > B[3] || z < B[4] || z > B[5]) continue;
+          long long q = (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+          for (int c = 0; c < 9; ++c) b.DQ[f][c * b.pvol[f] + q] = (T)a.A * b.DQ[f][c * b.pvol[f] + q];
+        }
+      }
+      pml_point<T, true>(b, a, x, y, z, p, Ux, Uy, Uz, rhoJ_inv, lambda2mu, J, DU);
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) df[c] = df[c] + DU[c];
+  } else {
+    // no RHS this pass: still scale point-local memory-variable / PML rates
+    if (RESP != RESP_EL && (a.flags & (F_SCALE | F_UPDATE))) {
+      T e[6] = {0, 0, 0, 0, 0, 0};
+      anelastic_point<T, RESP>(b, a, x, y, z, p, e, (T)0, df, false);
+    }
+    if (in_pml && (a.flags & F_SCALE)) {
+      for (int f = 0; f < 6; ++f) {
+        if (!b.pml_on[f]) continue;
+        const int *B = b.pb[f];
+        if (x < B[0] || x > B[1] || y < B[2] || y > B[3] || z < B[4] || z > B[5]) continue;
+        long long q = (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+        for (int c = 0; c < 9; ++c) b.DQ[f][c * b.pvol[f] + q] = (T)a.A * b.DQ[f][c * b.pvol[f] + q];
+      }
+    }
+  }
+
+  if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
+      z >= b.sbox[4] && z <= b.sbox[5])
+    add_sources<T, MESH>(b, tst, x, y, z, p, df);
+  if ((a.flags & F_SAT) && (x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz))
+    add_face_sats<T, MESH>(b, F, x, y, z, p, df, in_pml);
+  if ((a.flags & F_ISAT)) {
+    // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
+    int side = x == 1 ? 0 : (x == b.nx ? 1 : -1);
+    if (side >= 0 && b.isat[side]) {
+      const T pen = b.tau0 / b.hq;
+      long long fp = (long long)(y - 1) + (long long)b.ny * (z - 1);
+      long long fn = (long long)b.ny * b.nz;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) df[c] = df[c] - pen * b.isat[side][c * fn + fp];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) b.DF[c * V + p] = df[c];
+  if (a.flags & F_UPDATE) {
+    const T Bdt = (T)a.Bdt;
+    if (b.FC) {
+      // FP32: compensated (Kahan) accumulation of F
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        T f0 = F[c * V + p];
+        T comp = b.FC[c * V + p];
+        T yv = Bdt * df[c] - comp;
+        T tv = f0 + yv;
+        b.FC[c * V + p] = (tv - f0) - yv;
+        Fn[c * V + p] = tv;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Fn[c * V + p] = F[c * V + p] + Bdt * df[c];
+    }
+    if (in_pml) {
+      for (int f = 0; f < 6; ++f) {
+        if (!b.pml_on[f]) continue;
+        const int *B = b.pb[f];
+        if (x < B[0] || x > B[1] || y < B[2] || y > B[3] || z < B[4] || z > B[5]) continue;
+        long long q = (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+        for (int c = 0; c < 9; ++c) b.Q[f][c * b.pvol[f] + q] = b.Q[f][c * b.pvol[f] + q] + Bdt * b.DQ[f][c * b.pvol[f] + q];
+      }
+    }
+  }
+}
+
+// F <- F + dt*DF over every interior point (update_fields, split path): in place
+template <typename T>
+__global__ void k_update_inplace(Blk<T> b, int cur, double dt) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (x > b.nx || y > b.ny || z > b.nz) return;
+  const long long p = pidx(b, x, y, z);
+  T *F = cur ? b.F1 : b.F0;
+  const T d = (T)dt;
+  for (int c = 0; c < 9; ++c) F[c * b.vol + p] = F[c * b.vol + p] + d * b.DF[c * b.vol + p];
+}
+
+// rk_vector_openacc.f90:22-37 / :58-75 equivalents on flat device arrays
+__global__ void k_scale_array(double *r, long long n, double A) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long s = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += s) r[i] = A * r[i];
+}
+__global__ void k_axpy_array(double *x, const double *r, long long n, double dt) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long s = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += s) x[i] = x[i] + dt * r[i];
+}
+template <typename T>
+__global__ void k_scale_T(T *r, long long n, double A) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long s = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += s) r[i] = (T)A * r[i];
+}
+template <typename T>
+__global__ void k_axpy_T(T *x, const T *r, long long n, double dt) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long s = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += s) x[i] = x[i] + (T)dt * r[i];
+}
+
+// Receiver gather at the start of step n (stage 1, before the update) and
+// time advance at the end of a step.
+template <typename T>
+__global__ void k_sample(Blk<T> b, int cur, DevTime *tm, int w_stride, int increment) {
+  const T *F = cur ? b.F1 : b.F0;
+  int n = tm->n;
+  if (w_stride <= 0 || ((n - 1) % w_stride) != 0) return;
+  int s = tm->nsamp;
+  if (s < b.max_samples) {
+    for (int r = threadIdx.x; r < b.nrec; r += blockDim.x) {
+      double *o = b.seis + ((long long)s * b.nrec + r) * 4;
+      int i = b.ridx[3 * r], j = b.ridx[3 * r + 1], k = b.ridx[3 * r + 2];
+      o[0] = tm->t;
+      if (i > 0 && j > 0 && k > 0) {
+        long long p = pidx(b, i, j, k);
+        o[1] = (double)F[p];
+        o[2] = (double)F[b.vol + p];
+        o[3] = (double)F[2 * b.vol + p];
+      } else {
+        o[1] = o[2] = o[3] = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && increment) tm->nsamp = s + 1;
+}
+
+__global__ void k_advance(DevTime *tm, double dt) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    tm->t = tm->t + c_rkC[5] * dt;
+    tm->n = tm->n + 1;
+  }
+}
+
+// max |v| reduction (final-state diagnostics) with a non-finite flag
+template <typename T>
+__global__ void k_maxabs(const T *a, long long n, double *partial, int *nonfinite) {
+  __shared__ double sm[256];
+  double m = 0.0;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long s = (long long)gridDim.x * blockDim.x;
+  int bad = 0;
+  for (; i < n; i += s) {
+    double v = fabs((double)a[i]);
+    if (!(v <= 1.7976931348623157e308)) bad = 1;
+    else if (v > m) m = v;
+  }
+  sm[threadIdx.x] = m;
+  if (bad) atomicExch(nonfinite, 1);
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + k]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+}  // namespace wql3d

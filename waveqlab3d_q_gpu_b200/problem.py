@@ -132,6 +132,8 @@ class AnelasticParams:
     gamma: float = 0.0
     f_transition: float = 1.0
     coarse_grain: int = 0
+    coefficient_method: Optional[str] = None   # fQ8: 'conventional-nnls' or 'withers-2015'
+    weight_policy: Optional[str] = None        # fQ8: 'table-exact' or 'nonnegative-refit'
     tau: Optional[Sequence[float]] = None        # overrides the builders when given
     weight: Optional[Sequence[float]] = None
     strength_s: Optional[Sequence[float]] = None
