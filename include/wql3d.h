@@ -176,6 +176,22 @@ int wql3d_device_bytes(wql3d_domain *d, int64_t *bytes);
 int wql3d_kernel_launches(wql3d_domain *d, int64_t *launches);
 const char *wql3d_last_error(void);
 
+/* Allocation-free max|v| reduction over a device array.
+   No counterpart in the reference: it serves callers that cannot allocate GPU
+   memory when they need the diagnostic (for example a Fortran driver whose
+   device data is owned by fixed OpenACC data regions and audited for zero
+   allocations during time stepping).  The scratch is a static device array
+   inside libwql3d.so (1 MiB on every GPU that loads the library, held until
+   exit); the call allocates nothing.  array: device array of n doubles;
+   result and nonfinite: device-accessible outputs written on `stream`
+   (max |array[i]| and 1 if any element is NaN/Inf).  n may not exceed
+   WQL3D_NOALLOC_MAX_ELEMENTS (WQL3D_EINVAL otherwise).  The first call on a
+   device looks up the scratch address for that device, so make it before any
+   stream capture.  Calls whose kernels overlap on the GPU share the scratch
+   and race; calls ordered on one stream are safe. */
+#define WQL3D_NOALLOC_MAX_ELEMENTS (65536LL * 8192LL)
+int wql3d_max_abs_noalloc(const double *array, int64_t n, double *result, int32_t *nonfinite, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,7 @@ SIGNATURES = {
     "wql3d_device_bytes": [C.c_void_p, C.POINTER(C.c_int64)],
     "wql3d_kernel_launches": [C.c_void_p, C.POINTER(C.c_int64)],
     "wql3d_last_error": [],
+    "wql3d_max_abs_noalloc": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
 _LIB = None

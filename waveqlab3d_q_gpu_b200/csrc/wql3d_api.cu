@@ -111,6 +111,11 @@ struct Alloc {
 
 }  // namespace
 
+namespace wql3d {
+// lets other translation units of the library set the wql3d_last_error() text
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace wql3d
+
 struct HostBlock {
   int nq = 0, nr = 0, ns = 0;
   int mesh = 0;
