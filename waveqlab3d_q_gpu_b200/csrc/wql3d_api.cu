@@ -9,8 +9,10 @@
 #include "wql3d_device.cuh"
 #include "wql3d_iface.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -90,6 +92,7 @@ void host_row(int i, int n, int lit, int &cnt, int idx[8], double c[8]) {
 struct Alloc {
   std::vector<void *> ptrs;
   int64_t bytes = 0;
+  cudaStream_t stream = nullptr;  // zero-fills are ordered on the owning domain's stream
   template <typename P>
   cudaError_t get(P **p, size_t n, bool zero = true) {
     void *v = nullptr;
@@ -97,7 +100,13 @@ struct Alloc {
     if (nb == 0) nb = 16;
     cudaError_t e = cudaMalloc(&v, nb);
     if (e != cudaSuccess) return e;
-    if (zero) cudaMemset(v, 0, nb);
+    if (zero) {
+      e = cudaMemsetAsync(v, 0, nb, stream);
+      if (e != cudaSuccess) {
+        cudaFree(v);
+        return e;
+      }
+    }
     ptrs.push_back(v);
     bytes += (int64_t)nb;
     *p = (P *)v;
@@ -394,6 +403,28 @@ int setup_block(wql3d_domain *d, int bi) {
   }
   b.tau0 = (T)bd.tau0;
   for (int f = 0; f < 6; ++f) b.bc[f] = bd.bc[f];
+  {
+    // closure rows 1..6 and their right mirrors as (offset, coefficient),
+    // zero-padded to 8 taps, in the reference's summation order
+    std::vector<double> rc(12 * 8, 0.0);
+    std::vector<int> ro(12 * 8, 0);
+    for (int r = 0; r < 6; ++r)
+      for (int k = 0; k < kSbpCnt[r]; ++k) {
+        rc[r * 8 + k] = kSbpC[b.lit][r][k];
+        ro[r * 8 + k] = kSbpIdx[r][k] - (r + 1);
+        rc[(6 + r) * 8 + k] = -kSbpC[b.lit][r][k];
+        ro[(6 + r) * 8 + k] = (r + 1) - kSbpIdx[r][k];
+      }
+    double *drc;
+    int *dro;
+    CK(d->mem.get(&drc, rc.size()));
+    CK(d->mem.get(&dro, ro.size()));
+    CK(cudaMemcpyAsync(drc, rc.data(), sizeof(double) * rc.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(dro, ro.data(), sizeof(int) * ro.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    b.rowc = drc;
+    b.rowo = dro;
+  }
   // strict interior bounds, src/JU_xJU_yJU_z6.f90:16158-16173
   int np = bd.npml;
   int ix = bd.pml[0] ? std::max(np, 6) : 6, fx = bd.pml[1] ? std::max(np, 6) : 6;
@@ -642,11 +673,83 @@ int setup_block(wql3d_domain *d, int bi) {
   return WQL3D_OK;
 }
 
+// tuning of the Cartesian interior kernel (tile height TY, z-chunk length)
+struct Tuning {
+  int ty = 4;
+  int zchunk = 12;
+  int generic = 0;   // 1: every point through the generic per-point kernel
+  int split = 1;     // interior: two warp groups (velocity / stress rates) with register z-queues
+};
+
+Tuning tuning() {
+  static Tuning t = [] {
+    Tuning r;
+    if (const char *e = getenv("WQL3D_TY")) r.ty = atoi(e) == 8 ? 8 : 4;
+    if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = std::max(1, atoi(e));
+    if (const char *e = getenv("WQL3D_KERNEL")) {
+      r.generic = strcmp(e, "generic") == 0;
+      if (strcmp(e, "ring") == 0) r.split = 0;
+    }
+    return r;
+  }();
+  return t;
+}
+
+template <typename T, int RESP>
+void launch_interior_cart(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
+  Tuning tu = tuning();
+  int nxi = b.hi[0] - b.lo[0] + 1, nyi = b.hi[1] - b.lo[1] + 1, nzi = b.hi[2] - b.lo[2] + 1;
+  if (nxi <= 0 || nyi <= 0 || nzi <= 0) return;
+  if (tu.split) {
+    dim3 gr((nxi + 31) / 32, (nyi + tu.ty - 1) / tu.ty, (nzi + tu.zchunk - 1) / tu.zchunk);
+    if (tu.ty == 8) {
+      size_t sm = SplitSmem<T, 8>::bytes;
+      cudaFuncSetAttribute(k_interior_split<T, RESP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_interior_split<T, RESP, 8><<<gr, 512, sm, d->stream>>>(b, a, tu.zchunk);
+    } else {
+      size_t sm = SplitSmem<T, 4>::bytes;
+      cudaFuncSetAttribute(k_interior_split<T, RESP, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_interior_split<T, RESP, 4><<<gr, 256, sm, d->stream>>>(b, a, tu.zchunk);
+    }
+    d->launches++;
+    return;
+  }
+  dim3 gr((nxi + 31) / 32, (nyi + tu.ty - 1) / tu.ty, (nzi + tu.zchunk - 1) / tu.zchunk);
+  if (tu.ty == 8) {
+    size_t sm = InteriorSmem<T, 8>::bytes;
+    cudaFuncSetAttribute(k_interior_cart<T, RESP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_interior_cart<T, RESP, 8><<<gr, dim3(32, 8), sm, d->stream>>>(b, a, tu.zchunk);
+  } else {
+    size_t sm = InteriorSmem<T, 4>::bytes;
+    cudaFuncSetAttribute(k_interior_cart<T, RESP, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_interior_cart<T, RESP, 4><<<gr, dim3(32, 4), sm, d->stream>>>(b, a, tu.zchunk);
+  }
+  d->launches++;
+}
+
+template <typename T, int MESH, int RESP>
+void launch_shell(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
+  long long n = shell_count(b);
+  if (n <= 0) return;
+  k_shell<T, MESH, RESP><<<(unsigned)((n + 127) / 128), 128, 0, d->stream>>>(b, a, (int)n);
+  d->launches++;
+}
+
 template <typename T>
-void launch_stage(wql3d_domain *d, int bi, const StageArgs &a) {
+void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = false) {
   Blk<T> &b = blk<T>(d, bi);
-  dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
   int mesh = d->hb[bi].mesh;
+  if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !tuning().generic) {
+    // strict interior (z-marching kernel) + near-boundary shell
+    switch (d->response) {
+      case 0: launch_interior_cart<T, RESP_EL>(d, b, a); launch_shell<T, MESH_CART, RESP_EL>(d, b, a); break;
+      case 1: launch_interior_cart<T, RESP_Q4>(d, b, a); launch_shell<T, MESH_CART, RESP_Q4>(d, b, a); break;
+      case 2: launch_interior_cart<T, RESP_Q8>(d, b, a); launch_shell<T, MESH_CART, RESP_Q8>(d, b, a); break;
+      default: launch_interior_cart<T, RESP_FQ8>(d, b, a); launch_shell<T, MESH_CART, RESP_FQ8>(d, b, a); break;
+    }
+    return;
+  }
+  dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
   switch (d->response * 2 + mesh) {
     case 0: k_stage<T, MESH_CART, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
     case 1: k_stage<T, MESH_CURV, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
@@ -674,7 +777,7 @@ int enqueue_stage(wql3d_domain *d, int stage, double dt, int flags) {
     launch_iface<T>(d->iface, blk<T>(d, 0), blk<T>(d, 1), a, d->stream);
     d->launches++;
   }
-  for (int i = 0; i < d->nblocks; ++i) launch_stage<T>(d, i, a);
+  for (int i = 0; i < d->nblocks; ++i) launch_stage<T>(d, i, a, true);
   if (flags & F_UPDATE) {
     if (d->has_iface) {
       launch_iface_update<T>(d->iface, a, d->stream);
@@ -741,7 +844,9 @@ int run_steps(wql3d_domain *d, double dt, int nsteps, int w_stride) {
       // counting pass without launching: mirror enqueue_step's structure
       for (int k = 0; k < 2; ++k) {
         for (int i = 0; i < d->nblocks; ++i) per_pair += d->hb[i].nrec > 0 ? 1 : 0;
-        per_pair += 5 * (d->nblocks + (d->has_iface ? 2 : 0)) + 1;
+        int per_block = 0;
+        for (int i = 0; i < d->nblocks; ++i) per_block += d->hb[i].mesh == WQL3D_MESH_CARTESIAN ? 2 : 1;
+        per_pair += 5 * (per_block + (d->has_iface ? 2 : 0)) + 1;
       }
       d->launches = l0;
       d->cur = cur0;
@@ -828,6 +933,7 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     delete d;
     return fail(WQL3D_ECUDA, "stream creation failed");
   }
+  d->mem.stream = d->stream;
   auto cleanup = [&](int code) {
     cudaStreamSynchronize(d->stream);
     d->mem.release();
@@ -837,7 +943,9 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
   };
   if (d->mem.get(&d->time, 1) != cudaSuccess) return cleanup(fail(WQL3D_ENOMEM, "time"));
   DevTime t0 = {0.0, 1, 0};
-  cudaMemcpy(d->time, &t0, sizeof(t0), cudaMemcpyHostToDevice);
+  if (cudaMemcpyAsync(d->time, &t0, sizeof(t0), cudaMemcpyHostToDevice, d->stream) != cudaSuccess ||
+      cudaStreamSynchronize(d->stream) != cudaSuccess)
+    return cleanup(fail(WQL3D_ECUDA, "time init"));
   if (d->mem.get(&d->red, 592) != cudaSuccess || d->mem.get(&d->flag, 1) != cudaSuccess)
     return cleanup(fail(WQL3D_ENOMEM, "reduction scratch"));
   for (int i = 0; i < d->nblocks; ++i) {
@@ -937,10 +1045,12 @@ int wql3d_get_metrics(wql3d_domain *d, int bi, double *out) {
                                  : (d->fp32 ? (const void *)d->bf[bi].ms : (const void *)d->bd[bi].ms);
       if (d->fp32) {
         std::vector<float> tmp((size_t)nn[a] + 1);
-        CK(cudaMemcpy(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, d->stream));
+        CK(cudaStreamSynchronize(d->stream));
         for (size_t i = 0; i < tmp.size(); ++i) m[a][i] = tmp[i];
       } else {
-        CK(cudaMemcpy(m[a].data(), src, sizeof(double) * m[a].size(), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(m[a].data(), src, sizeof(double) * m[a].size(), cudaMemcpyDeviceToHost, d->stream));
+        CK(cudaStreamSynchronize(d->stream));
       }
     }
     memset(out, 0, sizeof(double) * 10 * n1);

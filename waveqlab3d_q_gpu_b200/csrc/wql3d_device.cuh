@@ -39,6 +39,17 @@ __constant__ int c_sbp_cnt[6];
 __constant__ int c_sbp_idx[6][8];
 __constant__ double c_sbp_c[2][6][8];
 
+// 9-point discrete delta weights for alpha = 0, 25, 50, 100 (src/moment_tensor.f90:976-1121)
+__constant__ double c_delta9[4][9] = {
+    {-0.01171875, -0.03125, 0.046875, 0.28125, 0.4296875, 0.28125, 0.046875, -0.03125, -0.01171875},
+    {-0.00246875, -0.02275, -0.014125, 0.16575, 0.4171875, 0.38675, 0.117875, -0.02975, -0.01846875},
+    {-0.00728125, -0.028, 0.014875, 0.224, 0.4265625, 0.336, 0.081375, -0.032, -0.01553125},
+    {-0.0095625, -0.02990625, 0.03053125, 0.25284375, 0.42890625, 0.30903125, 0.06384375, -0.03196875, -0.01371875}};
+
+// F components staged in the interior kernel's shared plane / z-ring
+__constant__ int c_smf[8] = {0, 1, 2, 3, 4, 6, 7, 8};
+__constant__ int c_qf[6] = {0, 1, 2, 5, 7, 8};
+
 struct DevSource {
   int type;
   int near[3];
@@ -72,6 +83,8 @@ struct Blk {
   T ihq, ihr, ihs;      // 1/h
   T cx[3], cy[3], cz[3];// interior coefficients c/h
   int lit;              // SBP literal precision (index into c_sbp_c)
+  const double *rowc;   // closure rows 0..11 (left 1..6, right n..n-5): 8 signed coefficients each
+  const int *rowo;      // matching tap offsets relative to the point
   // PML slabs (faces 0..5): box and Q / DQ (9 components each, slab-local)
   int npml;
   int pml_on[6];
@@ -190,14 +203,11 @@ __device__ inline double singular_source(int i, int i0, double h, double a, int 
     if (i == i0 + 2) return gap / h;
     return 0.0;
   }
-  const double w0[9] = {-0.01171875, -0.03125, 0.046875, 0.28125, 0.4296875, 0.28125, 0.046875, -0.03125, -0.01171875};
-  const double w25[9] = {-0.00246875, -0.02275, -0.014125, 0.16575, 0.4171875, 0.38675, 0.117875, -0.02975, -0.01846875};
-  const double w50[9] = {-0.00728125, -0.028, 0.014875, 0.224, 0.4265625, 0.336, 0.081375, -0.032, -0.01553125};
-  const double w100[9] = {-0.0095625, -0.02990625, 0.03053125, 0.25284375, 0.42890625, 0.30903125, 0.06384375, -0.03196875, -0.01371875};
   int k = i - i0;
   if (k < -4 || k > 4) return 0.0;
-  const double *w = alpha == 0 ? w0 : alpha == 25 ? w25 : alpha == 50 ? w50 : alpha == 100 ? w100 : nullptr;
-  if (!w) return 0.0;
+  int row = alpha == 0 ? 0 : alpha == 25 ? 1 : alpha == 50 ? 2 : alpha == 100 ? 3 : -1;
+  if (row < 0) return 0.0;
+  const double *w = c_delta9[row];
   return w[k + 4] / h;
 }
 
@@ -528,15 +538,79 @@ __device__ void jju6_row(const Blk<T> &b, const T *F, int x, int y, int z, long 
   }
 }
 
+// One tap of the near-boundary operator for all three metric rows:
+// velocities accumulate sum c*F; stresses accumulate ((c*F)*J)*X_row,a per row
+// (the reference's association, src/JU_xJU_yJU_z6.f90:52-68).
+template <typename T>
+__device__ __forceinline__ void jju_tap(const Blk<T> &b, const T *F, long long q, int a, T c, T sv[3], T acc[3][6]) {
+  const long long V = b.vol;
+  const T Jq = ld(b.J + q);
+  const T X0 = ld(b.met + (long long)(0 * 3 + a) * V + q);
+  const T X1 = ld(b.met + (long long)(1 * 3 + a) * V + q);
+  const T X2 = ld(b.met + (long long)(2 * 3 + a) * V + q);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) sv[f] = sv[f] + c * ld(F + f * V + q);
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const T cFJ = c * ld(F + (3 + f) * V + q) * Jq;
+    acc[0][f] = acc[0][f] + cFJ * X0;
+    acc[1][f] = acc[1][f] + cFJ * X1;
+    acc[2][f] = acc[2][f] + cFJ * X2;
+  }
+}
+
+// Near-boundary derivatives of all nine fields for the three metric rows:
+// U[row][f] = JJU_x6 with X = metricx / metricy / metricz (src/JU_xJU_yJU_z6.f90:12-809).
+template <typename T>
+__device__ void jju6_all(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T U[3][9]) {
+  const int pos[3] = {x, y, z};
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  const long long st[3] = {1, b.sy, b.sz};
+  const T ih[3] = {b.ihq, b.ihr, b.ihs};
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int f = 0; f < 9; ++f) U[r][f] = 0;
+#pragma unroll 1
+  for (int a = 0; a < 3; ++a) {
+    T sv[3] = {0, 0, 0};
+    T acc[3][6];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int f = 0; f < 6; ++f) acc[r][f] = 0;
+    const int i = pos[a], n = nn[a];
+    if (i >= 7 && i <= n - 6) {
+      const T cc[6] = {(T)(-1.0 / 60.0), (T)0.15, (T)-0.75, (T)0.75, (T)-0.15, (T)(1.0 / 60.0)};
+      const int off[6] = {-3, -2, -1, 1, 2, 3};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) jju_tap(b, F, p + (long long)off[k] * st[a], a, cc[k], sv, acc);
+    } else {
+      const int row = i <= 6 ? i - 1 : 6 + (n - i);
+      const double *rc = b.rowc + row * 8;
+      const int *ro = b.rowo + row * 8;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const T c = (T)__ldg(rc + k);
+        if (c != (T)0) jju_tap(b, F, p + (long long)__ldg(ro + k) * st[a], a, c, sv, acc);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const T Xp = ld(b.met + (long long)(r * 3 + a) * b.vol + p);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) U[r][f] = U[r][f] + ih[a] * (Xp * sv[f]);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) U[r][3 + f] = U[r][3 + f] + ih[a] * acc[r][f];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Stage kernel: one thread per grid point.
 // ---------------------------------------------------------------------------
 template <typename T, int MESH, int RESP>
-__global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (x > b.nx || y > b.ny || z > b.nz) return;
+__device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, int z) {
   const long long p = pidx(b, x, y, z);
   const long long V = b.vol;
   const T *F = a.cur ? b.F1 : b.F0;
@@ -647,9 +721,12 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
     // near boundaries and PML slabs, src/RHS_Interior.f90:136-281
     T Ux[9], Uy[9], Uz[9];
     const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
-    jju6_row<T>(b, F, x, y, z, p, 0, Ux);
-    jju6_row<T>(b, F, x, y, z, p, 1, Uy);
-    jju6_row<T>(b, F, x, y, z, p, 2, Uz);
+    {
+      T U[3][9];
+      jju6_all<T>(b, F, x, y, z, p, U);
+#pragma unroll
+      for (int f = 0; f < 9; ++f) { Ux[f] = U[0][f]; Uy[f] = U[1][f]; Uz[f] = U[2][f]; }
+    }
     const T J = ld(b.J + p);
     const T rhoJ_inv = (T)1 / (rho * J);
     const T lambda2mu = lam + (T)2 * mu;
@@ -747,6 +824,484 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
       }
     }
   }
+}
+
+template <typename T, int MESH, int RESP>
+__global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (x > b.nx || y > b.ny || z > b.nz) return;
+  point_update<T, MESH, RESP>(b, a, x, y, z);
+}
+
+// Number of near-boundary (shell) points: everything outside the strict
+// interior box, split into z-slabs, y-slabs of the middle planes and x-slabs
+// of the middle rows.
+template <typename T>
+__host__ __device__ inline long long shell_count(const Blk<T> &b) {
+  long long nx = b.nx, ny = b.ny;
+  long long zlo = b.lo[2] - 1, zhi = b.nz - b.hi[2], nzm = b.hi[2] - b.lo[2] + 1;
+  long long nym = b.hi[1] - b.lo[1] + 1;
+  long long plane = nx * (b.lo[1] - 1) + nx * (b.ny - b.hi[1]) + nym * ((b.lo[0] - 1) + (b.nx - b.hi[0]));
+  return nx * ny * (zlo + zhi) + (nzm > 0 ? nzm : 0) * plane;
+}
+
+template <typename T>
+__device__ inline void shell_decode(const Blk<T> &b, int idx, int &x, int &y, int &z) {
+  const int nx = b.nx, nxy = b.nx * b.ny;
+  const int n_zlo = nxy * (b.lo[2] - 1), n_zhi = nxy * (b.nz - b.hi[2]);
+  if (idx < n_zlo) {
+    z = 1 + idx / nxy; int r = idx - (z - 1) * nxy; y = 1 + r / nx; x = 1 + r - (y - 1) * nx;
+    return;
+  }
+  idx -= n_zlo;
+  if (idx < n_zhi) {
+    int zz = idx / nxy; z = b.hi[2] + 1 + zz; int r = idx - zz * nxy; y = 1 + r / nx; x = 1 + r - (y - 1) * nx;
+    return;
+  }
+  idx -= n_zhi;
+  const int ylo = nx * (b.lo[1] - 1), yhi = nx * (b.ny - b.hi[1]);
+  const int wx = (b.lo[0] - 1) + (b.nx - b.hi[0]);
+  const int nym = b.hi[1] - b.lo[1] + 1;
+  const int plane = ylo + yhi + nym * wx;
+  int zz = idx / plane;
+  z = b.lo[2] + zz;
+  int r = idx - zz * plane;
+  if (r < ylo) { y = 1 + r / nx; x = 1 + r - (y - 1) * nx; return; }
+  r -= ylo;
+  if (r < yhi) { int yy = r / nx; y = b.hi[1] + 1 + yy; x = 1 + r - yy * nx; return; }
+  r -= yhi;
+  int yy = r / wx;
+  y = b.lo[1] + yy;
+  int c = r - yy * wx;
+  x = c < (b.lo[0] - 1) ? 1 + c : b.hi[0] + 1 + (c - (b.lo[0] - 1));
+}
+
+template <typename T, int MESH, int RESP>
+__global__ void __launch_bounds__(128, 3) k_shell(Blk<T> b, StageArgs a, int count) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= count) return;
+  int x, y, z;
+  shell_decode(b, idx, x, y, z);
+  point_update<T, MESH, RESP>(b, a, x, y, z);
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous global -> shared copies (sm_80+ cp.async, still the lightest
+// path for element-granular halo gathers on sm_100a).  src_size 0 zero-fills.
+// ---------------------------------------------------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  int sz = valid ? BYTES : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gsrc), "n"(BYTES), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
+// Strict interior of a Cartesian block, src/JU_xJU_yJU_z6.f90:16426-16636,
+// fused with scale, sources and the RK update.  2.5-D: a block owns a
+// 32 x TY column tile and marches up a z-chunk.  x- and y-derivatives come
+// from a shared-memory plane with 3-point halos, double-buffered and filled
+// one plane ahead with cp.async; z-derivatives from a per-thread ring of
+// eight planes (six fields) in shared memory, also fed one plane ahead.
+// Every F value leaves HBM once per tile; halo re-reads hit L2.
+// smem plane fields: 0 vx 1 vy 2 vz 3 sxx 4 syy 5 sxy 6 sxz 7 syz
+// ring fields:       0 vx 1 vy 2 vz 3 szz 4 sxz 5 syz
+// ---------------------------------------------------------------------------
+template <typename T, int TY>
+struct InteriorSmem {
+  static constexpr int VEC = 16 / (int)sizeof(T);                  // elements per 16-byte cp.async
+  static constexpr int W = ((38 + VEC - 1 + VEC - 1) / VEC) * VEC;  // haloed row, whole chunks
+  static constexpr int H = TY + 6, NT = 32 * TY, RING = 8;
+  static constexpr int CH = W / VEC;                                // chunks per row
+  static constexpr size_t plane_elems = (size_t)8 * H * W;
+  static constexpr size_t bytes = sizeof(T) * (2 * plane_elems + (size_t)RING * 6 * NT);
+};
+
+template <typename T, int RESP, int TY>
+__global__ void __launch_bounds__(32 * TY, (TY == 4 ? 2 : 1)) k_interior_cart(Blk<T> b, StageArgs a, int zchunk) {
+  using SM = InteriorSmem<T, TY>;
+  constexpr int W = SM::W, H = SM::H, NT = SM::NT, RING = SM::RING, VEC = SM::VEC, CH = SM::CH;
+  constexpr int NPOS = H * CH, PPT = (NPOS + NT - 1) / NT;  // 16-byte chunk positions per plane field
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T (*S)[8][H][W] = reinterpret_cast<T (*)[8][H][W]>(smraw);                       // [2] haloed planes
+  T (*Z)[6][NT] = reinterpret_cast<T (*)[6][NT]>(smraw + sizeof(T) * 2 * SM::plane_elems);  // ring
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * 32 + tx;
+  const int x0 = b.lo[0] + blockIdx.x * 32;
+  const int y0 = b.lo[1] + blockIdx.y * TY;
+  const int zs = b.lo[2] + blockIdx.z * zchunk;
+  if (zs > b.hi[2]) return;
+  const int ze = min(zs + zchunk - 1, b.hi[2]);
+  const int x = x0 + tx, y = y0 + ty;
+  const bool active = x <= b.hi[0] && y <= b.hi[1];
+  const long long V = b.vol;
+  const T *F = a.cur ? b.F1 : b.F0;
+  T *Fn = a.cur ? b.F0 : b.F1;
+  const double t0 = a.time ? a.time->t : 0.0;
+  const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
+  const long long pc = pidx(b, min(x, b.nx), min(y, b.ny), zs);  // this thread's column (clamped)
+  // the haloed row starts at x0-3 rounded down to a 16-byte boundary of the
+  // padded row; sh is the resulting shift of x0-3 inside the shared row
+  const long long row0 = pidx(b, x0 - 3, y0 - 3, zs);             // element offset of (x0-3, y0-3, zs)
+  const int sh = (int)(row0 % VEC);
+  const long long base0 = row0 - sh;                               // 16-byte aligned
+  const long long rowlen = b.sy;                                   // padded row length
+  const long long rowstart0 = base0 - ((base0 % b.sz) % b.sy);     // start of the padded row of base0
+  // per-thread chunk positions of one plane field (identical for every plane and field)
+  int soff[PPT];
+  long long goff[PPT];
+  bool gok[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    int pos = tid + k * NT;
+    int yy = pos / CH, ch = pos - yy * CH;
+    soff[k] = yy * W + ch * VEC;
+    goff[k] = (long long)yy * b.sy + (long long)ch * VEC;
+    long long inrow = base0 - rowstart0 + (long long)ch * VEC;     // element index within the padded row
+    gok[k] = pos < NPOS && (y0 - 3 + yy) <= b.ny + 3 && inrow + VEC <= rowlen;
+  }
+  auto fill = [&](int zz, int buf) {
+    const long long plane0 = base0 + (long long)(zz - zs) * b.sz;
+    T *dst = &S[buf][0][0][0];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      const T *srcf = F + c_smf[f] * V + plane0;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k)
+        if (tid + k * NT < NPOS) cp_async<16>(dst + f * H * W + soff[k], gok[k] ? srcf + goff[k] : F, gok[k]);
+    }
+  };
+  auto ring = [&](int zz) {  // plane zz of the six ring fields into its slot
+    const long long pz = pc + (long long)(zz - zs) * b.sz;
+    const int slot = (zz - zs + 3 + RING) % RING;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) cp_async<sizeof(T)>(&Z[slot][f][tid], F + c_qf[f] * V + pz, true);
+  };
+
+  // prime: planes zs-3 .. zs+3 of the ring, haloed plane zs
+#pragma unroll 1
+  for (int zz = zs - 3; zz <= zs + 3; ++zz) ring(zz);
+  fill(zs, 0);
+  cp_async_commit();
+  T dfo[9], lam = 0, mu = 0, rho = 1;
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dfo[c] = b.DF[c * V + pc];
+    lam = b.M[pc]; mu = b.M[V + pc]; rho = b.M[2 * V + pc];
+  }
+  const T mx = active ? ld(b.mq + x) : (T)0, my = active ? ld(b.mr + y) : (T)0;
+
+  for (int z = zs; z <= ze; ++z) {
+    const int i = z - zs;
+    const int buf = i & 1;
+    const long long p = pc + (long long)i * b.sz;
+    cp_async_wait_all();
+    __syncthreads();  // plane z and ring plane z+3 resident; buffer buf^1 free
+    if (z + 1 <= ze) {
+      fill(z + 1, buf ^ 1);
+      ring(z + 4);
+    }
+    cp_async_commit();
+    // next step's rates and material (plain loads, consumed one step later)
+    T dfn[9], lamn = 0, mun = 0, rhon = 1;
+    if (active && z + 1 <= ze) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) dfn[c] = b.DF[c * V + p + b.sz];
+      lamn = b.M[p + b.sz]; mun = b.M[V + p + b.sz]; rhon = b.M[2 * V + p + b.sz];
+    }
+    if (active) {
+      const T mz = ld(b.ms + z);
+      const int sp1 = (i + 4) % RING, sp2 = (i + 5) % RING, sp3 = (i + 6) % RING;
+      const int sm1 = (i + 2) % RING, sm2 = (i + 1) % RING, sm3 = i % RING, s0 = (i + 3) % RING;
+      const T(*P)[H][W] = S[buf];
+#define DX(f) (((T)0 + (mx * b.cx[0]) * (P[f][ty + 3][tx + sh + 4] - P[f][ty + 3][tx + sh + 2])) + \
+               (mx * b.cx[1]) * (P[f][ty + 3][tx + sh + 5] - P[f][ty + 3][tx + sh + 1])) + \
+              (mx * b.cx[2]) * (P[f][ty + 3][tx + sh + 6] - P[f][ty + 3][tx + sh + 0])
+#define DY(f) (((T)0 + (my * b.cy[0]) * (P[f][ty + 4][tx + sh + 3] - P[f][ty + 2][tx + sh + 3])) + \
+               (my * b.cy[1]) * (P[f][ty + 5][tx + sh + 3] - P[f][ty + 1][tx + sh + 3])) + \
+              (my * b.cy[2]) * (P[f][ty + 6][tx + sh + 3] - P[f][ty + 0][tx + sh + 3])
+#define DZ(k) (((T)0 + (mz * b.cz[0]) * (Z[sp1][k][tid] - Z[sm1][k][tid])) + \
+               (mz * b.cz[1]) * (Z[sp2][k][tid] - Z[sm2][k][tid])) + \
+              (mz * b.cz[2]) * (Z[sp3][k][tid] - Z[sm3][k][tid])
+      T df[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) df[c] = (a.flags & F_SCALE) ? (T)a.A * dfo[c] : dfo[c];
+      const T a1 = (T)1 / rho, a2 = (T)2 * mu + lam, a3 = lam, a4 = mu;
+      const T vxx = DX(0), vyx = DX(1), vzx = DX(2);
+      const T vxy = DY(0), vyy = DY(1), vzy = DY(2);
+      const T vxz = DZ(0), vyz = DZ(1), vzz = DZ(2);
+      df[0] = df[0] + a1 * (DX(3) + DY(5) + DZ(4));
+      df[1] = df[1] + a1 * (DX(5) + DY(4) + DZ(5));
+      df[2] = df[2] + a1 * (DX(6) + DY(7) + DZ(3));
+      df[3] = df[3] + a2 * vxx + a3 * (vyy + vzz);
+      df[4] = df[4] + a2 * vyy + a3 * (vxx + vzz);
+      df[5] = df[5] + a2 * vzz + a3 * (vxx + vyy);
+      df[6] = df[6] + a4 * (vxy + vyx);
+      df[7] = df[7] + a4 * (vxz + vzx);
+      df[8] = df[8] + a4 * (vyz + vzy);
+#undef DX
+#undef DY
+#undef DZ
+      if (RESP != RESP_EL) {
+        T e[6] = {vxx, vyy, vzz, vxy + vyx, vxz + vzx, vyz + vzy};
+        T tr = vxx + vyy + vzz;
+        anelastic_point<T, RESP>(b, a, x, y, z, p, e, tr, df, true);
+      }
+      if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] &&
+          y <= b.sbox[3] && z >= b.sbox[4] && z <= b.sbox[5])
+        add_sources<T, MESH_CART>(b, tst, x, y, z, p, df);
+#pragma unroll
+      for (int c = 0; c < 9; ++c) b.DF[c * V + p] = df[c];
+      if (a.flags & F_UPDATE) {
+        const T Bdt = (T)a.Bdt;
+        T fc[9];
+        fc[0] = Z[s0][0][tid]; fc[1] = Z[s0][1][tid]; fc[2] = Z[s0][2][tid];
+        fc[3] = P[3][ty + 3][tx + sh + 3]; fc[4] = P[4][ty + 3][tx + sh + 3]; fc[5] = Z[s0][3][tid];
+        fc[6] = P[5][ty + 3][tx + sh + 3]; fc[7] = Z[s0][4][tid]; fc[8] = Z[s0][5][tid];
+        if (b.FC) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) {
+            T comp = b.FC[c * V + p];
+            T yv = Bdt * df[c] - comp;
+            T tv = fc[c] + yv;
+            b.FC[c * V + p] = (tv - fc[c]) - yv;
+            Fn[c * V + p] = tv;
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) Fn[c * V + p] = fc[c] + Bdt * df[c];
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) dfo[c] = dfn[c];
+    lam = lamn; mu = mun; rho = rhon;
+  }
+  cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+// Strict interior of a Cartesian block, two warp groups per tile.
+// Same arithmetic as k_interior_cart (src/JU_xJU_yJU_z6.f90:16426-16636), but
+// the nine outputs of a point are split: warps of group V (velocity rates)
+// need z-derivatives of s_xz, s_yz, s_zz, warps of group S (stress rates) of
+// v_x, v_y, v_z, so each thread's seven-plane z-queue is three fields and
+// lives in registers.  Shared memory holds only the double-buffered haloed
+// x-y plane, filled one plane ahead with 16-byte cp.async.
+// ---------------------------------------------------------------------------
+template <typename T, int TY>
+struct SplitSmem {
+  static constexpr int VEC = 16 / (int)sizeof(T);
+  static constexpr int W = ((38 + VEC - 1 + VEC - 1) / VEC) * VEC;
+  static constexpr int H = TY + 6, NP = 32 * TY, CH = W / VEC;
+  static constexpr size_t plane_elems = (size_t)8 * H * W;
+  static constexpr size_t bytes = sizeof(T) * 2 * plane_elems;
+};
+
+template <typename T, int RESP, int TY>
+__global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(Blk<T> b, StageArgs a, int zchunk) {
+  using SM = SplitSmem<T, TY>;
+  constexpr int W = SM::W, H = SM::H, NP = SM::NP, VEC = SM::VEC, CH = SM::CH;
+  constexpr int NT = 2 * NP;                                 // threads per block
+  constexpr int NPOS = H * CH, PPT = (NPOS + NT - 1) / NT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T (*S)[8][H][W] = reinterpret_cast<T (*)[8][H][W]>(smraw);
+  const int tid = threadIdx.x;
+  const bool gS = tid >= NP;                                 // stress-rate group
+  const int lt = gS ? tid - NP : tid;
+  const int tx = lt & 31, ty = lt >> 5;
+  const int x0 = b.lo[0] + blockIdx.x * 32;
+  const int y0 = b.lo[1] + blockIdx.y * TY;
+  const int zs = b.lo[2] + blockIdx.z * zchunk;
+  if (zs > b.hi[2]) return;
+  const int ze = min(zs + zchunk - 1, b.hi[2]);
+  const int x = x0 + tx, y = y0 + ty;
+  const bool active = x <= b.hi[0] && y <= b.hi[1];
+  const long long V = b.vol;
+  const T *F = a.cur ? b.F1 : b.F0;
+  T *Fn = a.cur ? b.F0 : b.F1;
+  const double t0 = a.time ? a.time->t : 0.0;
+  const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
+  const long long pc = pidx(b, min(x, b.nx), min(y, b.ny), zs);
+  const long long row0 = pidx(b, x0 - 3, y0 - 3, zs);
+  const int sh = (int)(row0 % VEC);
+  const long long base0 = row0 - sh;
+  const long long rowstart0 = base0 - ((base0 % b.sz) % b.sy);
+  int soff[PPT];
+  long long goff[PPT];
+  bool gok[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; ++k) {
+    int pos = tid + k * NT;
+    int yy = pos / CH, ch = pos - yy * CH;
+    soff[k] = yy * W + ch * VEC;
+    goff[k] = (long long)yy * b.sy + (long long)ch * VEC;
+    long long inrow = base0 - rowstart0 + (long long)ch * VEC;
+    gok[k] = pos < NPOS && (y0 - 3 + yy) <= b.ny + 3 && inrow + VEC <= b.sy;
+  }
+  auto fill = [&](int zz, int buf) {
+    const long long plane0 = base0 + (long long)(zz - zs) * b.sz;
+    T *dst = &S[buf][0][0][0];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      const T *srcf = F + c_smf[f] * V + plane0;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k)
+        if (tid + k * NT < NPOS) cp_async<16>(dst + f * H * W + soff[k], gok[k] ? srcf + goff[k] : F, gok[k]);
+    }
+  };
+  // z-queue fields: group V -> s_zz, s_xz, s_yz (F 5, 7, 8); group S -> v_x, v_y, v_z (F 0, 1, 2)
+  const int q0 = gS ? 0 : 5, q1 = gS ? 1 : 7, q2 = gS ? 2 : 8;
+  T q[3][7];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const long long pz = pc + (long long)(k - 3) * b.sz;
+    q[0][k] = ld(F + q0 * V + pz);
+    q[1][k] = ld(F + q1 * V + pz);
+    q[2][k] = ld(F + q2 * V + pz);
+  }
+  q[0][6] = ld(F + q0 * V + pc + 3 * b.sz);
+  q[1][6] = ld(F + q1 * V + pc + 3 * b.sz);
+  q[2][6] = ld(F + q2 * V + pc + 3 * b.sz);
+  fill(zs, 0);
+  cp_async_commit();
+  // this group's rates and material, one step ahead
+  const int nd = gS ? 6 : 3, d0 = gS ? 3 : 0;
+  T dfo[6], m0 = 0, m1 = 0;
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) dfo[c] = c < nd ? b.DF[(d0 + c) * V + pc] : (T)0;
+    if (gS) { m0 = b.M[pc]; m1 = b.M[V + pc]; } else { m0 = b.M[2 * V + pc]; }
+  }
+  const T mx = active ? ld(b.mq + x) : (T)0, my = active ? ld(b.mr + y) : (T)0;
+
+  for (int z = zs; z <= ze; ++z) {
+    const int i = z - zs;
+    const int buf = i & 1;
+    const long long p = pc + (long long)i * b.sz;
+    cp_async_wait_all();
+    __syncthreads();
+    if (z + 1 <= ze) fill(z + 1, buf ^ 1);
+    cp_async_commit();
+    T qn0 = 0, qn1 = 0, qn2 = 0, dfn[6], mn0 = 0, mn1 = 0;
+    if (z + 1 <= ze) {
+      const long long pn = p + 4 * b.sz;
+      qn0 = ld(F + q0 * V + pn); qn1 = ld(F + q1 * V + pn); qn2 = ld(F + q2 * V + pn);
+      if (active) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) dfn[c] = c < nd ? b.DF[(d0 + c) * V + p + b.sz] : (T)0;
+        if (gS) { mn0 = b.M[p + b.sz]; mn1 = b.M[V + p + b.sz]; } else { mn0 = b.M[2 * V + p + b.sz]; }
+      }
+    }
+    if (active) {
+      const T mz = ld(b.ms + z);
+      const T(*P)[H][W] = S[buf];
+      const int c0 = tx + sh + 3, r0 = ty + 3;
+#define DX(f) (((T)0 + (mx * b.cx[0]) * (P[f][r0][c0 + 1] - P[f][r0][c0 - 1])) + \
+               (mx * b.cx[1]) * (P[f][r0][c0 + 2] - P[f][r0][c0 - 2])) + \
+              (mx * b.cx[2]) * (P[f][r0][c0 + 3] - P[f][r0][c0 - 3])
+#define DY(f) (((T)0 + (my * b.cy[0]) * (P[f][r0 + 1][c0] - P[f][r0 - 1][c0])) + \
+               (my * b.cy[1]) * (P[f][r0 + 2][c0] - P[f][r0 - 2][c0])) + \
+              (my * b.cy[2]) * (P[f][r0 + 3][c0] - P[f][r0 - 3][c0])
+#define DZ(k) (((T)0 + (mz * b.cz[0]) * (q[k][4] - q[k][2])) + (mz * b.cz[1]) * (q[k][5] - q[k][1])) + \
+              (mz * b.cz[2]) * (q[k][6] - q[k][0])
+      const T Bdt = (T)a.Bdt;
+      const bool sc = (a.flags & F_SCALE) != 0;
+      if (!gS) {
+        // velocity rates: a1 * (d sxx/dx + d sxy/dy + d sxz/dz), ...   (queue: 0 szz, 1 sxz, 2 syz)
+        const T a1 = (T)1 / m0;
+        T df0 = sc ? (T)a.A * dfo[0] : dfo[0];
+        T df1 = sc ? (T)a.A * dfo[1] : dfo[1];
+        T df2 = sc ? (T)a.A * dfo[2] : dfo[2];
+        df0 = df0 + a1 * (DX(3) + DY(5) + DZ(1));
+        df1 = df1 + a1 * (DX(5) + DY(4) + DZ(2));
+        df2 = df2 + a1 * (DX(6) + DY(7) + DZ(0));
+        b.DF[0 * V + p] = df0;
+        b.DF[1 * V + p] = df1;
+        b.DF[2 * V + p] = df2;
+        if (a.flags & F_UPDATE) {
+          const T f0 = P[0][r0][c0], f1 = P[1][r0][c0], f2 = P[2][r0][c0];
+          if (b.FC) {
+            const T dv[3] = {df0, df1, df2}, fv[3] = {f0, f1, f2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              T comp = b.FC[c * V + p];
+              T yv = Bdt * dv[c] - comp;
+              T tv = fv[c] + yv;
+              b.FC[c * V + p] = (tv - fv[c]) - yv;
+              Fn[c * V + p] = tv;
+            }
+          } else {
+            Fn[0 * V + p] = f0 + Bdt * df0;
+            Fn[1 * V + p] = f1 + Bdt * df1;
+            Fn[2 * V + p] = f2 + Bdt * df2;
+          }
+        }
+      } else {
+        // stress rates from velocity gradients (queue: 0 vx, 1 vy, 2 vz)
+        const T lam = m0, mu = m1;
+        const T a2 = (T)2 * mu + lam, a3 = lam, a4 = mu;
+        const T vxx = DX(0), vyx = DX(1), vzx = DX(2);
+        const T vxy = DY(0), vyy = DY(1), vzy = DY(2);
+        const T vxz = DZ(0), vyz = DZ(1), vzz = DZ(2);
+        T df[9];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) df[3 + c] = sc ? (T)a.A * dfo[c] : dfo[c];
+        df[3] = df[3] + a2 * vxx + a3 * (vyy + vzz);
+        df[4] = df[4] + a2 * vyy + a3 * (vxx + vzz);
+        df[5] = df[5] + a2 * vzz + a3 * (vxx + vyy);
+        df[6] = df[6] + a4 * (vxy + vyx);
+        df[7] = df[7] + a4 * (vxz + vzx);
+        df[8] = df[8] + a4 * (vyz + vzy);
+        if (RESP != RESP_EL) {
+          T e[6] = {vxx, vyy, vzz, vxy + vyx, vxz + vzx, vyz + vzy};
+          T tr = vxx + vyy + vzz;
+          anelastic_point<T, RESP>(b, a, x, y, z, p, e, tr, df, true);
+        }
+        if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] &&
+            y <= b.sbox[3] && z >= b.sbox[4] && z <= b.sbox[5]) {
+          df[0] = df[1] = df[2] = (T)0;
+          add_sources<T, MESH_CART>(b, tst, x, y, z, p, df);
+        }
+#pragma unroll
+        for (int c = 3; c < 9; ++c) b.DF[c * V + p] = df[c];
+        if (a.flags & F_UPDATE) {
+          T fc[9];
+          fc[3] = P[3][r0][c0]; fc[4] = P[4][r0][c0];
+          fc[5] = ld(F + 5 * V + p);
+          fc[6] = P[5][r0][c0]; fc[7] = P[6][r0][c0]; fc[8] = P[7][r0][c0];
+          if (b.FC) {
+#pragma unroll
+            for (int c = 3; c < 9; ++c) {
+              T comp = b.FC[c * V + p];
+              T yv = Bdt * df[c] - comp;
+              T tv = fc[c] + yv;
+              b.FC[c * V + p] = (tv - fc[c]) - yv;
+              Fn[c * V + p] = tv;
+            }
+          } else {
+#pragma unroll
+            for (int c = 3; c < 9; ++c) Fn[c * V + p] = fc[c] + Bdt * df[c];
+          }
+        }
+      }
+#undef DX
+#undef DY
+#undef DZ
+    }
+    // advance the queue and the prefetched values
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { q[0][k] = q[0][k + 1]; q[1][k] = q[1][k + 1]; q[2][k] = q[2][k + 1]; }
+    q[0][6] = qn0; q[1][6] = qn1; q[2][6] = qn2;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) dfo[c] = dfn[c];
+    m0 = mn0; m1 = mn1;
+  }
+  cp_async_wait_all();
 }
 
 // F <- F + dt*DF over every interior point (update_fields, split path): in place
