@@ -29,9 +29,11 @@ def test_pin_case_final_state(wql3d_lib, oracle_lib):
 @pytest.mark.parametrize("mesh", ["cartesian", "curvilinear"])
 @pytest.mark.parametrize("response", ["elastic", "anelastic-Q4", "anelastic-Q8", "anelastic-fQ8"])
 @pytest.mark.parametrize("pml", [False, True])
-def test_single_stage_random_state(wql3d_lib, oracle_lib, mesh, response, pml):
+@pytest.mark.parametrize("f32lit", [False, True])
+def test_single_stage_random_state(wql3d_lib, oracle_lib, mesh, response, pml, f32lit):
     """One full RK stage from a random state: rates and fields to 1e-12 relative."""
     p = small_case(mesh=mesh, response=response, pml=pml)
+    p.closure_f32_literal = f32lit
     (F, DF), = random_state(p)
     dt = p.dt()
     o = oracle_lib.OracleDomain(p)
@@ -48,11 +50,18 @@ def test_single_stage_random_state(wql3d_lib, oracle_lib, mesh, response, pml):
 
 
 @pytest.mark.parametrize("mesh", ["cartesian", "curvilinear"])
-@pytest.mark.parametrize("response,pml", [("elastic", False), ("elastic", True), ("anelastic-Q8", True),
-                                          ("anelastic-Q4", False), ("anelastic-fQ8", True)])
-def test_multi_step_run(wql3d_lib, oracle_lib, mesh, response, pml):
-    """40 steps from rest with sources, SATs, receivers: fields, memory variables, seismograms."""
+@pytest.mark.parametrize("response,pml,f32lit", [("elastic", False, False), ("elastic", True, False),
+                                                 ("elastic", True, True), ("anelastic-Q8", True, True),
+                                                 ("anelastic-Q4", False, False), ("anelastic-fQ8", True, False)])
+def test_multi_step_run(wql3d_lib, oracle_lib, mesh, response, pml, f32lit):
+    """40 steps from rest with sources, SATs, receivers: fields, memory variables, seismograms.
+
+    f32lit selects the single-precision row-4 literal, whose off-diagonal
+    metric terms (~1e-10) send Cartesian blocks through the full-metric
+    near-boundary path instead of the separable one.
+    """
     p = small_case(mesh=mesh, response=response, pml=pml)
+    p.closure_f32_literal = f32lit
     nsteps = 40
     o = oracle_lib.OracleDomain(p)
     so = o.run(nsteps)[0]

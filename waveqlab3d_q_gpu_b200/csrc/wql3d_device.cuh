@@ -83,6 +83,7 @@ struct Blk {
   T ihq, ihr, ihs;      // 1/h
   T cx[3], cy[3], cz[3];// interior coefficients c/h
   int lit;              // SBP literal precision (index into c_sbp_c)
+  int sep;              // Cartesian block whose metric is diagonal to roundoff (separable shell)
   const double *rowc;   // closure rows 0..11 (left 1..6, right n..n-5): 8 signed coefficients each
   const int *rowo;      // matching tap offsets relative to the point
   // PML slabs (faces 0..5): box and Q / DQ (9 components each, slab-local)
@@ -280,7 +281,17 @@ __device__ void bc_vector(int plus, const T u[9], T Zs, T Zp, T r, const T l[3],
   ubc[8] = sg * (norm * (n[2] * F_y + n[1] * F_z));
 }
 
-template <typename T, int MESH>
+// face bases of a diagonal-metric Cartesian block: gen_orth_vectors applied to
+// the axis normals (src/unit_normals.f90:217-249)
+template <typename T>
+__device__ __forceinline__ void cart_basis(int axis, T l[3], T m[3], T n[3]) {
+  for (int c = 0; c < 3; ++c) { l[c] = 0; m[c] = 0; n[c] = 0; }
+  if (axis == 0) { n[0] = 1; m[1] = 1; l[2] = 1; }
+  else if (axis == 1) { n[1] = 1; m[2] = 1; l[0] = 1; }
+  else { n[2] = 1; m[1] = 1; l[0] = -1; }
+}
+
+template <typename T, int MESH, bool SEP>
 __device__ void add_face_sats(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T df[9], bool pml_point) {
   const int pos[3] = {x, y, z};
   const int nn[3] = {b.nx, b.ny, b.nz};
@@ -298,7 +309,10 @@ __device__ void add_face_sats(const Blk<T> &b, const T *F, int x, int y, int z, 
     T c_s = sqrt(mu / rho);
     T Zp = rho * c_p, Zs = rho * c_s;
     T l[3], m[3], n[3], norm;
-    {
+    if (SEP) {
+      cart_basis(axis, l, m, n);
+      norm = axis == 0 ? ld(b.mq + x) : axis == 1 ? ld(b.mr + y) : ld(b.ms + z);
+    } else {
       T qx = ld(b.met + (long long)(0 + axis) * b.vol + p);
       T qy = ld(b.met + (long long)(3 + axis) * b.vol + p);
       T qz = ld(b.met + (long long)(6 + axis) * b.vol + p);
@@ -606,10 +620,46 @@ __device__ void jju6_all(const Blk<T> &b, const T *F, int x, int y, int z, long 
   }
 }
 
+// Separable Cartesian near-boundary derivative of all nine fields along one
+// axis: m_a(i) * (1/h_a) * sum_k c_k F(k).  On a Cartesian grid whose metric
+// is diagonal to roundoff, J*X_a is constant along the axis, so this equals
+// JJU_x6's conservative form divided by J (src/JU_xJU_yJU_z6.f90:12-809).
+template <typename T>
+__device__ void sep_axis(const Blk<T> &b, const T *F, int i, int n, long long p, long long stride, T m, T ih, T U[9]) {
+  T s[9];
+#pragma unroll
+  for (int f = 0; f < 9; ++f) s[f] = 0;
+  if (i >= 7 && i <= n - 6) {
+    const T cc[6] = {(T)(-1.0 / 60.0), (T)0.15, (T)-0.75, (T)0.75, (T)-0.15, (T)(1.0 / 60.0)};
+    const int off[6] = {-3, -2, -1, 1, 2, 3};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const long long q = p + (long long)off[k] * stride;
+#pragma unroll
+      for (int f = 0; f < 9; ++f) s[f] = s[f] + cc[k] * ld(F + f * b.vol + q);
+    }
+  } else {
+    const int row = i <= 6 ? i - 1 : 6 + (n - i);
+    const double *rc = b.rowc + row * 8;
+    const int *ro = b.rowo + row * 8;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const T c = (T)__ldg(rc + k);
+      if (c != (T)0) {
+        const long long q = p + (long long)__ldg(ro + k) * stride;
+#pragma unroll
+        for (int f = 0; f < 9; ++f) s[f] = s[f] + c * ld(F + f * b.vol + q);
+      }
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 9; ++f) U[f] = ih * (m * s[f]);
+}
+
 // ---------------------------------------------------------------------------
 // Stage kernel: one thread per grid point.
 // ---------------------------------------------------------------------------
-template <typename T, int MESH, int RESP>
+template <typename T, int MESH, int RESP, bool SEP = false>
 __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, int z) {
   const long long p = pidx(b, x, y, z);
   const long long V = b.vol;
@@ -721,14 +771,21 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
     // near boundaries and PML slabs, src/RHS_Interior.f90:136-281
     T Ux[9], Uy[9], Uz[9];
     const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
-    {
+    T J, rhoJ_inv;
+    if (SEP) {
+      sep_axis<T>(b, F, x, b.nx, p, 1, ld(b.mq + x), b.ihq, Ux);
+      sep_axis<T>(b, F, y, b.ny, p, b.sy, ld(b.mr + y), b.ihr, Uy);
+      sep_axis<T>(b, F, z, b.nz, p, b.sz, ld(b.ms + z), b.ihs, Uz);
+      J = (T)1;
+      rhoJ_inv = (T)1 / rho;
+    } else {
       T U[3][9];
       jju6_all<T>(b, F, x, y, z, p, U);
 #pragma unroll
       for (int f = 0; f < 9; ++f) { Ux[f] = U[0][f]; Uy[f] = U[1][f]; Uz[f] = U[2][f]; }
+      J = ld(b.J + p);
+      rhoJ_inv = (T)1 / (rho * J);
     }
-    const T J = ld(b.J + p);
-    const T rhoJ_inv = (T)1 / (rho * J);
     const T lambda2mu = lam + (T)2 * mu;
     T DU[9];
     DU[0] = (Ux[3] + Uy[6] + Uz[7]) * rhoJ_inv;
@@ -758,7 +815,7 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
           for (int c = 0; c < 9; ++c) b.DQ[f][c * b.pvol[f] + q] = (T)a.A * b.DQ[f][c * b.pvol[f] + q];
         }
       }
-      pml_point<T, true>(b, a, x, y, z, p, Ux, Uy, Uz, rhoJ_inv, lambda2mu, J, DU);
+      pml_point<T, !SEP>(b, a, x, y, z, p, Ux, Uy, Uz, rhoJ_inv, lambda2mu, J, DU);
     }
 #pragma unroll
     for (int c = 0; c < 9; ++c) df[c] = df[c] + DU[c];
@@ -783,7 +840,7 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
       z >= b.sbox[4] && z <= b.sbox[5])
     add_sources<T, MESH>(b, tst, x, y, z, p, df);
   if ((a.flags & F_SAT) && (x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz))
-    add_face_sats<T, MESH>(b, F, x, y, z, p, df, in_pml);
+    add_face_sats<T, MESH, SEP>(b, F, x, y, z, p, df, in_pml);
   if ((a.flags & F_ISAT)) {
     // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
     int side = x == 1 ? 0 : (x == b.nx ? 1 : -1);
@@ -878,13 +935,13 @@ __device__ inline void shell_decode(const Blk<T> &b, int idx, int &x, int &y, in
   x = c < (b.lo[0] - 1) ? 1 + c : b.hi[0] + 1 + (c - (b.lo[0] - 1));
 }
 
-template <typename T, int MESH, int RESP>
+template <typename T, int MESH, int RESP, bool SEP>
 __global__ void __launch_bounds__(128, 3) k_shell(Blk<T> b, StageArgs a, int count) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= count) return;
   int x, y, z;
   shell_decode(b, idx, x, y, z);
-  point_update<T, MESH, RESP>(b, a, x, y, z);
+  point_update<T, MESH, RESP, SEP>(b, a, x, y, z);
 }
 
 // ---------------------------------------------------------------------------

@@ -167,7 +167,10 @@ class Problem:
     w_stride: int = 1
     source_order: int = 2
     source_alpha: int = 0
-    closure_f32_literal: bool = True
+    # SBP row-4 literal 0.013435342414630 carries no kind suffix in the
+    # reference: double under gfortran -fdefault-real-8 (cpu-release), single
+    # under nvfortran without -r8.  Both reproduce the published 16-digit pin.
+    closure_f32_literal: bool = False
     anelastic: AnelasticParams = field(default_factory=AnelasticParams)
     interface: InterfaceParams = field(default_factory=InterfaceParams)
     tau0: float = TAU0_TRADITIONAL6
