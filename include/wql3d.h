@@ -70,6 +70,21 @@ extern "C" {
 #define WQL3D_IFACE_SLIP_WEAKENING 1
 #define WQL3D_IFACE_LINEAR 2
 
+/* fault prestress and static friction: per-point maps (iface_tau0, iface_fs)
+   or the reference's TPV5 formulas (src/Interface_Condition.f90:1283-1294,
+   1822-1830) evaluated at the face coordinates */
+#define WQL3D_FAULT_MAPS 0
+#define WQL3D_FAULT_TPV5 1
+
+/* fault outputs of wql3d_get_fault_output (src/domain.f90:782-845,
+   src/fault_output.f90:73-122): [component][ns][nr] doubles */
+#define WQL3D_FO_S 0       /* 4: slip along n, m, l and cumulative |slip rate| integral */
+#define WQL3D_FO_SVEL 1    /* 3: v_hat - u_hat in (n, m, l), recorded at stage 1 */
+#define WQL3D_FO_UHAT 2    /* 6: slip velocity (3) and side-1 traction + prestress (3), stage 1 */
+#define WQL3D_FO_VHAT 3    /* 6: slip velocity (3) and side-2 traction + prestress (3), stage 1 */
+#define WQL3D_FO_STATE 4   /* 1: state variable W */
+#define WQL3D_FO_TRUP 5    /* 1: rupture time (1e9 where the slip rate never exceeded 1e-3) */
+
 typedef struct wql3d_domain wql3d_domain;
 
 /* Per-block description, filled once from the resolved configuration
@@ -116,8 +131,10 @@ typedef struct wql3d_domain_desc {
   double strength_s[8];        /* fQ8 S strengths */
   double strength_p[8];        /* fQ8 P strengths */
   int32_t coupling;            /* WQL3D_IFACE_* (two blocks) */
-  int32_t serial_shared;       /* 1: interface slip rates accumulated once per block side,
-                                  like the reference's one-process two-block run */
+  int32_t fault_problem;       /* WQL3D_FAULT_MAPS or WQL3D_FAULT_TPV5 */
+  int32_t serial_shared;       /* 1: both sides' interface solves add to the slip rate (twice per
+                                  stage), as in the reference's one-process two-block run;
+                                  0: once per stage, as in its one-rank-per-block run */
   double fs, fd, Dc;           /* slip-weakening parameters */
   const double *iface_tau0;    /* optional (3, ns, nr): initial tractions n, m, l on the interface */
   const double *iface_fs;      /* optional (ns, nr) static friction map */
@@ -138,6 +155,11 @@ int wql3d_get_rates(wql3d_domain *d, int block, double *DF, int32_t host_nb);
 int wql3d_get_memory_variables(wql3d_domain *d, int block, double *eta);   /* 6 x nmech x n, host_nb 0 */
 int wql3d_get_metrics(wql3d_domain *d, int block, double *metrics);       /* 10 x n: metricx, metricy, metricz, J */
 int wql3d_get_interface(wql3d_domain *d, double *out);                    /* per point S(4) W Svel trup */
+/* one fault output (WQL3D_FO_*) in the layout the reference writes its
+   fault files in; replaces write_fault_output / write_hat_output
+   (src/domain.f90:782-845).  The face traces (Uface, Vface) are the fields
+   at block 1's q-max and block 2's q-min faces (wql3d_get_fields). */
+int wql3d_get_fault_output(wql3d_domain *d, int kind, double *out);
 
 /* time integration: one RK stage (time_step.f90:109-147 loop body),
    one time step (time_step_RK) and a graph-captured run of many steps.

@@ -36,7 +36,7 @@ class OrcDesc(C.Structure):
 
 class OrcIface(C.Structure):
     _fields_ = [
-        ("coupling", C.c_int), ("double_ds", C.c_int),
+        ("coupling", C.c_int), ("double_ds", C.c_int), ("problem", C.c_int),
         ("fs", C.c_double), ("fd", C.c_double), ("Dc", C.c_double), ("alpha_lin", C.c_double),
         ("tau0_n", C.POINTER(C.c_double)), ("tau0_l", C.POINTER(C.c_double)),
         ("tau0_m", C.POINTER(C.c_double)), ("fs_map", C.POINTER(C.c_double)),
@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         L.orc_get_pml.argtypes = [vp, C.c_int, C.c_int, dp]
         L.orc_get_normals.argtypes = [vp, C.c_int, C.c_int, dp]
         L.orc_get_iface.argtypes = [vp, dp]
+        L.orc_get_fault.argtypes = [vp, C.c_int, dp]
         L.orc_receiver_index.argtypes = [vp, C.c_int, ip]
         L.orc_final_state.argtypes = [vp, dp, dp, dp]
         L.orc_q4_coefficients.argtypes = [C.c_double, C.c_double, dp, dp]
@@ -97,7 +98,7 @@ class OracleDomain:
     """One or two blocks advanced by the oracle's time_step_RK."""
 
     def __init__(self, problem, *, material_override=None, threads: Optional[int] = None):
-        from waveqlab3d_q_gpu_b200.problem import COUPLINGS, RESPONSES, STF_CODES
+        from waveqlab3d_q_gpu_b200.problem import COUPLINGS, FAULT_PROBLEMS, RESPONSES, STF_CODES
         from waveqlab3d_q_gpu_b200 import anelastic as an
 
         if threads is not None:
@@ -179,6 +180,7 @@ class OracleDomain:
             I = OrcIface()
             I.coupling = COUPLINGS[ip.coupling]
             I.double_ds = 1 if ip.serial_shared else 0
+            I.problem = FAULT_PROBLEMS[ip.problem]
             I.fs, I.fd, I.Dc = ip.fs, ip.fd, ip.Dc
             for name in ("tau0_n", "tau0_l", "tau0_m", "fs_map"):
                 a = getattr(ip, name)
@@ -298,6 +300,16 @@ class OracleDomain:
         nq, nr, ns = self.problem.blocks[0].nqrs
         a = np.zeros((ns, nr, 7))
         lib().orc_get_iface(self.handle, _dptr(a))
+        return a
+
+    FAULT_KINDS = {"S": (0, 4), "Svel": (1, 3), "Uhat": (2, 6), "Vhat": (3, 6), "state": (4, 1), "trup": (5, 1)}
+
+    def fault(self, name: str) -> np.ndarray:
+        """One fault output (src/fault_output.f90:73-122), shape (ncomp, ns, nr)."""
+        kind, nc = self.FAULT_KINDS[name]
+        nq, nr, ns = self.problem.blocks[0].nqrs
+        a = np.zeros((nc, ns, nr))
+        lib().orc_get_fault(self.handle, kind, _dptr(a))
         return a
 
     def receiver_index(self, b: int = 0) -> np.ndarray:

@@ -130,6 +130,7 @@ typedef struct {
   orc_iface_desc d;
   int nr, ns;
   double *S[4], *DS[4], *W, *DW, *Svel[3], *trup;
+  double *Uhat[6], *Vhat[6];  /* stage-1 fault outputs (fault%Uhat_pluspres, Vhat_pluspres) */
   double *t0n, *t0m, *t0l, *fsm;
 } oiface;
 
@@ -1128,6 +1129,7 @@ void *orc_create(int nblocks, const orc_desc *blocks, const orc_iface_desc *ifac
     for (int c = 0; c < 4; ++c) { I->S[c] = zalloc(n, 0.0); I->DS[c] = zalloc(n, 0.0); }
     I->W = zalloc(n, 0.0); I->DW = zalloc(n, 0.0);
     for (int c = 0; c < 3; ++c) I->Svel[c] = zalloc(n, 0.0);
+    for (int c = 0; c < 6; ++c) { I->Uhat[c] = zalloc(n, 0.0); I->Vhat[c] = zalloc(n, 0.0); }
     I->trup = zalloc(n, 1.0e9);
     I->t0n = zalloc(n, 0.0); I->t0m = zalloc(n, 0.0); I->t0l = zalloc(n, 0.0); I->fsm = zalloc(n, iface ? iface->fs : 0.0);
     if (iface) {
@@ -1151,6 +1153,7 @@ void orc_destroy(void *dv) {
   if (D->I) {
     for (int c = 0; c < 4; ++c) { free(D->I->S[c]); free(D->I->DS[c]); }
     for (int c = 0; c < 3; ++c) free(D->I->Svel[c]);
+    for (int c = 0; c < 6; ++c) { free(D->I->Uhat[c]); free(D->I->Vhat[c]); }
     free(D->I->W); free(D->I->DW); free(D->I->trup);
     free(D->I->t0n); free(D->I->t0m); free(D->I->t0l); free(D->I->fsm);
     free(D->I);
@@ -1305,5 +1308,306 @@ void orc_modulus_correction(int nmech, const double *tau, const double *weight, 
   }
 }
 
-/* interface coupling: filled in by wql3d_oracle_iface.c */
-void orc_iface_couple(odom *D, int ib, double t, int stage) { (void)D; (void)ib; (void)t; (void)stage; }
+/* ------------------------------------------------------------------------ */
+/* Block-interface coupling (q direction)                                    */
+/* ------------------------------------------------------------------------ */
+
+/* boxcar of unit amplitude on (-w, w), 1/2 within 100 eps of the edges:
+   src/Interface_Condition.f90:2438-2457 */
+static double boxcar(double x, double w) {
+  const double tol = 100.0 * 2.220446049250313e-16;
+  if (-w + tol < x && x < w - tol) return 1.0;
+  if (fabs(-w - x) <= tol || fabs(x - w) <= tol) return 0.5;
+  return 0.0;
+}
+
+/* initial tractions on the fault: src/Interface_Condition.f90:1802-1830 (TPV5),
+   or the per-point maps of the description */
+static void fault_prestress(const oiface *I, long k, const double x[3], double *T0n, double *T0m, double *T0l) {
+  if (I->d.problem == ORC_FAULT_TPV5) {
+    double tl = 70.0;
+    tl = tl + 8.0 * boxcar(x[1] - 7.5, 1.5) * boxcar(x[2] + 7.5, 1.5);
+    tl = tl + 11.6 * boxcar(x[1] - 7.5, 1.5) * boxcar(x[2], 1.5);
+    tl = tl - 8.0 * boxcar(x[1] - 7.5, 1.5) * boxcar(x[2] - 7.5, 1.5);
+    *T0n = -120.0; *T0m = 0.0; *T0l = tl;
+    return;
+  }
+  *T0n = I->t0n[k]; *T0m = I->t0m[k]; *T0l = I->t0l[k];
+}
+
+/* fault strength tau_str = sigma_n * f(slip): src/Interface_Condition.f90:1268-1299 */
+static double fault_strength(const oiface *I, long k, const double x[3], double sigma_n, double D) {
+  double fs, fd, Dc;
+  if (I->d.problem == ORC_FAULT_TPV5) {
+    fs = 0.677; fd = 0.525; Dc = 0.4;
+    fs = fs + 1.0e10 * (1.0 - boxcar(x[1], 15.0) * boxcar(x[2], 15.0));
+  } else {
+    fs = I->fsm[k]; fd = I->d.fd; Dc = I->d.Dc;
+  }
+  double f = fs - (fs - fd) * fmin(D, Dc) / Dc;
+  return sigma_n * f;
+}
+
+/* characteristic variables p = Z1 u - T (side 1), q = Z2 v + T (side 2) and the
+   locked-interface flux phi: common head of Welded_Interface, Linear_Friction and
+   Slip_Weakening_Friction (src/Interface_Condition.f90:540-575, 660-690, 780-815) */
+typedef struct {
+  double p[3], q[3], phi[3], eta_p, eta_s;
+} char_t;
+
+static void characteristics(const double *U, const double *V, double Z1s, double Z2s, double Z1p, double Z2p,
+                            char_t *c) {
+  c->p[0] = Z1p * U[0] - U[3];
+  c->p[1] = Z1s * U[1] - U[4];
+  c->p[2] = Z1s * U[2] - U[5];
+  c->q[0] = Z2p * V[0] + V[3];
+  c->q[1] = Z2s * V[1] + V[4];
+  c->q[2] = Z2s * V[2] + V[5];
+  c->eta_p = 1.0 / (1.0 / Z1p + 1.0 / Z2p);
+  c->eta_s = 1.0 / (1.0 / Z1s + 1.0 / Z2s);
+  c->phi[0] = c->eta_p * (c->q[0] / Z2p - c->p[0] / Z1p);
+  c->phi[1] = c->eta_s * (c->q[1] / Z2s - c->p[1] / Z1s);
+  c->phi[2] = c->eta_s * (c->q[2] / Z2s - c->p[2] / Z1s);
+}
+
+/* Welded_Interface, src/Interface_Condition.f90:504-598 */
+static void welded(const double *U, const double *V, double *P, double *Q, double Z1s, double Z2s, double Z1p,
+                   double Z2p) {
+  char_t c;
+  characteristics(U, V, Z1s, Z2s, Z1p, Z2p, &c);
+  P[0] = (c.q[0] - c.phi[0]) / Z2p; P[3] = c.phi[0];
+  Q[0] = (c.p[0] + c.phi[0]) / Z1p; Q[3] = c.phi[0];
+  P[2] = (c.q[2] - c.phi[2]) / Z2s; P[5] = c.phi[2];
+  Q[2] = (c.p[2] + c.phi[2]) / Z1s; Q[5] = c.phi[2];
+  P[1] = (c.q[1] - c.phi[1]) / Z2s; P[4] = c.phi[1];
+  Q[1] = (c.p[1] + c.phi[1]) / Z1s; Q[4] = c.phi[1];
+}
+
+/* Linear_Friction, src/Interface_Condition.f90:601-741.  The reference never
+   assigns u_out(2) (P_loc(2) keeps a stale value); this restatement sets it to
+   the u_m_hat that the routine computes. */
+static void linear_friction(const double *U, const double *V, double *P, double *Q, double Z1s, double Z2s,
+                            double Z1p, double Z2p, double alpha) {
+  char_t c;
+  characteristics(U, V, Z1s, Z2s, Z1p, Z2p, &c);
+  P[0] = (c.q[0] - c.phi[0]) / Z2p; P[3] = c.phi[0];
+  Q[0] = (c.p[0] + c.phi[0]) / Z1p; Q[3] = c.phi[0];
+  double tm = alpha / (alpha + c.eta_s) * c.phi[1];
+  double tl = alpha / (alpha + c.eta_s) * c.phi[2];
+  P[4] = tm; P[5] = tl; Q[4] = tm; Q[5] = tl;
+  Q[1] = (c.p[1] + tm) / Z1s + 1.0 / (alpha + c.eta_s) * c.phi[1];
+  Q[2] = (c.p[2] + tl) / Z1s + 1.0 / (alpha + c.eta_s) * c.phi[2];
+  P[1] = (c.q[1] - tm) / Z2s - 1.0 / (alpha + c.eta_s) * c.phi[1];
+  P[2] = (c.q[2] - tl) / Z2s - 1.0 / (alpha + c.eta_s) * c.phi[2];
+}
+
+/* Slip_Weakening_Friction with the closed-form solve,
+   src/Interface_Condition.f90:745-916 and 1095-1168 */
+static void slip_weakening(const oiface *I, long k, const double x[3], const double *U, const double *V, double *P,
+                           double *Q, double Z1s, double Z2s, double Z1p, double Z2p, double slip) {
+  char_t c;
+  characteristics(U, V, Z1s, Z2s, Z1p, Z2p, &c);
+  double T0n, T0m, T0l;
+  fault_prestress(I, k, x, &T0n, &T0m, &T0l);
+  P[0] = (c.q[0] - c.phi[0]) / Z2p; P[3] = c.phi[0];
+  Q[0] = (c.p[0] + c.phi[0]) / Z1p; Q[3] = c.phi[0];
+  double tau_lock = sqrt((T0l + c.phi[2]) * (T0l + c.phi[2]) + (T0m + c.phi[1]) * (T0m + c.phi[1]));
+  double sigma_n = fmax(0.0, -(T0n + c.phi[0]));
+  double tau_str = fault_strength(I, k, x, sigma_n, slip);
+  double tm_hat, tl_hat, vm, vl;
+  if (tau_lock > tau_str) {
+    double phi1 = T0m + c.phi[1], phi2 = T0l + c.phi[2];
+    double Phi = sqrt(phi1 * phi1 + phi2 * phi2);
+    double Vs = (Phi - tau_str) / c.eta_s;
+    vm = phi1 / (c.eta_s + tau_str / Vs);
+    vl = phi2 / (c.eta_s + tau_str / Vs);
+    double tau_m = phi1 - c.eta_s * vm;
+    double tau_l = phi2 - c.eta_s * vl;
+    tm_hat = tau_m - T0m;
+    tl_hat = tau_l - T0l;
+  } else {
+    tm_hat = c.phi[1];
+    tl_hat = c.phi[2];
+    vm = 0.0; vl = 0.0;
+  }
+  Q[1] = (tm_hat + c.p[1]) / Z1s + vm;
+  Q[2] = (tl_hat + c.p[2]) / Z1s + vl;
+  P[1] = (c.q[1] - tm_hat) / Z2s - vm;
+  P[2] = (c.q[2] - tl_hat) / Z2s - vl;
+  P[4] = tm_hat; P[5] = tl_hat; Q[4] = tm_hat; Q[5] = tl_hat;
+}
+
+static void rotate_in(double *w, const double n[3], const double m[3], const double l[3]) {
+  /* src/CouplingForcing.f90:466-520 */
+  double a[6];
+  memcpy(a, w, sizeof a);
+  w[0] = n[0] * a[0] + n[1] * a[1] + n[2] * a[2];
+  w[1] = m[0] * a[0] + m[1] * a[1] + m[2] * a[2];
+  w[2] = l[0] * a[0] + l[1] * a[1] + l[2] * a[2];
+  w[3] = n[0] * a[3] + n[1] * a[4] + n[2] * a[5];
+  w[4] = m[0] * a[3] + m[1] * a[4] + m[2] * a[5];
+  w[5] = l[0] * a[3] + l[1] * a[4] + l[2] * a[5];
+}
+
+static void rotate_back(double *w, const double n[3], const double m[3], const double l[3]) {
+  /* src/CouplingForcing.f90:524-580 */
+  double a[6];
+  memcpy(a, w, sizeof a);
+  for (int i = 0; i < 3; ++i) {
+    w[i] = n[i] * a[0] + m[i] * a[1] + l[i] * a[2];
+    w[3 + i] = n[i] * a[3] + m[i] * a[4] + l[i] * a[5];
+  }
+}
+
+/* SAT vector of one side from grid (g) and hat (h) values in x,y,z components:
+   src/CouplingForcing.f90:250-437.  side 1: characteristics p = 1/2 (Zu + T)
+   with the block-1 impedances, side 2: q = 1/2 (Zv - T) with block 2's, signs
+   flipped on the stress rows. */
+static void iface_sat(int side, const double *g, const double *h, double lambda, double mu, double rho,
+                      const double n[3], const double m[3], const double l[3], double qx, double qy, double qz,
+                      double *out) {
+  double c_p = sqrt((2.0 * mu + lambda) / rho), c_s = sqrt(mu / rho);
+  double Zp = rho * c_p, Zs = rho * c_s;
+  double norm = sqrt(qx * qx + qy * qy + qz * qz);
+  const double *e[3] = {n, m, l};
+  double Mz[3][3], Mi[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      Mz[i][j] = e[i][0] * e[j][0] * Zp + e[i][1] * e[j][1] * Zs + e[i][2] * e[j][2] * Zs;
+      Mi[i][j] = e[i][0] * e[j][0] * 1.0 / Zp + e[i][1] * e[j][1] * 1.0 / Zs + e[i][2] * e[j][2] * 1.0 / Zs;
+    }
+  double sg = side == 1 ? 1.0 : -1.0;
+  double dch[3];
+  for (int i = 0; i < 3; ++i) {
+    double chat = 0.5 * (Mz[i][0] * h[0] + Mz[i][1] * h[1] + Mz[i][2] * h[2] + sg * h[3 + i]);
+    double cg = 0.5 * (Mz[i][0] * g[0] + Mz[i][1] * g[1] + Mz[i][2] * g[2] + sg * g[3 + i]);
+    dch[i] = cg - chat;
+  }
+  double r[3];
+  for (int i = 0; i < 3; ++i) r[i] = Mi[i][0] * dch[0] + Mi[i][1] * dch[1] + Mi[i][2] * dch[2];
+  double l2m = 2.0 * mu + lambda;
+  for (int i = 0; i < 3; ++i) out[i] = norm / rho * dch[i];
+  if (side == 1) {
+    out[3] = l2m * qx * r[0] + lambda * qy * r[1] + lambda * qz * r[2];
+    out[4] = l2m * qy * r[1] + lambda * qz * r[2] + lambda * qx * r[0];
+    out[5] = l2m * qz * r[2] + lambda * qy * r[1] + lambda * qx * r[0];
+    out[6] = mu * (qy * r[0] + qx * r[1]);
+    out[7] = mu * (qz * r[0] + qx * r[2]);
+    out[8] = mu * (qz * r[1] + qy * r[2]);
+  } else {
+    out[3] = -l2m * qx * r[0] - lambda * qy * r[1] - lambda * qz * r[2];
+    out[4] = -l2m * qy * r[1] - lambda * qz * r[2] - lambda * qx * r[0];
+    out[5] = -l2m * qz * r[2] - lambda * qy * r[1] - lambda * qx * r[0];
+    out[6] = -mu * (qy * r[0] + qx * r[1]);
+    out[7] = -mu * (qz * r[0] + qx * r[2]);
+    out[8] = -mu * (qz * r[1] + qy * r[2]);
+  }
+}
+
+/* Impose_Interface_Condition (src/RHS_Interior.f90:1771-1843) for block ib's
+   side of the interface: ib == 2 is block 1 (its q-max face), ib == 1 is
+   block 2 (its q-min face).  Couple_Interface_x (src/CouplingForcing.f90:9-463)
+   builds tractions, rotates to (n, m, l), solves the interface law
+   (Interface_RHS, src/Interface_Condition.f90:12-489), records the stage-1
+   fault outputs, rotates back and forms the SAT vector of the calling side. */
+void orc_iface_couple(odom *D, int ib, double t, int stage) {
+  oiface *I = D->I;
+  oblk *b = ib == 2 ? D->B[0] : D->B[1];
+  int face = ib == 2 ? 1 : 0;            /* face index of the calling block */
+  int xend = ib == 2 ? b->nx : 1;
+  double *const *uF = ib == 2 ? b->faceF[1] : b->faceFopp[0];
+  double *const *vF = ib == 2 ? b->faceFopp[1] : b->faceF[0];
+  double *const *M1 = ib == 2 ? b->faceM[1] : b->faceMopp[0];
+  double *const *M2 = ib == 2 ? b->faceMopp[1] : b->faceM[0];
+  int accumulate = I->d.double_ds || ib == 2;
+  int record = I->d.double_ds || ib == 2;
+  const double pen = b->d.tau0 / b->hq;
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y) {
+      long k = (long)(y - 1) + (long)b->ny * (z - 1);
+      long p = ID(b, xend, y, z);
+      double n[3], m[3], l[3];
+      for (int c = 0; c < 3; ++c) { n[c] = b->nn[face][c][k]; m[c] = b->nm[face][c][k]; l[c] = b->nl[face][c][k]; }
+      double u[6], v[6];
+      u[0] = uF[0][k]; u[1] = uF[1][k]; u[2] = uF[2][k];
+      u[3] = n[0] * uF[3][k] + n[1] * uF[6][k] + n[2] * uF[7][k];
+      u[4] = n[0] * uF[6][k] + n[1] * uF[4][k] + n[2] * uF[8][k];
+      u[5] = n[0] * uF[7][k] + n[1] * uF[8][k] + n[2] * uF[5][k];
+      v[0] = vF[0][k]; v[1] = vF[1][k]; v[2] = vF[2][k];
+      v[3] = n[0] * vF[3][k] + n[1] * vF[6][k] + n[2] * vF[7][k];
+      v[4] = n[0] * vF[6][k] + n[1] * vF[4][k] + n[2] * vF[8][k];
+      v[5] = n[0] * vF[7][k] + n[1] * vF[8][k] + n[2] * vF[5][k];
+      rotate_in(u, n, m, l);
+      rotate_in(v, n, m, l);
+      /* Interface_RHS for this point */
+      double lambda1 = M1[0][k], mu1 = M1[1][k], rho1 = M1[2][k];
+      double lambda2 = M2[0][k], mu2 = M2[1][k], rho2 = M2[2][k];
+      double c1p = sqrt((2.0 * mu1 + lambda1) / rho1), c1s = sqrt(mu1 / rho1);
+      double c2p = sqrt((2.0 * mu2 + lambda2) / rho2), c2s = sqrt(mu2 / rho2);
+      double Z1s = rho1 * c1s, Z2s = rho2 * c2s, Z1p = rho1 * c1p, Z2p = rho2 * c2p;
+      double x[3] = {b->X[0][p], b->X[1][p], b->X[2][p]};
+      double P[6], Q[6];
+      switch (I->d.coupling) {
+        case ORC_IFACE_SLIP_WEAKENING:
+          slip_weakening(I, k, x, u, v, P, Q, Z1s, Z2s, Z1p, Z2p, I->S[3][k]);
+          break;
+        case ORC_IFACE_LINEAR:
+          linear_friction(u, v, P, Q, Z1s, Z2s, Z1p, Z2p, 1.0e14);
+          break;
+        default:
+          welded(u, v, P, Q, Z1s, Z2s, Z1p, Z2p);
+          break;
+      }
+      double Vel = sqrt((Q[1] - P[1]) * (Q[1] - P[1]) + (Q[2] - P[2]) * (Q[2] - P[2]));
+      if (accumulate) {
+        for (int c = 0; c < 3; ++c) I->DS[c][k] = I->DS[c][k] + Q[c] - P[c];
+        I->DS[3][k] = I->DS[3][k] + Vel;
+      }
+      if (stage == 1 && record) {
+        double T0n = 0.0, T0m = 0.0, T0l = 0.0;
+        if (I->d.coupling != ORC_IFACE_LOCKED) fault_prestress(I, k, x, &T0n, &T0m, &T0l);
+        /* Couple_Interface_x overwrites components 1:3 with v_hat - u_hat */
+        for (int c = 0; c < 3; ++c) {
+          double sv = Q[c] - P[c];
+          I->Uhat[c][k] = sv; I->Vhat[c][k] = sv; I->Svel[c][k] = sv;
+        }
+        I->Uhat[3][k] = P[3] + T0n; I->Vhat[3][k] = Q[3] + T0n;
+        I->Uhat[4][k] = P[4] + T0m; I->Vhat[4][k] = Q[4] + T0m;
+        I->Uhat[5][k] = P[5] + T0l; I->Vhat[5][k] = Q[5] + T0l;
+        /* rupture_front, src/CouplingForcing.f90:583-600 */
+        if (sqrt(I->Svel[1][k] * I->Svel[1][k] + I->Svel[2][k] * I->Svel[2][k]) > 1.0e-3)
+          I->trup[k] = fmin(I->trup[k], t);
+      }
+      rotate_back(u, n, m, l);
+      rotate_back(v, n, m, l);
+      rotate_back(P, n, m, l);
+      rotate_back(Q, n, m, l);
+      /* metric of the calling block at its interface face, used for both sides */
+      double qx = b->mx[0][p], qy = b->my[0][p], qz = b->mz[0][p];
+      double sat[9];
+      if (ib == 2) iface_sat(1, u, P, lambda1, mu1, rho1, n, m, l, qx, qy, qz, sat);
+      else iface_sat(2, v, Q, lambda2, mu2, rho2, n, m, l, qx, qy, qz, sat);
+      for (int c = 0; c < 9; ++c) b->DF[c][p] = b->DF[c][p] - pen * sat[c];
+    }
+}
+
+int orc_get_fault(void *dv, int kind, double *out) {
+  odom *D = (odom *)dv;
+  if (!D || !D->I) return -1;
+  oiface *I = D->I;
+  long n = (long)I->nr * I->ns;
+  double **src = NULL;
+  int nc = 0;
+  switch (kind) {
+    case ORC_FO_S: src = I->S; nc = 4; break;
+    case ORC_FO_SVEL: src = I->Svel; nc = 3; break;
+    case ORC_FO_UHAT: src = I->Uhat; nc = 6; break;
+    case ORC_FO_VHAT: src = I->Vhat; nc = 6; break;
+    case ORC_FO_STATE: src = &I->W; nc = 1; break;
+    case ORC_FO_TRUP: src = &I->trup; nc = 1; break;
+    default: return -1;
+  }
+  for (int c = 0; c < nc; ++c) memcpy(out + c * n, src[c], sizeof(double) * (size_t)n);
+  return nc;
+}
+

@@ -28,6 +28,9 @@ enum {
 
 /* interface coupling laws, src/Interface_Condition.f90 */
 enum { ORC_IFACE_LOCKED = 0, ORC_IFACE_SLIP_WEAKENING = 1, ORC_IFACE_LINEAR = 2 };
+enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1 };
+/* fault outputs, src/domain.f90:782-845 and src/fault_output.f90:73-122; layout [comp][ns][nr] */
+enum { ORC_FO_S = 0, ORC_FO_SVEL = 1, ORC_FO_UHAT = 2, ORC_FO_VHAT = 3, ORC_FO_STATE = 4, ORC_FO_TRUP = 5 };
 
 typedef struct {
   int nq, nr, ns;
@@ -55,7 +58,10 @@ typedef struct {
 
 typedef struct {
   int coupling;            /* ORC_IFACE_* */
-  int double_ds;           /* 1: serial-shared run, Interface_RHS accumulates DS once per block side */
+  int double_ds;           /* 1: one-process two-block run (src/domain.f90:615-644): Interface_RHS runs
+                              once per block side on the shared iface, so DS and DW grow twice per stage */
+  int problem;             /* ORC_FAULT_MAPS: prestress/static friction from the maps below;
+                              ORC_FAULT_TPV5: src/Interface_Condition.f90:1283-1299, 1822-1830 */
   /* slip-weakening / linear friction parameters (uniform over the fault) */
   double fs, fd, Dc, alpha_lin;
   const double *tau0_n;    /* optional per-face-point initial normal traction (nr*ns) */
@@ -84,6 +90,9 @@ void orc_set_eta(void *d, int b, const double *in);
 void orc_get_pml(void *d, int b, int face, double *out);/* 9*npts of slab */
 void orc_get_normals(void *d, int b, int face, double *out); /* 9*face points: n_l(3) n_m(3) n_n(3) */
 void orc_get_iface(void *d, double *out);               /* per point: S(4) W(1) Svel(1) trup(1) */
+/* one fault output (ORC_FO_*): S 4, Svel 3, Uhat 6, Vhat 6, state 1, trup 1 components;
+   Svel/Uhat/Vhat are the values recorded at stage 1 of the last step */
+int orc_get_fault(void *d, int kind, double *out);
 void orc_receiver_index(void *d, int b, int *idx);      /* 3 per receiver */
 void orc_final_state(void *d, double *maxF, double *maxEta, double *maxB);
 

@@ -85,3 +85,77 @@ def rel_l2(a, b):
     b = np.asarray(b, float).ravel()
     den = np.linalg.norm(b)
     return np.linalg.norm(a - b) / (den if den > 0 else 1.0)
+
+
+def tpv5_case(serial_shared=False, n=21, t_final=0.5):
+    """test_problems/test_rup_cart_fric.in of the reference: two 21^3 Cartesian
+    blocks on [-3,0] and [0,3] x [6,9] x [-1.5,1.5] meeting at x = 0, TPV5
+    slip-weakening fault (prestress and strength of
+    src/Interface_Condition.f90:1283-1294, 1822-1830), free surface at y = 6,
+    absorbing elsewhere, CFL 0.5, stations at the fault centre on each side."""
+    from waveqlab3d_q_gpu_b200.problem import InterfaceParams
+    b1 = Block(nqrs=(n, n, n), aqrs=(-3.0, 6.0, -1.5), bqrs=(0.0, 9.0, 1.5), rho_s_p=(2.67, 3.464, 6.0),
+               lqrs=(1, 2, 1), rqrs=(0, 1, 1), receivers=np.array([[-0.0, 7.5, 0.0]]))
+    b2 = Block(nqrs=(n, n, n), aqrs=(0.0, 6.0, -1.5), bqrs=(3.0, 9.0, 1.5), rho_s_p=(2.67, 3.464, 6.0),
+               lqrs=(0, 2, 1), rqrs=(1, 1, 1), receivers=np.array([[0.0, 7.5, 0.0]]))
+    ip = InterfaceParams(coupling="slip-weakening_friction", problem="TPV5", serial_shared=serial_shared)
+    return Problem(blocks=[b1, b2], response="elastic", type_of_mesh="cartesian", t_final=t_final, CFL=0.5,
+                   interface=ip, w_stride=1)
+
+
+def two_block_case(mesh="cartesian", coupling="locked", response="elastic", n=(15, 17, 19), seed=4,
+                   serial_shared=False, pml=False):
+    """Two blocks meeting at a q-direction interface, with a heterogeneous
+    medium (different on each side) and, for 'curvilinear', a smooth
+    non-orthogonal mapping that is continuous across the interface so the
+    two face traces sit at the same points.  Friction laws get uniform
+    prestress / strength maps that put part of the fault above strength."""
+    from waveqlab3d_q_gpu_b200.problem import InterfaceParams
+    rng = np.random.default_rng(seed)
+    nq, nr, ns = n
+    L = (2.0, 2.4, 2.2)
+    blocks = []
+    for side in range(2):
+        kw = {}
+        q = np.linspace(0.0, 1.0, nq)
+        xi = 0.5 * q if side == 0 else 0.5 + 0.5 * q     # global q in [0, 1]
+        if mesh == "curvilinear":
+            xi3 = xi[None, None, :]
+            r = np.linspace(0.0, 1.0, nr)[None, :, None]
+            s = np.linspace(0.0, 1.0, ns)[:, None, None]
+            amp = 0.04
+            x = 2 * L[0] * xi3 - L[0] + amp * np.sin(2 * np.pi * r) * np.sin(np.pi * s) * np.sin(np.pi * xi3)
+            y = L[1] * r + amp * np.sin(np.pi * xi3) * np.cos(np.pi * s)
+            z = L[2] * s + amp * np.sin(2 * np.pi * xi3) * np.sin(np.pi * r)
+            shape = (ns, nr, nq)
+            kw["coords"] = np.stack([np.broadcast_to(x, shape), np.broadcast_to(y, shape),
+                                     np.broadcast_to(z, shape)]).copy()
+        rho = (2.6 + 0.15 * side) + 0.2 * rng.random((ns, nr, nq))
+        cs = (3.2 + 0.2 * side) + 0.3 * rng.random((ns, nr, nq))
+        cp = np.sqrt(3.0) * cs
+        kw["material"] = np.stack([rho * (cp ** 2 - 2 * cs ** 2), rho * cs ** 2, rho])
+        a = (-L[0], 0.0, 0.0) if side == 0 else (0.0, 0.0, 0.0)
+        bq = (0.0, L[1], L[2]) if side == 0 else (L[0], L[1], L[2])
+        lq = (1, 2, 1) if side == 0 else (0, 2, 1)
+        rq = (0, 1, 3) if side == 0 else (1, 1, 3)
+        srcs = [Source("ricker", 8.0, 0.1, 1.0, 0.8, 1.2, 0.3, -0.2, 0.1,
+                       -0.9 if side == 0 else 0.8, 1.1, 1.05)]
+        rec = np.array([[-0.5 if side == 0 else 0.5, 1.0, 1.2], [0.0, 1.2, 1.1]])
+        b = Block(nqrs=n, aqrs=a, bqrs=bq, rho_s_p=(2.67, 3.464, 6.0), lqrs=lq, rqrs=rq, sources=srcs,
+                  receivers=rec, **kw)
+        if pml:
+            b.pml_lqrs = (side == 0, False, False)
+            b.pml_rqrs = (side == 1, True, False)
+            b.npml = 5
+        blocks.append(b)
+    ip = InterfaceParams(coupling=coupling, serial_shared=serial_shared)
+    if coupling != "locked":
+        ip.tau0_n = np.full((ns, nr), -120.0)
+        ip.tau0_m = np.full((ns, nr), 5.0)
+        yy = np.linspace(0.0, 1.0, nr)[None, :]
+        zz = np.linspace(0.0, 1.0, ns)[:, None]
+        ip.tau0_l = 70.0 + 12.0 * np.exp(-((yy - 0.5) ** 2 + (zz - 0.5) ** 2) / 0.05)
+        ip.fs_map = np.full((ns, nr), 0.677)
+    an = AnelasticParams(Qs0=40.0, Qp0=80.0, fref=1.0, fmin=0.05, fmax=20.0)
+    return Problem(blocks=blocks, response=response, type_of_mesh=mesh, t_final=0.2, CFL=0.4, source_order=4,
+                   anelastic=an, interface=ip)

@@ -41,7 +41,7 @@ class DomainDesc(C.Structure):
         ("Qs0", C.c_double), ("Qp0", C.c_double),
         ("tau", C.c_double * 8), ("weight", C.c_double * 8),
         ("strength_s", C.c_double * 8), ("strength_p", C.c_double * 8),
-        ("coupling", C.c_int32), ("serial_shared", C.c_int32),
+        ("coupling", C.c_int32), ("fault_problem", C.c_int32), ("serial_shared", C.c_int32),
         ("fs", C.c_double), ("fd", C.c_double), ("Dc", C.c_double),
         ("iface_tau0", dp), ("iface_fs", dp),
         ("max_samples", C.c_int32),
@@ -60,6 +60,7 @@ SIGNATURES = {
     "wql3d_get_memory_variables": [C.c_void_p, C.c_int, dp],
     "wql3d_get_metrics": [C.c_void_p, C.c_int, dp],
     "wql3d_get_interface": [C.c_void_p, dp],
+    "wql3d_get_fault_output": [C.c_void_p, C.c_int, dp],
     "wql3d_set_time": [C.c_void_p, C.c_double],
     "wql3d_get_time": [C.c_void_p, dp],
     "wql3d_stage": [C.c_void_p, C.c_int, C.c_double],

@@ -793,17 +793,12 @@ int enqueue_stage(wql3d_domain *d, int stage, double dt, int flags) {
   a.dt = dt;
   a.time = d->time;
   if (d->has_iface && (flags & F_ISAT)) {
+    // interface law, SAT vectors, DS = A DS + ... and S = S + B dt DS in one pass
     launch_iface<T>(d->iface, blk<T>(d, 0), blk<T>(d, 1), a, d->stream);
     d->launches++;
   }
   for (int i = 0; i < d->nblocks; ++i) launch_stage<T>(d, i, a, true);
-  if (flags & F_UPDATE) {
-    if (d->has_iface) {
-      launch_iface_update<T>(d->iface, a, d->stream);
-      d->launches++;
-    }
-    d->cur ^= 1;
-  }
+  if (flags & F_UPDATE) d->cur ^= 1;
   return WQL3D_OK;
 }
 
@@ -865,7 +860,7 @@ int run_steps(wql3d_domain *d, double dt, int nsteps, int w_stride) {
         for (int i = 0; i < d->nblocks; ++i) per_pair += d->hb[i].nrec > 0 ? 1 : 0;
         int per_block = 0;
         for (int i = 0; i < d->nblocks; ++i) per_block += d->hb[i].mesh == WQL3D_MESH_CARTESIAN ? 2 : 1;
-        per_pair += 5 * (per_block + (d->has_iface ? 2 : 0)) + 1;
+        per_pair += 5 * (per_block + (d->has_iface ? 1 : 0)) + 1;
       }
       d->launches = l0;
       d->cur = cur0;
@@ -972,8 +967,10 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     if (rc) return cleanup(rc);
   }
   if (d->nblocks == 2) {
-    rc = d->fp32 ? setup_iface<float>(d->iface, d->desc, d->bf[0], d->bf[1], d->mem.ptrs, d->mem.bytes, d->stream)
-                 : setup_iface<double>(d->iface, d->desc, d->bd[0], d->bd[1], d->mem.ptrs, d->mem.bytes, d->stream);
+    rc = d->fp32 ? setup_iface<float>(d->iface, d->desc, d->bf[0], d->bf[1], d->hb[0].coords, d->hb[1].coords,
+                                      d->mem, d->stream)
+                 : setup_iface<double>(d->iface, d->desc, d->bd[0], d->bd[1], d->hb[0].coords, d->hb[1].coords,
+                                       d->mem, d->stream);
     if (rc) return cleanup(fail(rc, "interface setup failed"));
     d->has_iface = true;
     if (d->fp32) { d->bf[0].isat[1] = (float *)d->iface.sat_m; d->bf[1].isat[0] = (float *)d->iface.sat_p; }
@@ -1092,6 +1089,14 @@ int wql3d_get_metrics(wql3d_domain *d, int bi, double *out) {
 int wql3d_get_interface(wql3d_domain *d, double *out) {
   if (!d || !d->has_iface) return fail(WQL3D_EINVAL, "no interface");
   return iface_download(d->iface, out, d->stream);
+}
+
+int wql3d_get_fault_output(wql3d_domain *d, int kind, double *out) {
+  if (!d || !d->has_iface) return fail(WQL3D_EINVAL, "no interface");
+  if (!out) return fail(WQL3D_EINVAL, "null output");
+  int rc = iface_fault_output(d->iface, kind, out, d->stream);
+  if (rc) return fail(rc, "fault output kind " + std::to_string(kind));
+  return WQL3D_OK;
 }
 
 int wql3d_set_time(wql3d_domain *d, double t) {
@@ -1249,10 +1254,8 @@ int wql3d_update_fields(wql3d_domain *d, double dt) {
     d->launches++;
   }
   if (d->has_iface) {
-    StageArgs a;
-    memset(&a, 0, sizeof(a));
-    a.Bdt = dt;
-    launch_iface_update<double>(d->iface, a, d->stream);
+    if (d->fp32) launch_iface_update<float>(d->iface, d->bf[0], d->bf[1], dt, d->stream);
+    else launch_iface_update<double>(d->iface, d->bd[0], d->bd[1], dt, d->stream);
     d->launches++;
   }
   CK(cudaGetLastError());

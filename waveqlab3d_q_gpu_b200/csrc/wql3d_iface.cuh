@@ -1,6 +1,27 @@
 // Block-interface coupling on the q-direction interface between two blocks.
+//
+// One thread per interface point (y, z) does, for both sides of the fault,
+// what the reference does in Impose_Interface_Condition / Couple_Interface_x /
+// Interface_RHS (src/RHS_Interior.f90:1771-1843, src/CouplingForcing.f90:9-463,
+// src/Interface_Condition.f90:12-916):
+//   tractions from the face stresses, rotation to the (n, m, l) basis of the
+//   calling block's face, the interface law (locked, linear friction or
+//   linear slip-weakening friction with its prestress and strength), the
+//   stage-1 fault outputs, rotation back and the characteristic SAT vector
+//   of the calling side.
+// Side 1 (the reference's ib = 2) is block 1's q-max face and side 2 (ib = 1)
+// block 2's q-min face; both read the same two face traces and each uses its
+// own face basis, metric and coordinates, as the reference's two calls do.
+// The SAT vectors go to sat_m / sat_p, which the stage kernels subtract at the
+// face points (DF -= tau0/hq * sat) after the physical-boundary SATs.
+//
+// Slip S (3 components + cumulative |V|) and the state W live here in FP64
+// for both field precisions: S = S + B dt DS after DS = A DS + (Q - P).
+// The friction law reads S before this stage's update, like Interface_RHS
+// reads I%S before update_fields.
 #pragma once
 
+#include <cmath>
 #include <vector>
 
 #include "wql3d.h"
@@ -10,27 +31,442 @@ namespace wql3d {
 
 struct IfaceDev {
   int ny = 0, nz = 0;
+  int coupling = WQL3D_IFACE_LOCKED;
+  int serial = 0;          // 1: both sides accumulate DS (one-process two-block reading)
+  double fd = 0.525, Dc = 0.4;
+  double *S = nullptr, *DS = nullptr;     // 4 x n
+  double *W = nullptr, *DW = nullptr;     // n
+  double *Svel = nullptr;                 // 3 x n (stage 1)
+  double *Uhat = nullptr, *Vhat = nullptr;// 6 x n (stage 1)
+  double *trup = nullptr;                 // n
+  double *t0[2] = {nullptr, nullptr};     // per side: 3 x n initial tractions n, m, l
+  double *fs[2] = {nullptr, nullptr};     // per side: n static friction
   void *sat_m = nullptr;   // SAT vector added at block 1's q-max face (F_x)
   void *sat_p = nullptr;   // SAT vector added at block 2's q-min face (G_x)
 };
 
+// boxcar of unit amplitude on (-w, w), 1/2 within 100 eps of the edges
+// (src/Interface_Condition.f90:2438-2457)
+inline double host_boxcar(double x, double w) {
+  const double tol = 100.0 * 2.220446049250313e-16;
+  if (-w + tol < x && x < w - tol) return 1.0;
+  if (std::fabs(-w - x) <= tol || std::fabs(x - w) <= tol) return 0.5;
+  return 0.0;
+}
+
+// TPV5 prestress and static friction at one fault point
+// (src/Interface_Condition.f90:1822-1830 and 1283-1294)
+inline void tpv5_point(const double x[3], double *T0n, double *T0m, double *T0l, double *fs) {
+  double tl = 70.0;
+  tl = tl + 8.0 * host_boxcar(x[1] - 7.5, 1.5) * host_boxcar(x[2] + 7.5, 1.5);
+  tl = tl + 11.6 * host_boxcar(x[1] - 7.5, 1.5) * host_boxcar(x[2], 1.5);
+  tl = tl - 8.0 * host_boxcar(x[1] - 7.5, 1.5) * host_boxcar(x[2] - 7.5, 1.5);
+  *T0n = -120.0;
+  *T0m = 0.0;
+  *T0l = tl;
+  *fs = 0.677 + 1.0e10 * (1.0 - host_boxcar(x[1], 15.0) * host_boxcar(x[2], 15.0));
+}
+
+// Allocate the interface state and build the per-side prestress / strength
+// maps.  coords0 / coords1: host coordinates of the two blocks (3 x nq*nr*ns,
+// x fastest); nq0 is block 1's q extent.
+template <typename T, typename AllocT>
+int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, const Blk<T> &b1,
+                const std::vector<double> &coords0, const std::vector<double> &coords1, AllocT &mem,
+                cudaStream_t s) {
+  if (b0.ny != b1.ny || b0.nz != b1.nz) return WQL3D_EINVAL;
+  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_LINEAR) return WQL3D_EINVAL;
+  if (desc.fault_problem != WQL3D_FAULT_MAPS && desc.fault_problem != WQL3D_FAULT_TPV5) return WQL3D_EINVAL;
+  const int ny = b0.ny, nz = b0.nz;
+  const long long n = (long long)ny * nz;
+  I.ny = ny;
+  I.nz = nz;
+  I.coupling = desc.coupling;
+  I.serial = desc.serial_shared ? 1 : 0;
+  I.fd = desc.fd;
+  I.Dc = desc.Dc;
+  if (mem.get(&I.S, 4 * n) || mem.get(&I.DS, 4 * n) || mem.get(&I.W, n) || mem.get(&I.DW, n) ||
+      mem.get(&I.Svel, 3 * n) || mem.get(&I.Uhat, 6 * n) || mem.get(&I.Vhat, 6 * n) || mem.get(&I.trup, n))
+    return WQL3D_ENOMEM;
+  T *sm = nullptr, *sp = nullptr;
+  if (mem.get(&sm, 9 * n) || mem.get(&sp, 9 * n)) return WQL3D_ENOMEM;
+  I.sat_m = sm;
+  I.sat_p = sp;
+  // trup starts at 1e9 (src/iface.f90); DS / DW start at 1e40 in the reference
+  // and are multiplied by A(1) = 0 before first use, so zero is equivalent.
+  std::vector<double> tr((size_t)n, 1.0e9);
+  if (cudaMemcpyAsync(I.trup, tr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return WQL3D_ECUDA;
+  const int nq[2] = {b0.nx, b1.nx};
+  const std::vector<double> *cs[2] = {&coords0, &coords1};
+  for (int side = 0; side < 2; ++side) {
+    std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs);
+    const int xend = side == 0 ? nq[0] : 1;
+    const long long nb = (long long)nq[side] * ny * nz;
+    for (int z = 1; z <= nz; ++z)
+      for (int y = 1; y <= ny; ++y) {
+        long long k = (long long)(y - 1) + (long long)ny * (z - 1);
+        if (desc.fault_problem == WQL3D_FAULT_TPV5) {
+          long long q = (long long)(xend - 1) + (long long)nq[side] * ((y - 1) + (long long)ny * (z - 1));
+          double x[3] = {(*cs[side])[(size_t)q], (*cs[side])[(size_t)(nb + q)], (*cs[side])[(size_t)(2 * nb + q)]};
+          tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
+        } else {
+          if (desc.iface_tau0)
+            for (int c = 0; c < 3; ++c) t0[(size_t)(c * n + k)] = desc.iface_tau0[c * n + k];
+          if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
+        }
+      }
+    if (mem.get(&I.t0[side], 3 * n) || mem.get(&I.fs[side], n)) return WQL3D_ENOMEM;
+    if (cudaMemcpyAsync(I.t0[side], t0.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(I.fs[side], f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return WQL3D_ECUDA;
+  }
+  // the host vectors above go out of scope: finish the copies first
+  if (cudaStreamSynchronize(s) != cudaSuccess) return WQL3D_ECUDA;
+  return WQL3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-point interface law in the (n, m, l) basis
+// ---------------------------------------------------------------------------
+struct IfacePoint {
+  double p[3], q[3], phi[3], eta_p, eta_s;
+};
+
+__device__ __forceinline__ void iface_characteristics(const double *U, const double *V, double Z1s, double Z2s,
+                                                      double Z1p, double Z2p, IfacePoint &c) {
+  // common head of Welded_Interface / Linear_Friction / Slip_Weakening_Friction
+  c.p[0] = __dsub_rn(__dmul_rn(Z1p, U[0]), U[3]);
+  c.p[1] = __dsub_rn(__dmul_rn(Z1s, U[1]), U[4]);
+  c.p[2] = __dsub_rn(__dmul_rn(Z1s, U[2]), U[5]);
+  c.q[0] = __dadd_rn(__dmul_rn(Z2p, V[0]), V[3]);
+  c.q[1] = __dadd_rn(__dmul_rn(Z2s, V[1]), V[4]);
+  c.q[2] = __dadd_rn(__dmul_rn(Z2s, V[2]), V[5]);
+  c.eta_p = 1.0 / (1.0 / Z1p + 1.0 / Z2p);
+  c.eta_s = 1.0 / (1.0 / Z1s + 1.0 / Z2s);
+  c.phi[0] = __dmul_rn(c.eta_p, __dsub_rn(c.q[0] / Z2p, c.p[0] / Z1p));
+  c.phi[1] = __dmul_rn(c.eta_s, __dsub_rn(c.q[1] / Z2s, c.p[1] / Z1s));
+  c.phi[2] = __dmul_rn(c.eta_s, __dsub_rn(c.q[2] / Z2s, c.p[2] / Z1s));
+}
+
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1])), __dmul_rn(a[2], b[2]));
+}
+
+// Interface law at one point: P (side-1 hats) and Q (side-2 hats) from the
+// rotated traces U, V.  T0 / fs: this side's prestress and static friction.
+__device__ void iface_law(const IfaceDev &I, const double *U, const double *V, double Z1s, double Z2s, double Z1p,
+                          double Z2p, const double T0[3], double fsk, double slip, double *P, double *Q) {
+  IfacePoint c;
+  iface_characteristics(U, V, Z1s, Z2s, Z1p, Z2p, c);
+  P[0] = __dsub_rn(c.q[0], c.phi[0]) / Z2p;
+  P[3] = c.phi[0];
+  Q[0] = __dadd_rn(c.p[0], c.phi[0]) / Z1p;
+  Q[3] = c.phi[0];
+  if (I.coupling == WQL3D_IFACE_SLIP_WEAKENING) {
+    // Slip_Weakening_Friction + solve('slip-weakening_friction'),
+    // src/Interface_Condition.f90:745-916, 1095-1168
+    const double T0n = T0[0], T0m = T0[1], T0l = T0[2];
+    const double al = __dadd_rn(T0l, c.phi[2]), am = __dadd_rn(T0m, c.phi[1]);
+    const double tau_lock = sqrt(__dadd_rn(__dmul_rn(al, al), __dmul_rn(am, am)));
+    const double sigma_n = fmax(0.0, -__dadd_rn(T0n, c.phi[0]));
+    // Tau_strength: f = fs - (fs - fd) min(D, Dc) / Dc
+    const double f = __dsub_rn(fsk, __dmul_rn(__dsub_rn(fsk, I.fd), fmin(slip, I.Dc)) / I.Dc);
+    const double tau_str = __dmul_rn(sigma_n, f);
+    double tm, tl, vm, vl;
+    if (tau_lock > tau_str) {
+      const double phi1 = am, phi2 = al;
+      const double Phi = sqrt(__dadd_rn(__dmul_rn(phi1, phi1), __dmul_rn(phi2, phi2)));
+      const double Vs = __dsub_rn(Phi, tau_str) / c.eta_s;
+      const double den = __dadd_rn(c.eta_s, tau_str / Vs);
+      vm = phi1 / den;
+      vl = phi2 / den;
+      tm = __dsub_rn(__dsub_rn(phi1, __dmul_rn(c.eta_s, vm)), T0m);
+      tl = __dsub_rn(__dsub_rn(phi2, __dmul_rn(c.eta_s, vl)), T0l);
+    } else {
+      tm = c.phi[1];
+      tl = c.phi[2];
+      vm = 0.0;
+      vl = 0.0;
+    }
+    Q[1] = __dadd_rn(__dadd_rn(tm, c.p[1]) / Z1s, vm);
+    Q[2] = __dadd_rn(__dadd_rn(tl, c.p[2]) / Z1s, vl);
+    P[1] = __dsub_rn(__dsub_rn(c.q[1], tm) / Z2s, vm);
+    P[2] = __dsub_rn(__dsub_rn(c.q[2], tl) / Z2s, vl);
+    P[4] = tm; P[5] = tl; Q[4] = tm; Q[5] = tl;
+  } else if (I.coupling == WQL3D_IFACE_LINEAR) {
+    // Linear_Friction with alpha = 1e14, src/Interface_Condition.f90:601-741
+    // (the reference leaves u_out(2) unassigned; it is set to u_m_hat here)
+    const double alpha = 1.0e14;
+    const double ae = __dadd_rn(alpha, c.eta_s);
+    const double tm = __dmul_rn(alpha / ae, c.phi[1]);
+    const double tl = __dmul_rn(alpha / ae, c.phi[2]);
+    P[4] = tm; P[5] = tl; Q[4] = tm; Q[5] = tl;
+    Q[1] = __dadd_rn(__dadd_rn(c.p[1], tm) / Z1s, __dmul_rn(1.0 / ae, c.phi[1]));
+    Q[2] = __dadd_rn(__dadd_rn(c.p[2], tl) / Z1s, __dmul_rn(1.0 / ae, c.phi[2]));
+    P[1] = __dsub_rn(__dsub_rn(c.q[1], tm) / Z2s, __dmul_rn(1.0 / ae, c.phi[1]));
+    P[2] = __dsub_rn(__dsub_rn(c.q[2], tl) / Z2s, __dmul_rn(1.0 / ae, c.phi[2]));
+  } else {
+    // Welded_Interface, src/Interface_Condition.f90:504-598
+    P[2] = __dsub_rn(c.q[2], c.phi[2]) / Z2s; P[5] = c.phi[2];
+    Q[2] = __dadd_rn(c.p[2], c.phi[2]) / Z1s; Q[5] = c.phi[2];
+    P[1] = __dsub_rn(c.q[1], c.phi[1]) / Z2s; P[4] = c.phi[1];
+    Q[1] = __dadd_rn(c.p[1], c.phi[1]) / Z1s; Q[4] = c.phi[1];
+  }
+}
+
+__device__ __forceinline__ void rot_in(double *w, const double n[3], const double m[3], const double l[3]) {
+  // Rotate_in_Local_Cordinates, src/CouplingForcing.f90:466-520
+  const double a[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
+  w[0] = dot3(n, a);
+  w[1] = dot3(m, a);
+  w[2] = dot3(l, a);
+  w[3] = dot3(n, a + 3);
+  w[4] = dot3(m, a + 3);
+  w[5] = dot3(l, a + 3);
+}
+
+__device__ __forceinline__ void rot_back(double *w, const double n[3], const double m[3], const double l[3]) {
+  // Rotate_Back_Physical_Cordinates, src/CouplingForcing.f90:524-580
+  const double a[6] = {w[0], w[1], w[2], w[3], w[4], w[5]};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    w[i] = __dadd_rn(__dadd_rn(__dmul_rn(n[i], a[0]), __dmul_rn(m[i], a[1])), __dmul_rn(l[i], a[2]));
+    w[3 + i] = __dadd_rn(__dadd_rn(__dmul_rn(n[i], a[3]), __dmul_rn(m[i], a[4])), __dmul_rn(l[i], a[5]));
+  }
+}
+
+// SAT vector of one side from grid (g) and hat (h) values in x, y, z
+// components, src/CouplingForcing.f90:250-437 (side 1: p = (Z u + T)/2 with
+// block 1's impedances; side 2: q = (Z v - T)/2 with block 2's, stress rows
+// negated).
+__device__ void iface_sat(int side, const double *g, const double *h, double lam, double mu, double rho,
+                          const double n[3], const double m[3], const double l[3], double qx, double qy,
+                          double qz, double *out) {
+  const double c_p = sqrt(__dadd_rn(__dmul_rn(2.0, mu), lam) / rho), c_s = sqrt(mu / rho);
+  const double Zp = __dmul_rn(rho, c_p), Zs = __dmul_rn(rho, c_s);
+  const double norm = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(qx, qx), __dmul_rn(qy, qy)), __dmul_rn(qz, qz)));
+  const double *e[3] = {n, m, l};
+  double Mz[3][3], Mi[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      Mz[i][j] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(e[i][0], e[j][0]), Zp), __dmul_rn(__dmul_rn(e[i][1], e[j][1]), Zs)),
+                           __dmul_rn(__dmul_rn(e[i][2], e[j][2]), Zs));
+      Mi[i][j] = __dadd_rn(__dadd_rn(__dmul_rn(e[i][0], e[j][0]) / Zp, __dmul_rn(e[i][1], e[j][1]) / Zs),
+                           __dmul_rn(e[i][2], e[j][2]) / Zs);
+    }
+  double dch[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double sh = __dadd_rn(__dadd_rn(__dmul_rn(Mz[i][0], h[0]), __dmul_rn(Mz[i][1], h[1])), __dmul_rn(Mz[i][2], h[2]));
+    double sg = __dadd_rn(__dadd_rn(__dmul_rn(Mz[i][0], g[0]), __dmul_rn(Mz[i][1], g[1])), __dmul_rn(Mz[i][2], g[2]));
+    sh = side == 1 ? __dadd_rn(sh, h[3 + i]) : __dsub_rn(sh, h[3 + i]);
+    sg = side == 1 ? __dadd_rn(sg, g[3 + i]) : __dsub_rn(sg, g[3 + i]);
+    dch[i] = __dsub_rn(__dmul_rn(0.5, sg), __dmul_rn(0.5, sh));
+  }
+  double r[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    r[i] = __dadd_rn(__dadd_rn(__dmul_rn(Mi[i][0], dch[0]), __dmul_rn(Mi[i][1], dch[1])), __dmul_rn(Mi[i][2], dch[2]));
+  const double l2m = __dadd_rn(__dmul_rn(2.0, mu), lam);
+  const double nr = norm / rho;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) out[i] = __dmul_rn(nr, dch[i]);
+  double s3 = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(l2m, qx), r[0]), __dmul_rn(__dmul_rn(lam, qy), r[1])), __dmul_rn(__dmul_rn(lam, qz), r[2]));
+  double s4 = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(l2m, qy), r[1]), __dmul_rn(__dmul_rn(lam, qz), r[2])), __dmul_rn(__dmul_rn(lam, qx), r[0]));
+  double s5 = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(l2m, qz), r[2]), __dmul_rn(__dmul_rn(lam, qy), r[1])), __dmul_rn(__dmul_rn(lam, qx), r[0]));
+  double s6 = __dmul_rn(mu, __dadd_rn(__dmul_rn(qy, r[0]), __dmul_rn(qx, r[1])));
+  double s7 = __dmul_rn(mu, __dadd_rn(__dmul_rn(qz, r[0]), __dmul_rn(qx, r[2])));
+  double s8 = __dmul_rn(mu, __dadd_rn(__dmul_rn(qz, r[1]), __dmul_rn(qy, r[2])));
+  const double sg = side == 1 ? 1.0 : -1.0;
+  out[3] = sg * s3; out[4] = sg * s4; out[5] = sg * s5;
+  out[6] = sg * s6; out[7] = sg * s7; out[8] = sg * s8;
+}
+
 template <typename T>
-int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, Blk<T> &b0, Blk<T> &b1, std::vector<void *> &ptrs,
-                int64_t &bytes, cudaStream_t s) {
-  (void)I; (void)desc; (void)b0; (void)b1; (void)ptrs; (void)bytes; (void)s;
-  return WQL3D_EINVAL;
+__global__ void __launch_bounds__(128) k_iface(Blk<T> b0, Blk<T> b1, IfaceDev I, StageArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = I.ny * I.nz;
+  if (k >= n) return;
+  const int y = k % I.ny + 1, z = k / I.ny + 1;
+  const T *F0 = a.cur ? b0.F1 : b0.F0;
+  const T *F1 = a.cur ? b1.F1 : b1.F0;
+  const long long p0 = pidx(b0, b0.nx, y, z), p1 = pidx(b1, 1, y, z);
+  double uF[9], vF[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    uF[c] = (double)F0[c * b0.vol + p0];
+    vF[c] = (double)F1[c * b1.vol + p1];
+  }
+  const double lam1 = (double)b0.M[p0], mu1 = (double)b0.M[b0.vol + p0], rho1 = (double)b0.M[2 * b0.vol + p0];
+  const double lam2 = (double)b1.M[p1], mu2 = (double)b1.M[b1.vol + p1], rho2 = (double)b1.M[2 * b1.vol + p1];
+  const double c1p = sqrt(__dadd_rn(__dmul_rn(2.0, mu1), lam1) / rho1), c1s = sqrt(mu1 / rho1);
+  const double c2p = sqrt(__dadd_rn(__dmul_rn(2.0, mu2), lam2) / rho2), c2s = sqrt(mu2 / rho2);
+  const double Z1s = __dmul_rn(rho1, c1s), Z2s = __dmul_rn(rho2, c2s);
+  const double Z1p = __dmul_rn(rho1, c1p), Z2p = __dmul_rn(rho2, c2p);
+
+  double ds[4], S4;
+  if (a.flags & F_ISAT) {
+    S4 = I.S[3 * n + k];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ds[c] = I.DS[c * n + k];
+    if (a.flags & F_SCALE) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ds[c] = __dmul_rn(a.A, ds[c]);
+    }
+    for (int side = 1; side <= 2; ++side) {
+      const Blk<T> &b = side == 1 ? b0 : b1;
+      const long long p = side == 1 ? p0 : p1;
+      const T *B = b.nrm[side == 1 ? 1 : 0];   // face basis l(3) m(3) n(3), face-local (y, z)
+      double n3[3], m3[3], l3[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        l3[c] = (double)B[(0 + c) * n + k];
+        m3[c] = (double)B[(3 + c) * n + k];
+        n3[c] = (double)B[(6 + c) * n + k];
+      }
+      // tractions T = sigma n and velocities, src/CouplingForcing.f90:99-165
+      double u[6], v[6];
+      u[0] = uF[0]; u[1] = uF[1]; u[2] = uF[2];
+      v[0] = vF[0]; v[1] = vF[1]; v[2] = vF[2];
+      {
+        const double su[3] = {uF[3], uF[6], uF[7]}, su2[3] = {uF[6], uF[4], uF[8]}, su3[3] = {uF[7], uF[8], uF[5]};
+        const double sv[3] = {vF[3], vF[6], vF[7]}, sv2[3] = {vF[6], vF[4], vF[8]}, sv3[3] = {vF[7], vF[8], vF[5]};
+        u[3] = dot3(n3, su); u[4] = dot3(n3, su2); u[5] = dot3(n3, su3);
+        v[3] = dot3(n3, sv); v[4] = dot3(n3, sv2); v[5] = dot3(n3, sv3);
+      }
+      rot_in(u, n3, m3, l3);
+      rot_in(v, n3, m3, l3);
+      const double T0[3] = {I.t0[side - 1][k], I.t0[side - 1][n + k], I.t0[side - 1][2 * n + k]};
+      double P[6], Q[6];
+      iface_law(I, u, v, Z1s, Z2s, Z1p, Z2p, T0, I.fs[side - 1][k], S4, P, Q);
+      const double Vel = sqrt(__dadd_rn(__dmul_rn(__dsub_rn(Q[1], P[1]), __dsub_rn(Q[1], P[1])),
+                                        __dmul_rn(__dsub_rn(Q[2], P[2]), __dsub_rn(Q[2], P[2]))));
+      if (side == 1 || I.serial) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ds[c] = __dsub_rn(__dadd_rn(ds[c], Q[c]), P[c]);
+        ds[3] = __dadd_rn(ds[3], Vel);
+      }
+      if (a.stage == 1 && (side == 1 || I.serial)) {
+        // fault outputs, src/Interface_Condition.f90:470-486 and
+        // src/CouplingForcing.f90:203-215 (components 1:3 = v_hat - u_hat)
+        const double Tn = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[0];
+        const double Tm = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[1];
+        const double Tl = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double sv = __dsub_rn(Q[c], P[c]);
+          I.Uhat[c * n + k] = sv;
+          I.Vhat[c * n + k] = sv;
+          I.Svel[c * n + k] = sv;
+        }
+        I.Uhat[3 * n + k] = __dadd_rn(P[3], Tn); I.Vhat[3 * n + k] = __dadd_rn(Q[3], Tn);
+        I.Uhat[4 * n + k] = __dadd_rn(P[4], Tm); I.Vhat[4 * n + k] = __dadd_rn(Q[4], Tm);
+        I.Uhat[5 * n + k] = __dadd_rn(P[5], Tl); I.Vhat[5 * n + k] = __dadd_rn(Q[5], Tl);
+        // rupture_front, src/CouplingForcing.f90:583-600
+        const double s1 = __dsub_rn(Q[1], P[1]), s2 = __dsub_rn(Q[2], P[2]);
+        if (sqrt(__dadd_rn(__dmul_rn(s1, s1), __dmul_rn(s2, s2))) > 1.0e-3) I.trup[k] = fmin(I.trup[k], a.time->t);
+      }
+      rot_back(u, n3, m3, l3);
+      rot_back(v, n3, m3, l3);
+      rot_back(P, n3, m3, l3);
+      rot_back(Q, n3, m3, l3);
+      // metric of the calling block at its interface face (q1 = q2)
+      const double qx = (double)b.met[(long long)0 * b.vol + p];
+      const double qy = (double)b.met[(long long)3 * b.vol + p];
+      const double qz = (double)b.met[(long long)6 * b.vol + p];
+      double sat[9];
+      if (side == 1) iface_sat(1, u, P, lam1, mu1, rho1, n3, m3, l3, qx, qy, qz, sat);
+      else iface_sat(2, v, Q, lam2, mu2, rho2, n3, m3, l3, qx, qy, qz, sat);
+      T *out = (T *)(side == 1 ? I.sat_m : I.sat_p);
+#pragma unroll
+      for (int c = 0; c < 9; ++c) out[c * n + k] = (T)sat[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) I.DS[c * n + k] = ds[c];
+    if (a.flags & F_SCALE) I.DW[k] = __dmul_rn(a.A, I.DW[k]);
+  }
+  if (a.flags & F_UPDATE) {
+    // update_fields for the interface (src/iface.f90): S = S + B dt DS
+#pragma unroll
+    for (int c = 0; c < 4; ++c) I.S[c * n + k] = __dadd_rn(I.S[c * n + k], __dmul_rn(a.Bdt, I.DS[c * n + k]));
+    I.W[k] = __dadd_rn(I.W[k], __dmul_rn(a.Bdt, I.DW[k]));
+  }
+}
+
+__global__ void k_iface_scale(IfaceDev I, double A) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = I.ny * I.nz;
+  if (k >= n) return;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) I.DS[c * n + k] = __dmul_rn(A, I.DS[c * n + k]);
+  I.DW[k] = __dmul_rn(A, I.DW[k]);
 }
 
 template <typename T>
 void launch_iface(IfaceDev &I, const Blk<T> &b0, const Blk<T> &b1, const StageArgs &a, cudaStream_t s) {
-  (void)I; (void)b0; (void)b1; (void)a; (void)s;
+  const int n = I.ny * I.nz;
+  k_iface<T><<<(n + 127) / 128, 128, 0, s>>>(b0, b1, I, a);
 }
 
 template <typename T>
-void launch_iface_update(IfaceDev &I, const StageArgs &a, cudaStream_t s) { (void)I; (void)a; (void)s; }
+void launch_iface_update(IfaceDev &I, const Blk<T> &b0, const Blk<T> &b1, double Bdt, cudaStream_t s) {
+  StageArgs a;
+  a.cur = 0;
+  a.flags = F_UPDATE;
+  a.stage = 0;
+  a.A = 1.0;
+  a.Bdt = Bdt;
+  a.dt = 0.0;
+  a.time = nullptr;
+  const int n = I.ny * I.nz;
+  k_iface<T><<<(n + 127) / 128, 128, 0, s>>>(b0, b1, I, a);
+}
 
-inline void iface_scale(IfaceDev &I, double A, cudaStream_t s) { (void)I; (void)A; (void)s; }
+inline void iface_scale(IfaceDev &I, double A, cudaStream_t s) {
+  const int n = I.ny * I.nz;
+  k_iface_scale<<<(n + 127) / 128, 128, 0, s>>>(I, A);
+}
 
-inline int iface_download(IfaceDev &I, double *out, cudaStream_t s) { (void)I; (void)out; (void)s; return WQL3D_EINVAL; }
+// per point S(4) W Svel(|m,l| slip rate at stage 1) trup, like the oracle's orc_get_iface
+inline int iface_download(IfaceDev &I, double *out, cudaStream_t s) {
+  const long long n = (long long)I.ny * I.nz;
+  std::vector<double> S((size_t)(4 * n)), W((size_t)n), V((size_t)(3 * n)), tr((size_t)n);
+  if (cudaMemcpyAsync(S.data(), I.S, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(W.data(), I.W, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(V.data(), I.Svel, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(tr.data(), I.trup, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return WQL3D_ECUDA;
+  for (long long k = 0; k < n; ++k) {
+    for (int c = 0; c < 4; ++c) out[7 * k + c] = S[(size_t)(c * n + k)];
+    out[7 * k + 4] = W[(size_t)k];
+    out[7 * k + 5] = std::sqrt(V[(size_t)(n + k)] * V[(size_t)(n + k)] + V[(size_t)(2 * n + k)] * V[(size_t)(2 * n + k)]);
+    out[7 * k + 6] = tr[(size_t)k];
+  }
+  return WQL3D_OK;
+}
+
+// one fault output (WQL3D_FO_*), layout [component][z][y]
+inline int iface_fault_output(IfaceDev &I, int kind, double *out, cudaStream_t s) {
+  const long long n = (long long)I.ny * I.nz;
+  const double *src = nullptr;
+  int nc = 0;
+  switch (kind) {
+    case WQL3D_FO_S: src = I.S; nc = 4; break;
+    case WQL3D_FO_SVEL: src = I.Svel; nc = 3; break;
+    case WQL3D_FO_UHAT: src = I.Uhat; nc = 6; break;
+    case WQL3D_FO_VHAT: src = I.Vhat; nc = 6; break;
+    case WQL3D_FO_STATE: src = I.W; nc = 1; break;
+    case WQL3D_FO_TRUP: src = I.trup; nc = 1; break;
+    default: return WQL3D_EINVAL;
+  }
+  if (cudaMemcpyAsync(out, src, sizeof(double) * nc * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return WQL3D_ECUDA;
+  return WQL3D_OK;
+}
 
 }  // namespace wql3d

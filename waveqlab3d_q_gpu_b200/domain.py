@@ -31,7 +31,7 @@ from typing import List, Optional, Tuple
 import numpy as np
 
 from . import _lib
-from .problem import COUPLINGS, RESPONSES, RK_A, RK_B, RK_C, STF_CODES, Problem
+from .problem import COUPLINGS, FAULT_PROBLEMS, RESPONSES, RK_A, RK_B, RK_C, STF_CODES, Problem
 
 
 @dataclass
@@ -89,6 +89,7 @@ class Domain:
         ip = problem.interface
         d.coupling = COUPLINGS[ip.coupling]
         d.serial_shared = 1 if ip.serial_shared else 0
+        d.fault_problem = FAULT_PROBLEMS[ip.problem]
         d.fs, d.fd, d.Dc = ip.fs, ip.fd, ip.Dc
         if nb == 2:
             nq, nr, ns = problem.blocks[0].nqrs
@@ -264,6 +265,18 @@ class Domain:
         nq, nr, ns = self.problem.blocks[0].nqrs
         a = np.zeros((ns, nr, 7))
         _lib.check(_lib.load().wql3d_get_interface(self.handle, _ptr(a)), "wql3d_get_interface")
+        return a
+
+    FAULT_KINDS = {"S": (0, 4), "Svel": (1, 3), "Uhat": (2, 6), "Vhat": (3, 6), "state": (4, 1), "trup": (5, 1)}
+
+    def fault(self, name: str) -> np.ndarray:
+        """One fault output (``S``, ``Svel``, ``Uhat``, ``Vhat``, ``state``, ``trup``) as
+        (ncomp, ns, nr), the layout of the reference's ``_interface.*`` files
+        (src/fault_output.f90:73-122); ``Uface`` / ``Vface`` come from :meth:`fields`."""
+        kind, nc = self.FAULT_KINDS[name]
+        nq, nr, ns = self.problem.blocks[0].nqrs
+        a = np.zeros((nc, ns, nr))
+        _lib.check(_lib.load().wql3d_get_fault_output(self.handle, kind, _ptr(a)), "wql3d_get_fault_output")
         return a
 
     def seismograms(self, b: int = 0) -> np.ndarray:

@@ -35,6 +35,8 @@ STF_CODES = {
 RESPONSES = {"elastic": 0, "anelastic-Q4": 1, "anelastic-Q8": 2, "anelastic-fQ8": 3}
 
 COUPLINGS = {"locked": 0, "slip-weakening_friction": 1, "linear_friction": 2}
+# fault prestress / strength: per-point maps, or the reference's TPV5 formulas
+FAULT_PROBLEMS = {None: 0, "maps": 0, "TPV5": 1}
 
 # Kennedy-Carpenter (5,4) low-storage coefficients, src/time_step.f90:53-62
 RK_A = (
@@ -152,7 +154,13 @@ class InterfaceParams:
     tau0_m: Optional[np.ndarray] = None   # (ns, nr) initial shear traction along m
     tau0_l: Optional[np.ndarray] = None   # (ns, nr) initial shear traction along l
     fs_map: Optional[np.ndarray] = None   # (ns, nr) static friction map
-    serial_shared: bool = True            # DS accumulated once per block side (serial run)
+    # True: both sides' interface solves add to the slip rate, as in the
+    # reference's one-process two-block run (src/domain.f90:615-644 calls
+    # Interface_RHS once per block on one shared iface); False: once per
+    # stage, as in its one-rank-per-block run, which the archived rupture
+    # output (test_problems/truth/1) follows.
+    serial_shared: bool = False
+    problem: Optional[str] = None         # 'TPV5': prestress and strength of src/Interface_Condition.f90
 
 
 @dataclass
