@@ -1,22 +1,28 @@
 #!/usr/bin/env python3
 """Benchmark of the B200-native WaveQLab3D per-step volume update.
 
-Workload (one "step" = one low-storage RK time step of the whole block):
-plain FP64, one Cartesian block of 101^3 points at h = 0.1 km, homogeneous
-elastic medium (Vp 6 km/s, Vs 3.464 km/s, rho 2.67 g/cm^3), traditional
-6th-order SBP, free-surface SAT on the q-min face and characteristic
-absorbing SAT on the other five, explosive moment-tensor source at the
-centre with a Ricker wavelet f0 = 2 Hz, CFL 0.5, a 10 x 10 receiver grid on
-the free surface.  The default --steps 500 is the configuration's full run.
-Inputs are synthetic (generated here; there is no dataset).
+Default workload (``--workload hill``): the curvilinear two-block Q8 + PML
+problem.  A 201 x 201 x 201-point domain at h = 0.05 km split at mid-depth
+into two 101 x 201 x 201 blocks joined by a locked q-interface; Gaussian-hill
+topography (0.8 km, sigma 2.5 km) with seeded random bumps; Vs layered
+2.0 -> 3.5 km/s, Vp = sqrt(3) Vs, rho = 1.7 + 0.2 Vp; Q8 with per-point
+Qs = 50 Vs, Qp = 2 Qs; free surface on top, 20-point PML on the sides and
+bottom; seeded double-couple with a Ricker wavelet f0 = 3 Hz; 10 x 10
+surface stations.  One "step" is one five-stage low-storage RK time step of
+both blocks and the interface.  The plain FP64 path gives ``value``; the
+FP32 path with compensated state accumulation is measured on the same
+workload and reported under ``fp32`` with its seismogram error against FP64.
 
-Prints one JSON line (rank 0).  ``--impl reference`` times the CPU
-restatement of the reference solver (the Fortran reference needs gfortran
-and MPI, which this image lacks) on the host cores instead.
+``--workload cartesian`` times the plain FP64 single Cartesian 101^3 block
+(explosive Ricker source, free surface on the q-min face) instead.
+
+Inputs are synthetic (generated here; there is no dataset).  Prints one JSON
+line (rank 0).  ``--impl reference`` times the CPU restatement of the
+reference solver on the host cores (the Fortran reference needs gfortran and
+MPI, which this image lacks).
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -29,18 +35,56 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Gpt-updates/s"
 UNIT = "Gpt/s"
-WORDS_PER_POINT_STAGE = 39          # F r/w + DF r/w (9 each) + lambda, mu, rho
-BYTES_PER_WORD = 8
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=101)
+    ap.add_argument("--workload", default="hill", choices=["hill", "cartesian"])
+    ap.add_argument("--n", type=int, default=None, help="points per axis (201 hill, 101 cartesian)")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
+
+
+def make_problem(args, steps):
+    from waveqlab3d_q_gpu_b200.configs import cartesian_101, hill_two_block_q8
+    if args.workload == "cartesian":
+        n = args.n or 101
+        return cartesian_101(n, steps), f"cartesian-elastic-fp64-{n}^3-traditional6-ricker-10x10rec"
+    n = args.n or 201
+    return (hill_two_block_q8(n, steps=steps),
+            f"curvilinear-2block-{n}^3-hill-q8-pml20-locked-ricker3hz-10x10rec")
+
+
+def words_per_stage(problem):
+    """Algorithmic words per RK stage, summed over all points: F r/w and DF r/w
+    (36), lambda mu rho (3), curvilinear metric + J (10), Q4/Q8 memory
+    variables and their rates read and written (24 per mechanism) + Qs^-1,
+    Qp^-1 (2), fQ8 (24 per mechanism), 36 per PML slab a point lies in.
+    Ghost cells, halo re-reads and the O(n^2) face / interface / source terms
+    are not counted."""
+    per_pt = 36 + 3
+    if problem.type_of_mesh == "curvilinear":
+        per_pt += 10
+    nm = problem.nmech
+    if problem.response in ("anelastic-Q4", "anelastic-Q8"):
+        per_pt += 24 * nm + 2
+    elif problem.response == "anelastic-fQ8":
+        per_pt += 24 * nm
+    total = 0
+    for b in problem.blocks:
+        nq, nr, ns = b.nqrs
+        total += per_pt * b.npoints
+        if b.npml > 0:
+            face = {0: nr * ns, 1: nq * ns, 2: nq * nr}
+            for f, on in enumerate(b.pml()):
+                if on:
+                    total += 36 * b.npml * face[f // 2]
+    return total
 
 
 def load_peaks():
@@ -52,13 +96,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic(n):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+def load_traffic(key):
+    """DRAM bytes per RK stage of the stage kernels from the committed ncu summary, if any."""
     try:
         with open(os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")) as f:
             t = json.load(f)
-        rec = t.get(str(n))
-        return None if rec is None else float(rec["dram_bytes_per_launch"])
+        rec = t.get(key)
+        return None if rec is None else float(rec["dram_bytes_per_stage"])
     except Exception:
         return None
 
@@ -117,65 +161,73 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_sample(problem, target_s=12.0, max_steps=40):
-    """Time the CPU oracle (restatement of the reference solver) on a bounded sample."""
+def oracle_steps(problem, steps, warmup, budget_s):
+    """Time the CPU oracle (restatement of the reference solver, OpenMP over
+    z) for at most ``steps`` time steps or ``budget_s`` seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     oracle.build()
     d = oracle.OracleDomain(problem)
-    npts = problem.blocks[0].npoints
-    d.run(1)  # warm-up step
-    steps, t0 = 0, time.perf_counter()
-    while steps < max_steps:
+    for _ in range(warmup):
         d.run(1)
-        steps += 1
-        if time.perf_counter() - t0 > target_s:
+    n, t0 = 0, time.perf_counter()
+    while n < steps:
+        d.run(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
     d.close()
-    return {"value": npts * steps / el / 1e9, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
-            "kind": "port", "sample": f"{steps} RK time steps of the {problem.blocks[0].nqrs[0]}^3 workload "
-                                      f"({el:.1f} s, OpenMP over z)"}, el / steps
+    npts = sum(b.npoints for b in problem.blocks)
+    return npts * n / el / 1e9, n, el, int(os.environ["OMP_NUM_THREADS"])
 
 
 def run_reference(args, rank, world):
-    from waveqlab3d_q_gpu_b200.configs import cartesian_101
     if rank != 0:
         return
-    p = cartesian_101(args.n, max(args.steps, 1))
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    oracle.build()
-    d = oracle.OracleDomain(p)
-    npts = p.blocks[0].npoints
-    for _ in range(min(args.warmup, 2)):
-        d.run(1)
-    # each timed step is one RK time step of the workload; the run is capped
-    # at about three minutes of CPU time
-    t0 = time.perf_counter()
-    steps = 0
-    while steps < args.steps:
-        d.run(1)
-        steps += 1
-        if time.perf_counter() - t0 > 180.0:
-            break
-    el = time.perf_counter() - t0
-    value = npts * steps / el / 1e9
+    p, name = make_problem(args, max(args.steps, 1))
+    value, n, el, cores = oracle_steps(p, args.steps, min(args.warmup, 1), 150.0)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cartesian-elastic-fp64-{args.n}^3-traditional6-ricker-10x10rec"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-                         "sample": f"{steps} RK time steps of the {args.n}^3 workload (CPU restatement of the "
-                                   f"reference solver; the Fortran reference needs gfortran + MPI, absent here)"},
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": name},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n} RK time steps of the workload in {el:.1f} s (CPU restatement of the "
+                                   f"reference solver, OpenMP over z; the Fortran reference needs gfortran + MPI, "
+                                   f"absent here)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def timed_run(g, stream, K, barrier):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    g.run(K)
+    e1.record(stream)
+    g.synchronize()
+    barrier()
+    return e0.elapsed_time(e1)
+
+
+def stage_time(g, stream, dt, nst=20):
+    """Average duration of one RK stage (both blocks' stage kernels and the
+    interface kernel) on the library stream."""
+    import torch
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    g.stage(2, dt)
+    s0.record(stream)
+    for i in range(nst):
+        g.stage(2 + i % 4, dt)
+    s1.record(stream)
+    g.synchronize()
+    return s0.elapsed_time(s1) / nst
 
 
 def main():
@@ -196,15 +248,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from waveqlab3d_q_gpu_b200 import build
     build.build()
-    from waveqlab3d_q_gpu_b200.configs import cartesian_101
     from waveqlab3d_q_gpu_b200.domain import Domain
 
-    K, W = args.steps, args.warmup
-    p = cartesian_101(args.n, K)
-    npts = p.blocks[0].npoints
+    K, W = args.steps, max(args.warmup, 3)
+    p, name = make_problem(args, K + W + 4)
+    npts = sum(b.npoints for b in p.blocks)
     dt = p.dt()
-    g = Domain(p, nsteps_hint=K + W + 4)
-    stream = torch.cuda.ExternalStream(g.stream_handle())
+    nb = len(p.blocks)
 
     def barrier():
         torch.cuda.synchronize()
@@ -212,96 +262,110 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warm-up (also captures the CUDA graph)
-    g.run(W)
-    g.synchronize()
-    barrier()
-    l0 = g.kernel_launches()
-    clocks = ClockSampler(local)
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    g.run(K)
-    e1.record(stream)
-    g.synchronize()
-    barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    launches = g.kernel_launches() - l0
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * npts * K / (ms / 1e3) / 1e9
+        return float(t.item())
 
-    # dominant kernel: the fused stage kernel, timed alone on the library stream
-    nst = 40
-    s0 = torch.cuda.Event(enable_timing=True)
-    s1 = torch.cuda.Event(enable_timing=True)
-    s0.record(stream)
-    for i in range(nst):
-        g.stage(1 + i % 4, dt)
-    s1.record(stream)
-    g.synchronize()
-    stage_ms = s0.elapsed_time(s1) / nst
     peak, peak_kind = load_peaks()
-    alg_bytes = WORDS_PER_POINT_STAGE * BYTES_PER_WORD * npts
-    achieved = alg_bytes / (stage_ms / 1e3) / 1e9
-    traffic = load_traffic(args.n)
+    words = words_per_stage(p)
+    results = {}
+    precisions = ["fp64"] if args.no_fp32 else ["fp64", "fp32"]
+    clk = None
+    for prec in precisions:
+        g = Domain(p, precision=prec, nsteps_hint=K + W + 4)
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        g.run(W)                      # warm-up, captures the CUDA graph
+        g.synchronize()
+        l0 = g.kernel_launches()
+        clocks = ClockSampler(local) if prec == "fp64" else None
+        if clocks:
+            clocks.start()
+        ms = timed_run(g, stream, K, barrier)
+        if clocks:
+            clk = clocks.stop()
+        launches = g.kernel_launches() - l0
+        ms = max_over_ranks(ms)
+        seis = g.seismograms(0)
+        st_ms = stage_time(g, stream, dt)
+        w = 8 if prec == "fp64" else 4
+        achieved = words * w / (st_ms / 1e3) / 1e9
+        results[prec] = {"ms_per_step": ms / K, "value": world * npts * K / (ms / 1e3) / 1e9,
+                         "launches": int(launches), "stage_ms": st_ms, "achieved": achieved, "seis": seis,
+                         "bytes": g.device_bytes()}
+        g.close()
+        del g
+        torch.cuda.empty_cache()
+    r64 = results["fp64"]
 
     # end to end through the public API with pinned host buffers: upload the
-    # state, run K steps, read back the seismograms and the final fields
-    nq = p.blocks[0].nqrs[0]
-    Fh = torch.zeros((9, nq, nq, nq), dtype=torch.float64, pin_memory=True).numpy()
-    DFh = torch.zeros((9, nq, nq, nq), dtype=torch.float64, pin_memory=True).numpy()
+    # initial fields of both blocks, run K steps, read back the stations and
+    # the final fields of both blocks
+    hosts = []
+    for b in p.blocks:
+        nq, nr, ns = b.nqrs
+        hosts.append(torch.zeros((9, ns, nr, nq), dtype=torch.float64, pin_memory=True).numpy())
     g2 = Domain(p, nsteps_hint=K + 4)
     g2.run(2)
     g2.synchronize()
     g2.t = 0.0
     barrier()
     t0 = time.perf_counter()
-    g2.set_fields(Fh)
-    g2.set_rates_array(DFh)
+    for bi in range(nb):
+        g2.set_fields(hosts[bi], bi)
     g2.run(K)
-    seis = g2.seismograms()
-    g2.fields(out=Fh)
+    seis2 = g2.seismograms(0)
+    for bi in range(nb):
+        g2.fields(bi, out=hosts[bi])
     g2.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    h2d = 2 * Fh.nbytes
-    d2h = Fh.nbytes + seis.nbytes
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = sum(h.nbytes for h in hosts)
+    d2h = sum(h.nbytes for h in hosts) + seis2.nbytes
     e2e = {"value": world * npts * K / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
            "d2h_bytes_per_step": d2h / K,
-           "what": "set_fields + set_rates from pinned host, run K steps, read seismograms + final fields"}
+           "what": "set_fields of both blocks from pinned host, run K steps, read stations + final fields"}
     g2.close()
+    del g2
 
     cpu = None
-    if rank == 0 and world == 1:
-        cpu, _ = cpu_sample(cartesian_101(args.n, K))
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, n, el, cores = oracle_steps(p, 2, 0, 30.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{n} RK time step(s) of the same workload in {el:.1f} s (CPU restatement of the "
+                         f"reference solver, OpenMP over z)"}
 
     if rank == 0:
+        traffic = load_traffic(name)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": r64["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"cartesian-elastic-fp64-{args.n}^3-traditional6-ricker-10x10rec",
-                       "points": npts, "rk_stages_per_step": 5, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (state %.0f MB per GPU)" % (g.device_bytes() / 1e6)},
+            "config": {"workload": name, "points": npts, "blocks": nb, "rk_stages_per_step": 5,
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (%.1f GB on the device per precision run)" % (r64["bytes"] / 1e9),
+                       "timed_steps_of_run": f"{K} of the configuration's 1500"},
             "e2e": e2e,
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_stage<double,cartesian,elastic>", "stage_ms": stage_ms,
-                         "alg_bytes_per_launch": alg_bytes},
+            "gpu_launches": r64["launches"],
+            "roofline": {"bound": "hbm", "achieved": r64["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": r64["achieved"] / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "one RK stage: stage kernels of both blocks + interface kernel",
+                         "stage_ms": r64["stage_ms"], "alg_bytes_per_stage": words * 8},
             "cpu_baseline": cpu,
             "clocks": clk,
         }
+        if "fp32" in results:
+            r32 = results["fp32"]
+            s64, s32 = r64["seis"][:, :, 1:], r32["seis"][:, :, 1:]
+            err = float(np.linalg.norm(s32 - s64) / max(np.linalg.norm(s64), 1e-300))
+            line["fp32"] = {"value": r32["value"], "ms_per_step": r32["ms_per_step"],
+                            "speedup_vs_fp64": r32["value"] / r64["value"],
+                            "roofline": {"achieved": r32["achieved"], "frac": r32["achieved"] / peak,
+                                         "stage_ms": r32["stage_ms"], "alg_bytes_per_stage": words * 4,
+                                         "note": "compensation array (+18 words/pt/stage) not counted"},
+                            "seismogram_rel_l2_vs_fp64": err, "gpu_launches": r32["launches"]}
         print(json.dumps(line), flush=True)
-    g.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -158,6 +158,7 @@ struct wql3d_domain {
   cudaGraphExec_t graph = nullptr;
   double g_dt = 0.0;
   int g_w = -1, g_cur = -1;
+  int64_t g_launches = 0;         // kernels in one replay of the captured two-step graph
   int64_t launches = 0;
   double *red = nullptr;
   int *flag = nullptr;
@@ -440,6 +441,7 @@ int setup_block(wql3d_domain *d, int bi) {
   CK(M.get(&b.DF, 9 * vol));
   CK(M.get(&b.M, 3 * vol));
   if (d->fp32) CK(M.get(&b.FC, 9 * vol));
+  if (bd.mesh == WQL3D_MESH_CURVILINEAR) CK(M.get(&b.G, 18 * vol, false));
   {
     // rates start at the reference's 1e40 sentinel (src/fields.f90:39) in FP64;
     // the first stage scales them by A(1) = 0.  FP32 cannot hold 1e40: zero.
@@ -769,6 +771,21 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
     return;
   }
   dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
+  if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !tuning().generic) {
+    // derivative pass, then the point update of every point
+    if (a.flags & F_RHS) {
+      k_curv_grad<T><<<gr, th, 0, d->stream>>>(b, a.cur);
+      d->launches++;
+    }
+    switch (d->response) {
+      case 0: k_curv_update<T, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
+      case 1: k_curv_update<T, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
+      case 2: k_curv_update<T, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
+      default: k_curv_update<T, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
+    }
+    d->launches++;
+    return;
+  }
   switch (d->response * 2 + mesh) {
     case 0: k_stage<T, MESH_CART, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
     case 1: k_stage<T, MESH_CURV, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
@@ -848,23 +865,10 @@ int run_steps(wql3d_domain *d, double dt, int nsteps, int w_stride) {
       d->g_dt = dt;
       d->g_w = w_stride;
       d->g_cur = cur0;
+      d->g_launches = d->launches - l0;
       d->launches = l0;
     }
-    // launches per replay: count by re-enqueue size
-    int64_t per_pair = 0;
-    {
-      int64_t l0 = d->launches;
-      int cur0 = d->cur;
-      // counting pass without launching: mirror enqueue_step's structure
-      for (int k = 0; k < 2; ++k) {
-        for (int i = 0; i < d->nblocks; ++i) per_pair += d->hb[i].nrec > 0 ? 1 : 0;
-        int per_block = 0;
-        for (int i = 0; i < d->nblocks; ++i) per_block += d->hb[i].mesh == WQL3D_MESH_CARTESIAN ? 2 : 1;
-        per_pair += 5 * (per_block + (d->has_iface ? 1 : 0)) + 1;
-      }
-      d->launches = l0;
-      d->cur = cur0;
-    }
+    const int64_t per_pair = d->g_launches;
     for (int k = 0; k < pairs; ++k) {
       CK(cudaGraphLaunch(d->graph, d->stream));
       d->launches += per_pair;

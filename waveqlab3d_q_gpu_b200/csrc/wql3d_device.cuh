@@ -72,6 +72,7 @@ struct Blk {
   T *F0, *F1;           // field buffers (9 components each)
   T *DF;                // rates (9 components)
   T *FC;                // FP32 path: Kahan compensation for F (9 components)
+  T *G;                 // curvilinear: 18 derivative terms per point from k_curv_grad (see there)
   T *M;                 // lambda, mu, rho
   // Cartesian: per-axis diagonal metric 1/X_a(i) (index 1..n)
   const T *mq, *mr, *ms;
@@ -659,7 +660,7 @@ __device__ void sep_axis(const Blk<T> &b, const T *F, int i, int n, long long p,
 // ---------------------------------------------------------------------------
 // Stage kernel: one thread per grid point.
 // ---------------------------------------------------------------------------
-template <typename T, int MESH, int RESP, bool SEP = false>
+template <typename T, int MESH, int RESP, bool SEP = false, bool GIN = false>
 __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, int z) {
   const long long p = pidx(b, x, y, z);
   const long long V = b.vol;
@@ -686,7 +687,7 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
   // scale / integrate PML rates of points not reached by the RHS path
   const bool rhs = (a.flags & F_RHS) != 0;
 
-  if (rhs && interior) {
+  if (rhs && interior && !GIN) {
     // strict interior, src/JU_xJU_yJU_z6.f90:16177-16636
     T DFx[9], DFy[9], DFz[9];
 #pragma unroll
@@ -772,7 +773,24 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
     T Ux[9], Uy[9], Uz[9];
     const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
     T J, rhoJ_inv;
-    if (SEP) {
+    if (GIN) {
+      // the derivative terms k_curv_grad left for this point
+      const T *Gp = b.G + p;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        Ux[f] = Gp[(0 + f) * V];
+        Uy[f] = Gp[(3 + f) * V];
+        Uz[f] = Gp[(6 + f) * V];
+      }
+      Ux[3] = Gp[9 * V];  Ux[6] = Gp[10 * V]; Ux[7] = Gp[11 * V];
+      Uy[6] = Gp[12 * V]; Uy[4] = Gp[13 * V]; Uy[8] = Gp[14 * V];
+      Uz[7] = Gp[15 * V]; Uz[8] = Gp[16 * V]; Uz[5] = Gp[17 * V];
+      Ux[4] = Ux[5] = Ux[8] = (T)0;
+      Uy[3] = Uy[5] = Uy[7] = (T)0;
+      Uz[3] = Uz[4] = Uz[6] = (T)0;
+      J = ld(b.J + p);
+      rhoJ_inv = (T)1 / (rho * J);
+    } else if (SEP) {
       sep_axis<T>(b, F, x, b.nx, p, 1, ld(b.mq + x), b.ihq, Ux);
       sep_axis<T>(b, F, y, b.ny, p, b.sy, ld(b.mr + y), b.ihr, Uy);
       sep_axis<T>(b, F, z, b.nz, p, b.sz, ld(b.ms + z), b.ihs, Uz);
@@ -890,6 +908,99 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
   const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
   if (x > b.nx || y > b.ny || z > b.nz) return;
   point_update<T, MESH, RESP>(b, a, x, y, z);
+}
+
+// ---------------------------------------------------------------------------
+// Curvilinear stage, first pass: the derivative terms of JJU_x6
+// (src/JU_xJU_yJU_z6.f90:12-809) that the point update uses, for every point
+// of the block, interior and near-boundary alike (the reference's interior
+// form, src/JU_xJU_yJU_z6.f90:16177-16424, is the same operator with the
+// central row, summed in another order).  Per axis a with row coefficients
+// c_k: velocities X_r(p) * (1/h_a) sum_k c_k v(k), stresses
+// (1/h_a) sum_k ((c_k s(k)) J(k)) X_r(k) for the nine (stress, metric row)
+// pairs the rates need.  G holds, component-major with the field stride:
+//   0-8   dv_x/dx, dv_y/dx, dv_z/dx, dv_x/dy, ..., dv_z/dz   (Ux, Uy, Uz 1:3)
+//   9-17  Ux4, Ux7, Ux8, Uy7, Uy5, Uy9, Uz8, Uz9, Uz6        (1-based JJU_x6 slots)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_curv_grad(Blk<T> b, int cur) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (x > b.nx || y > b.ny || z > b.nz) return;
+  const long long p = pidx(b, x, y, z);
+  const long long V = b.vol;
+  const T *F = cur ? b.F1 : b.F0;
+  const int pos[3] = {x, y, z};
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  const long long st[3] = {1, b.sy, b.sz};
+  const T ih[3] = {b.ihq, b.ihr, b.ihs};
+  T U[9], S[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) { U[k] = 0; S[k] = 0; }
+#pragma unroll 1
+  for (int ax = 0; ax < 3; ++ax) {
+    T sv[3] = {0, 0, 0};
+    T acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = 0;
+    const T *X0 = b.met + (long long)(0 * 3 + ax) * V;
+    const T *X1 = b.met + (long long)(1 * 3 + ax) * V;
+    const T *X2 = b.met + (long long)(2 * 3 + ax) * V;
+    auto tap = [&](long long q, T c) {
+      const T Jq = ld(b.J + q);
+      const T x0 = ld(X0 + q), x1 = ld(X1 + q), x2 = ld(X2 + q);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) sv[f] = sv[f] + c * ld(F + f * V + q);
+      const T sxx = c * ld(F + 3 * V + q) * Jq, syy = c * ld(F + 4 * V + q) * Jq;
+      const T szz = c * ld(F + 5 * V + q) * Jq, sxy = c * ld(F + 6 * V + q) * Jq;
+      const T sxz = c * ld(F + 7 * V + q) * Jq, syz = c * ld(F + 8 * V + q) * Jq;
+      acc[0] = acc[0] + sxx * x0; acc[1] = acc[1] + sxy * x0; acc[2] = acc[2] + sxz * x0;
+      acc[3] = acc[3] + sxy * x1; acc[4] = acc[4] + syy * x1; acc[5] = acc[5] + syz * x1;
+      acc[6] = acc[6] + sxz * x2; acc[7] = acc[7] + syz * x2; acc[8] = acc[8] + szz * x2;
+    };
+    const int i = pos[ax], n = nn[ax];
+    if (i >= 7 && i <= n - 6) {
+      const T cc[6] = {(T)(-1.0 / 60.0), (T)0.15, (T)-0.75, (T)0.75, (T)-0.15, (T)(1.0 / 60.0)};
+      const int off[6] = {-3, -2, -1, 1, 2, 3};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) tap(p + (long long)off[k] * st[ax], cc[k]);
+    } else {
+      const int row = i <= 6 ? i - 1 : 6 + (n - i);
+      const double *rc = b.rowc + row * 8;
+      const int *ro = b.rowo + row * 8;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const T c = (T)__ldg(rc + k);
+        if (c != (T)0) tap(p + (long long)__ldg(ro + k) * st[ax], c);
+      }
+    }
+    const T xp[3] = {ld(X0 + p), ld(X1 + p), ld(X2 + p)};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int f = 0; f < 3; ++f) U[r * 3 + f] = U[r * 3 + f] + ih[ax] * (xp[r] * sv[f]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S[k] = S[k] + ih[ax] * acc[k];
+  }
+  T *Gp = b.G + p;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    Gp[k * V] = U[k];
+    Gp[(9 + k) * V] = S[k];
+  }
+}
+
+// Curvilinear stage, second pass: every point through the near-boundary
+// point update with the derivative terms of k_curv_grad (anelastic, PML,
+// sources, SATs, interface SAT, RK update).
+template <typename T, int RESP>
+__global__ void __launch_bounds__(256, 2) k_curv_update(Blk<T> b, StageArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (x > b.nx || y > b.ny || z > b.nz) return;
+  point_update<T, MESH_CURV, RESP, false, true>(b, a, x, y, z);
 }
 
 // Number of near-boundary (shell) points: everything outside the strict
