@@ -615,6 +615,7 @@ int setup_block(wql3d_domain *d, int bi) {
     CK(M.get(&b.deta, (size_t)6 * d->nmech * vol));
     for (int i = 0; i < 8; ++i) {
       b.tau[i] = (T)d->desc.tau[i];
+      b.itau[i] = (T)(1.0 / d->desc.tau[i]);
       b.w[i] = (T)d->desc.weight[i];
       b.ss[i] = (T)d->desc.strength_s[i];
       b.ps[i] = (T)d->desc.strength_p[i];
@@ -698,6 +699,10 @@ struct Tuning {
   int zchunk = 12;
   int generic = 0;   // 1: every point through the generic per-point kernel
   int split = 1;     // interior: two warp groups (velocity / stress rates) with register z-queues
+  int lean = 1;      // curvilinear update: k_curv_point (0: generic point update k_curv_update)
+  int curv_lb = 0;   // k_curv_point threads x min blocks: 0 = 256x2, 1 = 128x3, 2 = 256x1
+  int curv_bx = 32;  // k_curv_point tile width along x (32, 64)
+  int grad_bx = 32;  // k_curv_grad tile width along x (32, 64)
 };
 
 Tuning tuning() {
@@ -705,9 +710,13 @@ Tuning tuning() {
     Tuning r;
     if (const char *e = getenv("WQL3D_TY")) r.ty = atoi(e) == 8 ? 8 : 4;
     if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = std::max(1, atoi(e));
+    if (const char *e = getenv("WQL3D_CURV_LB")) r.curv_lb = std::min(2, std::max(0, atoi(e)));
+    if (const char *e = getenv("WQL3D_CURV_BX")) r.curv_bx = atoi(e) == 64 ? 64 : 32;
+    if (const char *e = getenv("WQL3D_GRAD_BX")) r.grad_bx = atoi(e) == 64 ? 64 : 32;
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
       if (strcmp(e, "ring") == 0) r.split = 0;
+      if (strcmp(e, "curv_generic_update") == 0) r.lean = 0;
     }
     return r;
   }();
@@ -756,6 +765,18 @@ void launch_shell(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
   d->launches++;
 }
 
+template <typename T, int MAXT, int MINB>
+void launch_curv_point(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
+  const int bx = tuning().curv_bx, by = MAXT / bx / 2;
+  dim3 th(bx, by, 2), gr((b.nx + bx - 1) / bx, (b.ny + by - 1) / by, (b.nz + 1) / 2);
+  switch (d->response) {
+    case 0: k_curv_point<T, RESP_EL, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 1: k_curv_point<T, RESP_Q4, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 2: k_curv_point<T, RESP_Q8, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+    default: k_curv_point<T, RESP_FQ8, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+  }
+}
+
 template <typename T>
 void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = false) {
   Blk<T> &b = blk<T>(d, bi);
@@ -774,14 +795,30 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
   if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !tuning().generic) {
     // derivative pass, then the point update of every point
     if (a.flags & F_RHS) {
-      k_curv_grad<T><<<gr, th, 0, d->stream>>>(b, a.cur);
+      const int gbx = tuning().grad_bx, gby = 256 / gbx / 2;
+      dim3 gth(gbx, gby, 2), ggr((b.nx + gbx - 1) / gbx, (b.ny + gby - 1) / gby, (b.nz + 1) / 2);
+      k_curv_grad<T><<<ggr, gth, 0, d->stream>>>(b, a.cur);
       d->launches++;
     }
-    switch (d->response) {
-      case 0: k_curv_update<T, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
-      case 1: k_curv_update<T, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
-      case 2: k_curv_update<T, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
-      default: k_curv_update<T, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
+    // the lean kernel keeps one PML slab per axis: blocks whose two slabs on
+    // an axis overlap (2 npml > n) take the generic update
+    bool overlap = false;
+    const int nax[3] = {b.nx, b.ny, b.nz};
+    for (int ax = 0; ax < 3; ++ax)
+      if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) overlap = true;
+    if (tuning().lean && !overlap) {
+      switch (tuning().curv_lb) {
+        case 1: launch_curv_point<T, 128, 3>(d, b, a); break;
+        case 2: launch_curv_point<T, 256, 1>(d, b, a); break;
+        default: launch_curv_point<T, 256, 2>(d, b, a); break;
+      }
+    } else {
+      switch (d->response) {
+        case 0: k_curv_update<T, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
+        case 1: k_curv_update<T, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
+        case 2: k_curv_update<T, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
+        default: k_curv_update<T, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
+      }
     }
     d->launches++;
     return;

@@ -99,6 +99,7 @@ struct Blk {
   T *eta, *deta;
   const T *qs, *qp;
   T tau[8], w[8], ss[8], ps[8];
+  T itau[8];            // 1/tau (the lean curvilinear update multiplies instead of dividing)
   int coarse;
   // physical boundaries
   int bc[6];
@@ -1001,6 +1002,337 @@ __global__ void __launch_bounds__(256, 2) k_curv_update(Blk<T> b, StageArgs a) {
   const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
   if (x > b.nx || y > b.ny || z > b.nz) return;
   point_update<T, MESH_CURV, RESP, false, true>(b, a, x, y, z);
+}
+
+// ---------------------------------------------------------------------------
+// Lean curvilinear point update (the second pass after k_curv_grad): the
+// near-boundary point update of src/RHS_Interior.f90:136-281 for every point
+// -- rates from the derivative terms, memory variables
+// (src/RHS_Interior.f90:2599-2908, :3361-3477), PML with the anelastic strain
+// correction (:1846-2265, :2351-2451), sources, face and interface SATs and
+// the RK update -- written for memory-level parallelism:
+//   * the six PML slabs are visited with compile-time face indices, so the
+//     slab boxes, damping and Q / DQ stay in registers; Q and DQ are read
+//     once and written once per stage (scale, source, integrate);
+//   * memory variables are streamed through restrict pointers so the loads
+//     of the next component can be issued before the stores of this one;
+//   * 1/tau is applied as a multiplication (one rounding instead of a
+//     division; well inside the parity tolerance).
+// ---------------------------------------------------------------------------
+template <typename T, int F>
+__device__ __forceinline__ bool slab_has(const Blk<T> &b, int x, int y, int z) {
+  if (!b.pml_on[F]) return false;
+  const int *B = b.pb[F];
+  return x >= B[0] && x <= B[1] && y >= B[2] && y <= B[3] && z >= B[4] && z <= B[5];
+}
+
+template <typename T, int F>
+__device__ __forceinline__ long long slab_index(const Blk<T> &b, int x, int y, int z) {
+  const int *B = b.pb[F];
+  return (long long)(x - B[0]) + (long long)(B[1] - B[0] + 1) * ((long long)(y - B[2]) + (long long)(B[3] - B[2] + 1) * (long long)(z - B[4]));
+}
+
+template <typename T, int F>
+__device__ __forceinline__ T slab_damping(const Blk<T> &b, int x, int y, int z) {
+  constexpr int axis = F >> 1;
+  const int i = axis == 0 ? x : axis == 1 ? y : z;
+  const int n = axis == 0 ? b.nx : axis == 1 ? b.ny : b.nz;
+  const T v = (F == 4) ? (T)(i - b.npml) : ((F & 1) ? (T)(i - (n - b.npml)) : (T)(i - (1 + b.npml)));
+  return b.d0 * fabs(v / (T)b.npml);
+}
+
+// One PML slab per axis: the point lies in at most one of the axis's two
+// slabs (the host sends blocks whose two slabs on an axis overlap to the
+// generic update).
+template <typename T>
+struct AxisSlab {
+  bool in;
+  T d;
+  T *Q, *DQ;
+  long long PV;
+};
+
+template <typename T, int AX>
+__device__ __forceinline__ void axis_slab(const Blk<T> &b, int x, int y, int z, AxisSlab<T> &s) {
+  constexpr int FL = 2 * AX, FH = 2 * AX + 1;
+  const bool hi = slab_has<T, FH>(b, x, y, z);
+  const bool lo = !hi && slab_has<T, FL>(b, x, y, z);
+  s.in = hi || lo;
+  if (hi) {
+    const long long q = slab_index<T, FH>(b, x, y, z);
+    s.d = slab_damping<T, FH>(b, x, y, z);
+    s.Q = b.Q[FH] + q;
+    s.DQ = b.DQ[FH] + q;
+    s.PV = b.pvol[FH];
+  } else if (lo) {
+    const long long q = slab_index<T, FL>(b, x, y, z);
+    s.d = slab_damping<T, FL>(b, x, y, z);
+    s.Q = b.Q[FL] + q;
+    s.DQ = b.DQ[FL] + q;
+    s.PV = b.pvol[FL];
+  }
+}
+
+// one slab of one point: scale DQ (F_SCALE), subtract the PML damping terms
+// from the rates and add the auxiliary-field sources to DQ (rhs;
+// src/RHS_Interior.f90:1913-2265, J form; the source terms are re-read from
+// the derivative scratch Gp), store DQ and integrate Q (F_UPDATE)
+template <typename T, int AX>
+__device__ __forceinline__ void slab_pass(const StageArgs &a, const AxisSlab<T> &s, bool rhs, bool integrate,
+                                          const T *Gp, long long V, T rhoJ_inv, T lambda2mu, T lam, T mu, T J,
+                                          T df[9]) {
+  if (!s.in) return;
+  T Q[9], DQ[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    Q[c] = s.Q[c * s.PV];
+    const T v = s.DQ[c * s.PV];
+    DQ[c] = (a.flags & F_SCALE) ? (T)a.A * v : v;
+  }
+  if (rhs) {
+    const T d = s.d;
+    df[0] = df[0] - d * J * Q[0] * rhoJ_inv;
+    df[1] = df[1] - d * J * Q[1] * rhoJ_inv;
+    df[2] = df[2] - d * J * Q[2] * rhoJ_inv;
+    df[3] = df[3] - d * (lambda2mu * Q[3] + lam * Q[4] + lam * Q[5]);
+    df[4] = df[4] - d * (lam * Q[3] + lambda2mu * Q[4] + lam * Q[5]);
+    df[5] = df[5] - d * (lam * Q[3] + lam * Q[4] + lambda2mu * Q[5]);
+    df[6] = df[6] - mu * d * Q[6];
+    df[7] = df[7] - mu * d * Q[7];
+    df[8] = df[8] - mu * d * Q[8];
+    // G slots: 0-8 velocity gradients (Ux, Uy, Uz 1:3), 9-17 Ux4 Ux7 Ux8 Uy7 Uy5 Uy9 Uz8 Uz9 Uz6
+    T src[9];
+    if (AX == 2) {
+      src[0] = Gp[15 * V] / J; src[1] = Gp[16 * V] / J; src[2] = Gp[17 * V] / J; src[3] = 0; src[4] = 0;
+      src[5] = Gp[8 * V]; src[6] = 0; src[7] = Gp[6 * V]; src[8] = Gp[7 * V];
+    } else if (AX == 1) {
+      src[0] = Gp[12 * V] / J; src[1] = Gp[13 * V] / J; src[2] = Gp[14 * V] / J; src[3] = 0; src[4] = Gp[4 * V];
+      src[5] = 0; src[6] = Gp[3 * V]; src[7] = 0; src[8] = Gp[5 * V];
+    } else {
+      src[0] = Gp[9 * V] / J; src[1] = Gp[10 * V] / J; src[2] = Gp[11 * V] / J; src[3] = Gp[0 * V]; src[4] = 0;
+      src[5] = 0; src[6] = Gp[1 * V]; src[7] = Gp[2 * V]; src[8] = 0;
+    }
+    const T cfs = (T)1;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) DQ[c] = DQ[c] + src[c] - (d + cfs) * Q[c];
+  }
+  const T Bdt = (T)a.Bdt;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    s.DQ[c * s.PV] = DQ[c];
+    if (integrate) s.Q[c * s.PV] = Q[c] + Bdt * DQ[c];
+  }
+}
+
+// Q <- Q + B dt DQ for a slab whose DQ the face SAT changed after slab_pass
+template <typename T>
+__device__ __forceinline__ void slab_integrate(const StageArgs &a, const AxisSlab<T> &s) {
+  if (!s.in) return;
+  const T Bdt = (T)a.Bdt;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) s.Q[c * s.PV] = s.Q[c * s.PV] + Bdt * s.DQ[c * s.PV];
+}
+
+// memory variables of one point: eta sums subtracted from s[3:9] (when
+// do_rhs), rates scaled / accumulated, eta integrated (F_UPDATE)
+template <typename T, int RESP>
+__device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p, T lam,
+                                               T mu, const T e[6], T tr, T s[9], bool do_rhs) {
+  constexpr int N = RESP == RESP_Q4 ? 4 : 8;
+  const long long V = b.vol;
+  T qs = 0, qp = 0;
+  if (RESP != RESP_FQ8) { qs = ld(b.qs + p); qp = ld(b.qp + p); }
+  const int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
+  T *__restrict__ ep = b.eta + p;
+  T *__restrict__ dp = b.deta + p;
+  const T A = (T)a.A, Bdt = (T)a.Bdt;
+  const T two_mu = (T)2 * mu, l2m = lam + (T)2 * mu;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    T ev[N], dv[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      ev[i] = ep[(long long)(c * N + i) * V];
+      dv[i] = dp[(long long)(c * N + i) * V];
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      if (a.flags & F_SCALE) dv[i] = A * dv[i];
+    if (do_rhs) {
+      T sum = ev[0];
+#pragma unroll
+      for (int i = 1; i < N; ++i) sum = sum + ev[i];
+      s[3 + c] = s[3 + c] - sum;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        if (RESP == RESP_FQ8) {
+          if (b.coarse && (i + 1) != active) continue;
+          const T ss = b.ss[i], ps = b.ps[i];
+          if (c < 3)
+            dv[i] = dv[i] + (((ss * two_mu) * e[c] + (l2m * ps - two_mu * ss) * tr) - ev[i]) * b.itau[i];
+          else
+            dv[i] = dv[i] + (ss * mu * e[c] - ev[i]) * b.itau[i];
+        } else {
+          const T w = b.w[i];
+          if (c < 3)
+            dv[i] = dv[i] + (((w * two_mu * qs) * e[c] + (w * (l2m * qp - two_mu * qs)) * tr) - ev[i]) * b.itau[i];
+          else
+            dv[i] = dv[i] + (w * mu * qs * e[c] - ev[i]) * b.itau[i];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      dp[(long long)(c * N + i) * V] = dv[i];
+      if (a.flags & F_UPDATE) ep[(long long)(c * N + i) * V] = ev[i] + Bdt * dv[i];
+    }
+  }
+}
+
+template <typename T, int RESP, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+  if (x > b.nx || y > b.ny || z > b.nz) return;
+  const long long p = pidx(b, x, y, z);
+  const long long V = b.vol;
+  const T *__restrict__ F = a.cur ? b.F1 : b.F0;
+  T *__restrict__ Fn = a.cur ? b.F0 : b.F1;
+  T *__restrict__ DFp = b.DF + p;
+  T df[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const T v = DFp[c * V];
+    df[c] = (a.flags & F_SCALE) ? (T)a.A * v : v;
+  }
+  AxisSlab<T> sx, sy, sz;
+  sx.in = sy.in = sz.in = false;
+  if (b.npml > 0) {
+    axis_slab<T, 0>(b, x, y, z, sx);
+    axis_slab<T, 1>(b, x, y, z, sy);
+    axis_slab<T, 2>(b, x, y, z, sz);
+  }
+  const bool in_pml = sx.in || sy.in || sz.in;
+  // a face point's SAT also changes DQ of its slab (add_face_sats), so its
+  // slabs are integrated after the SATs
+  const bool face_pt = x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz;
+  const bool defer = in_pml && face_pt && (a.flags & F_SAT);
+  const bool integrate = (a.flags & F_UPDATE) && !defer;
+  const T lam = b.M[p], mu = b.M[V + p];
+  if (a.flags & F_RHS) {
+    const T rho = b.M[2 * V + p];
+    const T *__restrict__ Gp = b.G + p;
+    T Ux[9], Uy[9], Uz[9];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      Ux[f] = Gp[(0 + f) * V];
+      Uy[f] = Gp[(3 + f) * V];
+      Uz[f] = Gp[(6 + f) * V];
+    }
+    Ux[3] = Gp[9 * V];  Ux[6] = Gp[10 * V]; Ux[7] = Gp[11 * V];
+    Uy[6] = Gp[12 * V]; Uy[4] = Gp[13 * V]; Uy[8] = Gp[14 * V];
+    Uz[7] = Gp[15 * V]; Uz[8] = Gp[16 * V]; Uz[5] = Gp[17 * V];
+    Ux[4] = Ux[5] = Ux[8] = (T)0;
+    Uy[3] = Uy[5] = Uy[7] = (T)0;
+    Uz[3] = Uz[4] = Uz[6] = (T)0;
+    const T J = ld(b.J + p);
+    const T rhoJ_inv = (T)1 / (rho * J);
+    const T lambda2mu = lam + (T)2 * mu;
+    T DU[9];
+    DU[0] = (Ux[3] + Uy[6] + Uz[7]) * rhoJ_inv;
+    DU[1] = (Ux[6] + Uy[4] + Uz[8]) * rhoJ_inv;
+    DU[2] = (Ux[7] + Uy[8] + Uz[5]) * rhoJ_inv;
+    DU[3] = lambda2mu * Ux[0] + lam * (Uy[1] + Uz[2]);
+    DU[4] = lambda2mu * Uy[1] + lam * (Ux[0] + Uz[2]);
+    DU[5] = lambda2mu * Uz[2] + lam * (Ux[0] + Uy[1]);
+    DU[6] = mu * (Uy[0] + Ux[1]);
+    DU[7] = mu * (Uz[0] + Ux[2]);
+    DU[8] = mu * (Uz[1] + Uy[2]);
+    if (RESP != RESP_EL) {
+      T e[6] = {Ux[0], Uy[1], Uz[2], Uy[0] + Ux[1], Uz[0] + Ux[2], Uz[1] + Uy[2]};
+      T tr;
+      if (in_pml) {
+        // PML strain correction (src/RHS_Interior.f90:2351-2451)
+        const T dx = sx.in ? sx.d : (T)0, dy = sy.in ? sy.d : (T)0, dz = sz.in ? sz.d : (T)0;
+        const T qx3 = sx.in ? sx.Q[3 * sx.PV] : (T)0, qx6 = sx.in ? sx.Q[6 * sx.PV] : (T)0;
+        const T qx7 = sx.in ? sx.Q[7 * sx.PV] : (T)0;
+        const T qy4 = sy.in ? sy.Q[4 * sy.PV] : (T)0, qy6 = sy.in ? sy.Q[6 * sy.PV] : (T)0;
+        const T qy8 = sy.in ? sy.Q[8 * sy.PV] : (T)0;
+        const T qz5 = sz.in ? sz.Q[5 * sz.PV] : (T)0, qz7 = sz.in ? sz.Q[7 * sz.PV] : (T)0;
+        const T qz8 = sz.in ? sz.Q[8 * sz.PV] : (T)0;
+        e[0] = e[0] - dx * qx3;
+        e[1] = e[1] - dy * qy4;
+        e[2] = e[2] - dz * qz5;
+        e[3] = e[3] - dx * qx6 - dy * qy6;
+        e[4] = e[4] - dx * qx7 - dz * qz7;
+        e[5] = e[5] - dy * qy8 - dz * qz8;
+        tr = e[0] + e[1] + e[2];
+      } else {
+        tr = Ux[0] + Uy[1] + Uz[2];
+      }
+      anelastic_lean<T, RESP>(b, a, x, y, z, p, lam, mu, e, tr, DU, true);
+    }
+#pragma unroll
+    for (int c = 0; c < 9; ++c) df[c] = df[c] + DU[c];
+    // PML damping and auxiliary fields, reference slab order z, y, x (one
+    // slab per axis), subtracted from the rates after the RHS
+    slab_pass<T, 2>(a, sz, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+    slab_pass<T, 1>(a, sy, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+    slab_pass<T, 0>(a, sx, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+  } else {
+    if (RESP != RESP_EL && (a.flags & (F_SCALE | F_UPDATE))) {
+      T e[6] = {0, 0, 0, 0, 0, 0};
+      anelastic_lean<T, RESP>(b, a, x, y, z, p, lam, mu, e, (T)0, df, false);
+    }
+    if (in_pml && (a.flags & (F_SCALE | F_UPDATE))) {
+      slab_pass<T, 2>(a, sz, false, integrate, b.G + p, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+      slab_pass<T, 1>(a, sy, false, integrate, b.G + p, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+      slab_pass<T, 0>(a, sx, false, integrate, b.G + p, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    }
+  }
+  if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
+      z >= b.sbox[4] && z <= b.sbox[5]) {
+    const double t0 = a.time ? a.time->t : 0.0;
+    const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
+    add_sources<T, MESH_CURV>(b, tst, x, y, z, p, df);
+  }
+  if ((a.flags & F_SAT) && face_pt) add_face_sats<T, MESH_CURV, false>(b, F, x, y, z, p, df, in_pml);
+  if (defer && (a.flags & F_UPDATE)) {
+    slab_integrate<T>(a, sz);
+    slab_integrate<T>(a, sy);
+    slab_integrate<T>(a, sx);
+  }
+  if (a.flags & F_ISAT) {
+    // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
+    const int side = x == 1 ? 0 : (x == b.nx ? 1 : -1);
+    if (side >= 0 && b.isat[side]) {
+      const T pen = b.tau0 / b.hq;
+      const long long fp = (long long)(y - 1) + (long long)b.ny * (z - 1);
+      const long long fn = (long long)b.ny * b.nz;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) df[c] = df[c] - pen * b.isat[side][c * fn + fp];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) DFp[c * V] = df[c];
+  if (a.flags & F_UPDATE) {
+    const T Bdt = (T)a.Bdt;
+    if (b.FC) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        const T f0 = F[c * V + p];
+        const T comp = b.FC[c * V + p];
+        const T yv = Bdt * df[c] - comp;
+        const T tv = f0 + yv;
+        b.FC[c * V + p] = (tv - f0) - yv;
+        Fn[c * V + p] = tv;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Fn[c * V + p] = F[c * V + p] + Bdt * df[c];
+    }
+  }
 }
 
 // Number of near-boundary (shell) points: everything outside the strict
