@@ -442,6 +442,7 @@ int setup_block(wql3d_domain *d, int bi) {
   CK(M.get(&b.M, 3 * vol));
   if (d->fp32) CK(M.get(&b.FC, 9 * vol));
   if (bd.mesh == WQL3D_MESH_CURVILINEAR) CK(M.get(&b.G, 18 * vol, false));
+  if (bd.mesh == WQL3D_MESH_CURVILINEAR && d->response != 0) CK(M.get(&b.S6, 6 * vol, false));
   {
     // rates start at the reference's 1e40 sentinel (src/fields.f90:39) in FP64;
     // the first stage scales them by A(1) = 0.  FP32 cannot hold 1e40: zero.
@@ -701,8 +702,8 @@ struct Tuning {
   int split = 1;     // interior: two warp groups (velocity / stress rates) with register z-queues
   int lean = 1;      // curvilinear update: k_curv_point (0: generic point update k_curv_update)
   int curv_lb = 0;   // k_curv_point threads x min blocks: 0 = 256x2, 1 = 128x3, 2 = 256x1
-  int curv_bx = 32;  // k_curv_point tile width along x (32, 64)
   int grad_bx = 32;  // k_curv_grad tile width along x (32, 64)
+  int an_minb = 3;   // k_curv_anelastic: resident 128-thread blocks per SM (3, 4 or 6)
 };
 
 Tuning tuning() {
@@ -711,7 +712,7 @@ Tuning tuning() {
     if (const char *e = getenv("WQL3D_TY")) r.ty = atoi(e) == 8 ? 8 : 4;
     if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = std::max(1, atoi(e));
     if (const char *e = getenv("WQL3D_CURV_LB")) r.curv_lb = std::min(2, std::max(0, atoi(e)));
-    if (const char *e = getenv("WQL3D_CURV_BX")) r.curv_bx = atoi(e) == 64 ? 64 : 32;
+    if (const char *e = getenv("WQL3D_AN_MINB")) r.an_minb = atoi(e);
     if (const char *e = getenv("WQL3D_GRAD_BX")) r.grad_bx = atoi(e) == 64 ? 64 : 32;
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
@@ -765,10 +766,19 @@ void launch_shell(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
   d->launches++;
 }
 
+template <typename T, int MINB>
+void launch_curv_anelastic(wql3d_domain *d, Blk<T> &b, const StageArgs &a, unsigned gr, unsigned th) {
+  switch (d->response) {
+    case 1: k_curv_anelastic<T, RESP_Q4, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+    case 2: k_curv_anelastic<T, RESP_Q8, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+    default: k_curv_anelastic<T, RESP_FQ8, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
+  }
+}
+
 template <typename T, int MAXT, int MINB>
 void launch_curv_point(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
-  const int bx = tuning().curv_bx, by = MAXT / bx / 2;
-  dim3 th(bx, by, 2), gr((b.nx + bx - 1) / bx, (b.ny + by - 1) / by, (b.nz + 1) / 2);
+  const long long npts = (long long)b.nx * b.ny * b.nz;
+  const unsigned th = MAXT, gr = (unsigned)((npts + MAXT - 1) / MAXT);
   switch (d->response) {
     case 0: k_curv_point<T, RESP_EL, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
     case 1: k_curv_point<T, RESP_Q4, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
@@ -807,6 +817,17 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
     for (int ax = 0; ax < 3; ++ax)
       if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) overlap = true;
     if (tuning().lean && !overlap) {
+      if (d->response != 0 && (a.flags & (F_RHS | F_SCALE | F_UPDATE))) {
+        // memory variables first: k_curv_point subtracts their sums
+        const long long npts = (long long)b.nx * b.ny * b.nz;
+        const unsigned ath = 128, agr = (unsigned)((npts + 127) / 128);
+        switch (tuning().an_minb) {
+          case 6: launch_curv_anelastic<T, 6>(d, b, a, agr, ath); break;
+          case 3: launch_curv_anelastic<T, 3>(d, b, a, agr, ath); break;
+          default: launch_curv_anelastic<T, 4>(d, b, a, agr, ath); break;
+        }
+        d->launches++;
+      }
       switch (tuning().curv_lb) {
         case 1: launch_curv_point<T, 128, 3>(d, b, a); break;
         case 2: launch_curv_point<T, 256, 1>(d, b, a); break;

@@ -73,6 +73,7 @@ struct Blk {
   T *DF;                // rates (9 components)
   T *FC;                // FP32 path: Kahan compensation for F (9 components)
   T *G;                 // curvilinear: 18 derivative terms per point from k_curv_grad (see there)
+  T *S6;                // curvilinear anelastic: per stress component the sum of the memory variables
   T *M;                 // lambda, mu, rho
   // Cartesian: per-axis diagonal metric 1/X_a(i) (index 1..n)
   const T *mq, *mr, *ms;
@@ -1043,54 +1044,43 @@ __device__ __forceinline__ T slab_damping(const Blk<T> &b, int x, int y, int z) 
 
 // One PML slab per axis: the point lies in at most one of the axis's two
 // slabs (the host sends blocks whose two slabs on an axis overlap to the
-// generic update).
-template <typename T>
+// generic update).  Only the membership is kept; the slab index, damping and
+// array pointers are recomputed where they are used.
 struct AxisSlab {
-  bool in;
-  T d;
-  T *Q, *DQ;
-  long long PV;
+  bool lo, hi;
+  __device__ __forceinline__ bool in() const { return lo || hi; }
 };
 
 template <typename T, int AX>
-__device__ __forceinline__ void axis_slab(const Blk<T> &b, int x, int y, int z, AxisSlab<T> &s) {
-  constexpr int FL = 2 * AX, FH = 2 * AX + 1;
-  const bool hi = slab_has<T, FH>(b, x, y, z);
-  const bool lo = !hi && slab_has<T, FL>(b, x, y, z);
-  s.in = hi || lo;
-  if (hi) {
-    const long long q = slab_index<T, FH>(b, x, y, z);
-    s.d = slab_damping<T, FH>(b, x, y, z);
-    s.Q = b.Q[FH] + q;
-    s.DQ = b.DQ[FH] + q;
-    s.PV = b.pvol[FH];
-  } else if (lo) {
-    const long long q = slab_index<T, FL>(b, x, y, z);
-    s.d = slab_damping<T, FL>(b, x, y, z);
-    s.Q = b.Q[FL] + q;
-    s.DQ = b.DQ[FL] + q;
-    s.PV = b.pvol[FL];
-  }
+__device__ __forceinline__ AxisSlab axis_slab(const Blk<T> &b, int x, int y, int z) {
+  AxisSlab s;
+  s.hi = slab_has<T, 2 * AX + 1>(b, x, y, z);
+  s.lo = !s.hi && slab_has<T, 2 * AX>(b, x, y, z);
+  return s;
 }
 
-// one slab of one point: scale DQ (F_SCALE), subtract the PML damping terms
+// one slab F of one point: scale DQ (F_SCALE), subtract the PML damping terms
 // from the rates and add the auxiliary-field sources to DQ (rhs;
 // src/RHS_Interior.f90:1913-2265, J form; the source terms are re-read from
-// the derivative scratch Gp), store DQ and integrate Q (F_UPDATE)
-template <typename T, int AX>
-__device__ __forceinline__ void slab_pass(const StageArgs &a, const AxisSlab<T> &s, bool rhs, bool integrate,
-                                          const T *Gp, long long V, T rhoJ_inv, T lambda2mu, T lam, T mu, T J,
-                                          T df[9]) {
-  if (!s.in) return;
+// the derivative scratch Gp), store DQ and integrate Q (integrate)
+template <typename T, int F>
+__device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int x, int y, int z, bool rhs,
+                                        bool integrate, const T *Gp, long long V, T rhoJ_inv, T lambda2mu, T lam,
+                                        T mu, T J, T df[9]) {
+  constexpr int AX = F >> 1;
+  const long long q = slab_index<T, F>(b, x, y, z);
+  const long long PV = b.pvol[F];
+  T *Qp = b.Q[F] + q;
+  T *DQp = b.DQ[F] + q;
   T Q[9], DQ[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
-    Q[c] = s.Q[c * s.PV];
-    const T v = s.DQ[c * s.PV];
+    Q[c] = Qp[c * PV];
+    const T v = DQp[c * PV];
     DQ[c] = (a.flags & F_SCALE) ? (T)a.A * v : v;
   }
   if (rhs) {
-    const T d = s.d;
+    const T d = slab_damping<T, F>(b, x, y, z);
     df[0] = df[0] - d * J * Q[0] * rhoJ_inv;
     df[1] = df[1] - d * J * Q[1] * rhoJ_inv;
     df[2] = df[2] - d * J * Q[2] * rhoJ_inv;
@@ -1119,22 +1109,58 @@ __device__ __forceinline__ void slab_pass(const StageArgs &a, const AxisSlab<T> 
   const T Bdt = (T)a.Bdt;
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
-    s.DQ[c * s.PV] = DQ[c];
-    if (integrate) s.Q[c * s.PV] = Q[c] + Bdt * DQ[c];
+    DQp[c * PV] = DQ[c];
+    if (integrate) Qp[c * PV] = Q[c] + Bdt * DQ[c];
   }
 }
 
+template <typename T, int AX>
+__device__ __forceinline__ void slab_pass(const Blk<T> &b, const StageArgs &a, int x, int y, int z, AxisSlab s,
+                                          bool rhs, bool integrate, const T *Gp, long long V, T rhoJ_inv,
+                                          T lambda2mu, T lam, T mu, T J, T df[9]) {
+  if (s.hi) slab_do<T, 2 * AX + 1>(b, a, x, y, z, rhs, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+  else if (s.lo) slab_do<T, 2 * AX>(b, a, x, y, z, rhs, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+}
+
 // Q <- Q + B dt DQ for a slab whose DQ the face SAT changed after slab_pass
-template <typename T>
-__device__ __forceinline__ void slab_integrate(const StageArgs &a, const AxisSlab<T> &s) {
-  if (!s.in) return;
+template <typename T, int F>
+__device__ __forceinline__ void slab_int(const Blk<T> &b, const StageArgs &a, int x, int y, int z) {
+  const long long q = slab_index<T, F>(b, x, y, z);
+  const long long PV = b.pvol[F];
+  T *Qp = b.Q[F] + q;
+  const T *DQp = b.DQ[F] + q;
   const T Bdt = (T)a.Bdt;
 #pragma unroll
-  for (int c = 0; c < 9; ++c) s.Q[c * s.PV] = s.Q[c * s.PV] + Bdt * s.DQ[c * s.PV];
+  for (int c = 0; c < 9; ++c) Qp[c * PV] = Qp[c * PV] + Bdt * DQp[c * PV];
+}
+
+template <typename T, int AX>
+__device__ __forceinline__ void slab_integrate(const Blk<T> &b, const StageArgs &a, int x, int y, int z, AxisSlab s) {
+  if (s.hi) slab_int<T, 2 * AX + 1>(b, a, x, y, z);
+  else if (s.lo) slab_int<T, 2 * AX>(b, a, x, y, z);
+}
+
+// PML strain correction term d * Q[c] of the slab of one axis (0 outside)
+template <typename T, int AX>
+__device__ __forceinline__ void slab_strain(const Blk<T> &b, int x, int y, int z, AxisSlab s, int c0, int c1, int c2,
+                                            T &d, T &q0, T &q1, T &q2) {
+  d = 0; q0 = 0; q1 = 0; q2 = 0;
+  if (!s.in()) return;
+  constexpr int FL = 2 * AX, FH = 2 * AX + 1;
+  const long long q = s.hi ? slab_index<T, FH>(b, x, y, z) : slab_index<T, FL>(b, x, y, z);
+  const long long PV = s.hi ? b.pvol[FH] : b.pvol[FL];
+  const T *Qp = (s.hi ? b.Q[FH] : b.Q[FL]) + q;
+  d = s.hi ? slab_damping<T, FH>(b, x, y, z) : slab_damping<T, FL>(b, x, y, z);
+  q0 = Qp[c0 * PV]; q1 = Qp[c1 * PV]; q2 = Qp[c2 * PV];
 }
 
 // memory variables of one point: eta sums subtracted from s[3:9] (when
-// do_rhs), rates scaled / accumulated, eta integrated (F_UPDATE)
+// do_rhs), rates scaled / accumulated, eta integrated (F_UPDATE).  The rate
+// of src/RHS_Interior.f90:2599-2908 (Q4 / Q8) is regrouped per component as
+// w_l * (2 mu Qs^-1 e) + w_l * (((lambda + 2 mu) Qp^-1 - 2 mu Qs^-1) tr) and
+// that of :3361-3477 (fQ8) as s_l (2 mu e) + (p_l (lambda + 2 mu) tr -
+// s_l 2 mu tr), so only per-point scalars and the per-mechanism constants
+// are live: the same products in another association (rounding level).
 template <typename T, int RESP>
 __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p, T lam,
                                                T mu, const T e[6], T tr, T s[9], bool do_rhs) {
@@ -1143,10 +1169,14 @@ __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs 
   T qs = 0, qp = 0;
   if (RESP != RESP_FQ8) { qs = ld(b.qs + p); qp = ld(b.qp + p); }
   const int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
-  T *__restrict__ ep = b.eta + p;
-  T *__restrict__ dp = b.deta + p;
+  T *ep = b.eta + p;
+  T *dp = b.deta + p;
   const T A = (T)a.A, Bdt = (T)a.Bdt;
   const T two_mu = (T)2 * mu, l2m = lam + (T)2 * mu;
+  // per-point factors of the rates
+  const T fn = RESP == RESP_FQ8 ? two_mu : two_mu * qs;               // normal strain factor
+  const T ft = RESP == RESP_FQ8 ? (T)0 : (l2m * qp - two_mu * qs);    // trace factor (Q4/Q8)
+  const T fs = RESP == RESP_FQ8 ? mu : mu * qs;                        // shear strain factor
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
     T ev[N], dv[N];
@@ -1163,21 +1193,19 @@ __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs 
 #pragma unroll
       for (int i = 1; i < N; ++i) sum = sum + ev[i];
       s[3 + c] = s[3 + c] - sum;
+      const T ge = (c < 3 ? fn : fs) * e[c];
+      const T gt = ft * tr, l2t = l2m * tr, m2t = two_mu * tr;
 #pragma unroll
       for (int i = 0; i < N; ++i) {
         if (RESP == RESP_FQ8) {
           if (b.coarse && (i + 1) != active) continue;
           const T ss = b.ss[i], ps = b.ps[i];
-          if (c < 3)
-            dv[i] = dv[i] + (((ss * two_mu) * e[c] + (l2m * ps - two_mu * ss) * tr) - ev[i]) * b.itau[i];
-          else
-            dv[i] = dv[i] + (ss * mu * e[c] - ev[i]) * b.itau[i];
+          if (c < 3) dv[i] = dv[i] + ((ss * ge + (ps * l2t - ss * m2t)) - ev[i]) * b.itau[i];
+          else dv[i] = dv[i] + (ss * ge - ev[i]) * b.itau[i];
         } else {
           const T w = b.w[i];
-          if (c < 3)
-            dv[i] = dv[i] + (((w * two_mu * qs) * e[c] + (w * (l2m * qp - two_mu * qs)) * tr) - ev[i]) * b.itau[i];
-          else
-            dv[i] = dv[i] + (w * mu * qs * e[c] - ev[i]) * b.itau[i];
+          if (c < 3) dv[i] = dv[i] + ((w * ge + w * gt) - ev[i]) * b.itau[i];
+          else dv[i] = dv[i] + (w * ge - ev[i]) * b.itau[i];
         }
       }
     }
@@ -1189,12 +1217,77 @@ __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs 
   }
 }
 
+// Curvilinear memory variables, a streaming pass between k_curv_grad and
+// k_curv_point: strain rates from the velocity gradients of G (PML-corrected
+// in slabs), memory-variable rates scaled / accumulated, the per-component
+// sums of the memory variables (before this stage's update) left in S6 for
+// k_curv_point to subtract from the stress rates, and (F_UPDATE) eta
+// integrated.
+// point of a flattened (x fastest) 1-D launch over the block; false past the end
+template <typename T>
+__device__ __forceinline__ bool flat_point(const Blk<T> &b, int &x, int &y, int &z) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= b.nx * b.ny * b.nz) return false;
+  const int r = j / b.nx;
+  x = j - r * b.nx + 1;
+  z = r / b.ny;
+  y = r - z * b.ny + 1;
+  z = z + 1;
+  return true;
+}
+
+template <typename T, int RESP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_curv_anelastic(Blk<T> b, StageArgs a) {
+  int x, y, z;
+  if (!flat_point(b, x, y, z)) return;
+  const long long p = pidx(b, x, y, z);
+  const long long V = b.vol;
+  const bool rhs = (a.flags & F_RHS) != 0;
+  const T lam = b.M[p], mu = b.M[V + p];
+  T e[6] = {0, 0, 0, 0, 0, 0}, tr = 0;
+  if (rhs) {
+    const T *Gp = b.G + p;
+    const T Ux0 = Gp[0], Ux1 = Gp[V], Ux2 = Gp[2 * V];
+    const T Uy0 = Gp[3 * V], Uy1 = Gp[4 * V], Uy2 = Gp[5 * V];
+    const T Uz0 = Gp[6 * V], Uz1 = Gp[7 * V], Uz2 = Gp[8 * V];
+    e[0] = Ux0; e[1] = Uy1; e[2] = Uz2;
+    e[3] = Uy0 + Ux1; e[4] = Uz0 + Ux2; e[5] = Uz1 + Uy2;
+    AxisSlab sx = {false, false}, sy = {false, false}, sz = {false, false};
+    if (b.npml > 0) {
+      sx = axis_slab<T, 0>(b, x, y, z);
+      sy = axis_slab<T, 1>(b, x, y, z);
+      sz = axis_slab<T, 2>(b, x, y, z);
+    }
+    if (sx.in() || sy.in() || sz.in()) {
+      // src/RHS_Interior.f90:2351-2451
+      T dx, qx3, qx6, qx7, dy, qy4, qy6, qy8, dz, qz5, qz7, qz8;
+      slab_strain<T, 0>(b, x, y, z, sx, 3, 6, 7, dx, qx3, qx6, qx7);
+      slab_strain<T, 1>(b, x, y, z, sy, 4, 6, 8, dy, qy4, qy6, qy8);
+      slab_strain<T, 2>(b, x, y, z, sz, 5, 7, 8, dz, qz5, qz7, qz8);
+      e[0] = e[0] - dx * qx3;
+      e[1] = e[1] - dy * qy4;
+      e[2] = e[2] - dz * qz5;
+      e[3] = e[3] - dx * qx6 - dy * qy6;
+      e[4] = e[4] - dx * qx7 - dz * qz7;
+      e[5] = e[5] - dy * qy8 - dz * qz8;
+      tr = e[0] + e[1] + e[2];
+    } else {
+      tr = Ux0 + Uy1 + Uz2;
+    }
+  }
+  T s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  anelastic_lean<T, RESP>(b, a, x, y, z, p, lam, mu, e, tr, s, rhs);
+  if (rhs) {
+    // s[3 + c] = -sum_l eta_c,l
+#pragma unroll
+    for (int c = 0; c < 6; ++c) b.S6[c * V + p] = s[3 + c];
+  }
+}
+
 template <typename T, int RESP, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (x > b.nx || y > b.ny || z > b.nz) return;
+  int x, y, z;
+  if (!flat_point(b, x, y, z)) return;
   const long long p = pidx(b, x, y, z);
   const long long V = b.vol;
   const T *__restrict__ F = a.cur ? b.F1 : b.F0;
@@ -1206,90 +1299,54 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     const T v = DFp[c * V];
     df[c] = (a.flags & F_SCALE) ? (T)a.A * v : v;
   }
-  AxisSlab<T> sx, sy, sz;
-  sx.in = sy.in = sz.in = false;
+  AxisSlab sx = {false, false}, sy = {false, false}, sz = {false, false};
   if (b.npml > 0) {
-    axis_slab<T, 0>(b, x, y, z, sx);
-    axis_slab<T, 1>(b, x, y, z, sy);
-    axis_slab<T, 2>(b, x, y, z, sz);
+    sx = axis_slab<T, 0>(b, x, y, z);
+    sy = axis_slab<T, 1>(b, x, y, z);
+    sz = axis_slab<T, 2>(b, x, y, z);
   }
-  const bool in_pml = sx.in || sy.in || sz.in;
+  const bool in_pml = sx.in() || sy.in() || sz.in();
   // a face point's SAT also changes DQ of its slab (add_face_sats), so its
   // slabs are integrated after the SATs
   const bool face_pt = x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz;
   const bool defer = in_pml && face_pt && (a.flags & F_SAT);
   const bool integrate = (a.flags & F_UPDATE) && !defer;
-  const T lam = b.M[p], mu = b.M[V + p];
+  const T *Gp = b.G + p;
   if (a.flags & F_RHS) {
-    const T rho = b.M[2 * V + p];
-    const T *__restrict__ Gp = b.G + p;
-    T Ux[9], Uy[9], Uz[9];
-#pragma unroll
-    for (int f = 0; f < 3; ++f) {
-      Ux[f] = Gp[(0 + f) * V];
-      Uy[f] = Gp[(3 + f) * V];
-      Uz[f] = Gp[(6 + f) * V];
-    }
-    Ux[3] = Gp[9 * V];  Ux[6] = Gp[10 * V]; Ux[7] = Gp[11 * V];
-    Uy[6] = Gp[12 * V]; Uy[4] = Gp[13 * V]; Uy[8] = Gp[14 * V];
-    Uz[7] = Gp[15 * V]; Uz[8] = Gp[16 * V]; Uz[5] = Gp[17 * V];
-    Ux[4] = Ux[5] = Ux[8] = (T)0;
-    Uy[3] = Uy[5] = Uy[7] = (T)0;
-    Uz[3] = Uz[4] = Uz[6] = (T)0;
+    const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
     const T J = ld(b.J + p);
     const T rhoJ_inv = (T)1 / (rho * J);
     const T lambda2mu = lam + (T)2 * mu;
-    T DU[9];
-    DU[0] = (Ux[3] + Uy[6] + Uz[7]) * rhoJ_inv;
-    DU[1] = (Ux[6] + Uy[4] + Uz[8]) * rhoJ_inv;
-    DU[2] = (Ux[7] + Uy[8] + Uz[5]) * rhoJ_inv;
-    DU[3] = lambda2mu * Ux[0] + lam * (Uy[1] + Uz[2]);
-    DU[4] = lambda2mu * Uy[1] + lam * (Ux[0] + Uz[2]);
-    DU[5] = lambda2mu * Uz[2] + lam * (Ux[0] + Uy[1]);
-    DU[6] = mu * (Uy[0] + Ux[1]);
-    DU[7] = mu * (Uz[0] + Ux[2]);
-    DU[8] = mu * (Uz[1] + Uy[2]);
+    // rates of src/RHS_Interior.f90:238-254 from the derivative terms
+    df[0] = df[0] + (Gp[9 * V] + Gp[12 * V] + Gp[15 * V]) * rhoJ_inv;
+    df[1] = df[1] + (Gp[10 * V] + Gp[13 * V] + Gp[16 * V]) * rhoJ_inv;
+    df[2] = df[2] + (Gp[11 * V] + Gp[14 * V] + Gp[17 * V]) * rhoJ_inv;
+    {
+      const T Ux0 = Gp[0], Ux1 = Gp[V], Ux2 = Gp[2 * V];
+      const T Uy0 = Gp[3 * V], Uy1 = Gp[4 * V], Uy2 = Gp[5 * V];
+      const T Uz0 = Gp[6 * V], Uz1 = Gp[7 * V], Uz2 = Gp[8 * V];
+      df[3] = df[3] + (lambda2mu * Ux0 + lam * (Uy1 + Uz2));
+      df[4] = df[4] + (lambda2mu * Uy1 + lam * (Ux0 + Uz2));
+      df[5] = df[5] + (lambda2mu * Uz2 + lam * (Ux0 + Uy1));
+      df[6] = df[6] + mu * (Uy0 + Ux1);
+      df[7] = df[7] + mu * (Uz0 + Ux2);
+      df[8] = df[8] + mu * (Uz1 + Uy2);
+    }
     if (RESP != RESP_EL) {
-      T e[6] = {Ux[0], Uy[1], Uz[2], Uy[0] + Ux[1], Uz[0] + Ux[2], Uz[1] + Uy[2]};
-      T tr;
-      if (in_pml) {
-        // PML strain correction (src/RHS_Interior.f90:2351-2451)
-        const T dx = sx.in ? sx.d : (T)0, dy = sy.in ? sy.d : (T)0, dz = sz.in ? sz.d : (T)0;
-        const T qx3 = sx.in ? sx.Q[3 * sx.PV] : (T)0, qx6 = sx.in ? sx.Q[6 * sx.PV] : (T)0;
-        const T qx7 = sx.in ? sx.Q[7 * sx.PV] : (T)0;
-        const T qy4 = sy.in ? sy.Q[4 * sy.PV] : (T)0, qy6 = sy.in ? sy.Q[6 * sy.PV] : (T)0;
-        const T qy8 = sy.in ? sy.Q[8 * sy.PV] : (T)0;
-        const T qz5 = sz.in ? sz.Q[5 * sz.PV] : (T)0, qz7 = sz.in ? sz.Q[7 * sz.PV] : (T)0;
-        const T qz8 = sz.in ? sz.Q[8 * sz.PV] : (T)0;
-        e[0] = e[0] - dx * qx3;
-        e[1] = e[1] - dy * qy4;
-        e[2] = e[2] - dz * qz5;
-        e[3] = e[3] - dx * qx6 - dy * qy6;
-        e[4] = e[4] - dx * qx7 - dz * qz7;
-        e[5] = e[5] - dy * qy8 - dz * qz8;
-        tr = e[0] + e[1] + e[2];
-      } else {
-        tr = Ux[0] + Uy[1] + Uz[2];
-      }
-      anelastic_lean<T, RESP>(b, a, x, y, z, p, lam, mu, e, tr, DU, true);
-    }
+      // minus the memory-variable sums left by k_curv_anelastic
 #pragma unroll
-    for (int c = 0; c < 9; ++c) df[c] = df[c] + DU[c];
-    // PML damping and auxiliary fields, reference slab order z, y, x (one
-    // slab per axis), subtracted from the rates after the RHS
-    slab_pass<T, 2>(a, sz, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-    slab_pass<T, 1>(a, sy, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-    slab_pass<T, 0>(a, sx, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-  } else {
-    if (RESP != RESP_EL && (a.flags & (F_SCALE | F_UPDATE))) {
-      T e[6] = {0, 0, 0, 0, 0, 0};
-      anelastic_lean<T, RESP>(b, a, x, y, z, p, lam, mu, e, (T)0, df, false);
+      for (int c = 0; c < 6; ++c) df[3 + c] = df[3 + c] + b.S6[c * V + p];
     }
-    if (in_pml && (a.flags & (F_SCALE | F_UPDATE))) {
-      slab_pass<T, 2>(a, sz, false, integrate, b.G + p, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
-      slab_pass<T, 1>(a, sy, false, integrate, b.G + p, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
-      slab_pass<T, 0>(a, sx, false, integrate, b.G + p, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    // PML damping and auxiliary fields, reference slab order z, y, x
+    if (in_pml) {
+      slab_pass<T, 2>(b, a, x, y, z, sz, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 1>(b, a, x, y, z, sy, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 0>(b, a, x, y, z, sx, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
     }
+  } else if (in_pml && (a.flags & (F_SCALE | F_UPDATE))) {
+    slab_pass<T, 2>(b, a, x, y, z, sz, false, integrate, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 1>(b, a, x, y, z, sy, false, integrate, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 0>(b, a, x, y, z, sx, false, integrate, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
   }
   if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
       z >= b.sbox[4] && z <= b.sbox[5]) {
@@ -1299,9 +1356,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
   }
   if ((a.flags & F_SAT) && face_pt) add_face_sats<T, MESH_CURV, false>(b, F, x, y, z, p, df, in_pml);
   if (defer && (a.flags & F_UPDATE)) {
-    slab_integrate<T>(a, sz);
-    slab_integrate<T>(a, sy);
-    slab_integrate<T>(a, sx);
+    slab_integrate<T, 2>(b, a, x, y, z, sz);
+    slab_integrate<T, 1>(b, a, x, y, z, sy);
+    slab_integrate<T, 0>(b, a, x, y, z, sx);
   }
   if (a.flags & F_ISAT) {
     // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
