@@ -139,6 +139,12 @@ typedef struct wql3d_domain_desc {
   const double *iface_tau0;    /* optional (3, ns, nr): initial tractions n, m, l on the interface */
   const double *iface_fs;      /* optional (ns, nr) static friction map */
   int32_t max_samples;         /* receiver samples kept on the device */
+  /* manufactured solution (src/mms.f90:136-235): when mms != 0 every point's
+     rates get the forcing u*_t - L(u*) and the face SATs the exact boundary
+     data u - u* (src/BoundaryConditions.f90:84-88); such a domain runs the
+     generic per-point kernel */
+  int32_t mms;
+  double mms_nt, mms_nx, mms_ny, mms_nz;
   wql3d_block_desc block[2];
 } wql3d_domain_desc;
 

@@ -31,6 +31,8 @@ class OrcDesc(C.Structure):
         ("nsrc", C.c_int), ("src_order", C.c_int), ("src_alpha", C.c_int),
         ("src_type", C.POINTER(C.c_int)), ("src_par", C.POINTER(C.c_double)),
         ("nrec", C.c_int), ("rec_xyz", C.POINTER(C.c_double)),
+        ("mms", C.c_int), ("mms_nt", C.c_double), ("mms_nx", C.c_double), ("mms_ny", C.c_double),
+        ("mms_nz", C.c_double),
     ]
 
 
@@ -69,6 +71,7 @@ def lib() -> C.CDLL:
         L.orc_get_normals.argtypes = [vp, C.c_int, C.c_int, dp]
         L.orc_get_iface.argtypes = [vp, dp]
         L.orc_get_fault.argtypes = [vp, C.c_int, dp]
+        L.orc_mms_exact.argtypes = [vp, C.c_int, C.c_double, dp]
         L.orc_receiver_index.argtypes = [vp, C.c_int, ip]
         L.orc_final_state.argtypes = [vp, dp, dp, dp]
         L.orc_q4_coefficients.argtypes = [C.c_double, C.c_double, dp, dp]
@@ -160,6 +163,10 @@ class OracleDomain:
                 for k in range(len(sstr)):
                     d.sstr[k], d.pstr[k] = sstr[k], pstr[k]
             d.tau0 = problem.tau0
+            if problem.mms is not None:
+                d.mms = 1
+                d.mms_nt, d.mms_nx, d.mms_ny, d.mms_nz = (problem.mms.nt, problem.mms.nx, problem.mms.ny,
+                                                          problem.mms.nz)
             d.nsrc = len(b.sources)
             d.src_order = problem.source_order
             d.src_alpha = problem.source_alpha
@@ -310,6 +317,12 @@ class OracleDomain:
         nq, nr, ns = self.problem.blocks[0].nqrs
         a = np.zeros((nc, ns, nr))
         lib().orc_get_fault(self.handle, kind, _dptr(a))
+        return a
+
+    def mms_exact(self, t: float, b: int = 0) -> np.ndarray:
+        """Manufactured solution at time t on block b's grid, shape (9, ns, nr, nq)."""
+        a = np.zeros(self._shape(b, 9))
+        lib().orc_mms_exact(self.handle, b, float(t), _dptr(a))
         return a
 
     def receiver_index(self, b: int = 0) -> np.ndarray:

@@ -805,7 +805,63 @@ static void structure(double Ux[9], const double Uq[9], double rho, double mu, d
   Ux[8] = mu * Uq[8];
 }
 
-static void impose_boundary_condition(oblk *b) {
+/* ------------------------------------------------------------------------ */
+/* Manufactured solution: src/mms.f90:136-235                                */
+/* ------------------------------------------------------------------------ */
+static void mms_eval(const orc_desc *d, double t, const double X[3], double u[9]) {
+  const double ct = cos(d->mms_nt * PI_WP * t);
+  const double a = sin(d->mms_nx * PI_WP * X[0]) * sin(d->mms_ny * PI_WP * X[1]) * sin(d->mms_nz * PI_WP * X[2]);
+  const double c = cos(d->mms_nx * PI_WP * X[0]) * cos(d->mms_ny * PI_WP * X[1]) * cos(d->mms_nz * PI_WP * X[2]);
+  for (int k = 0; k < 3; ++k) u[k] = ct * a;
+  for (int k = 3; k < 9; ++k) u[k] = ct * c;
+}
+
+/* time and space derivatives of the solution, :176-235 */
+static void mms_derivs(const orc_desc *d, double t, const double X[3], double ut[9], double ux[9], double uy[9],
+                       double uz[9]) {
+  const double kt = d->mms_nt * PI_WP, kx = d->mms_nx * PI_WP, ky = d->mms_ny * PI_WP, kz = d->mms_nz * PI_WP;
+  const double ct = cos(kt * t), st = sin(kt * t);
+  const double sx = sin(kx * X[0]), cx = cos(kx * X[0]);
+  const double sy = sin(ky * X[1]), cy = cos(ky * X[1]);
+  const double sz = sin(kz * X[2]), cz = cos(kz * X[2]);
+  for (int k = 0; k < 3; ++k) {
+    ut[k] = -kt * st * sx * sy * sz;
+    ux[k] = kx * ct * cx * sy * sz;
+    uy[k] = ky * ct * sx * cy * sz;
+    uz[k] = kz * ct * sx * sy * cz;
+  }
+  for (int k = 3; k < 9; ++k) {
+    ut[k] = -kt * st * cx * cy * cz;
+    ux[k] = -kx * ct * sx * cy * cz;
+    uy[k] = -ky * ct * cx * sy * cz;
+    uz[k] = -kz * ct * cx * cy * sz;
+  }
+}
+
+/* DU -= L(u*) - u*_t at every point (mms_forcing, src/mms.f90:77-134) */
+static void mms_forcing(oblk *b, double t) {
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) {
+        long p = ID(b, x, y, z);
+        double X[3] = {b->X[0][p], b->X[1][p], b->X[2][p]};
+        double ut[9], ux[9], uy[9], uz[9], f[9];
+        mms_derivs(&b->d, t, X, ut, ux, uy, uz);
+        const double lam = b->M[0][p], mu = b->M[1][p], rho = b->M[2][p];
+        f[0] = (1.0 / rho) * (ux[3] + uy[6] + uz[7]);
+        f[1] = (1.0 / rho) * (ux[6] + uy[4] + uz[8]);
+        f[2] = (1.0 / rho) * (ux[7] + uy[8] + uz[5]);
+        f[3] = (2.0 * mu + lam) * ux[0] + lam * uy[1] + lam * uz[2];
+        f[4] = lam * ux[0] + (2.0 * mu + lam) * uy[1] + lam * uz[2];
+        f[5] = lam * ux[0] + lam * uy[1] + (2.0 * mu + lam) * uz[2];
+        f[6] = mu * (uy[0] + ux[1]);
+        f[7] = mu * (uz[0] + ux[2]);
+        f[8] = mu * (uz[1] + uy[2]);
+        for (int c = 0; c < 9; ++c) b->DF[c][p] = b->DF[c][p] - (f[c] - ut[c]);
+      }
+}
+
+static void impose_boundary_condition(oblk *b, double t) {
   const double tau0 = b->d.tau0;
   const double hs_[3] = {b->hq, b->hr, b->hs};
   for (int f = 0; f < 6; ++f) {
@@ -833,6 +889,11 @@ static void impose_boundary_condition(oblk *b) {
         double l3[3], m3[3], n3[3], u[9], ubc[9];
         for (int c = 0; c < 3; ++c) { l3[c] = b->nl[f][c][fp]; m3[c] = b->nm[f][c][fp]; n3[c] = b->nn[f][c][fp]; }
         for (int c = 0; c < 9; ++c) u[c] = b->F[c][p];
+        if (b->d.mms) { /* u - switch*fu, src/BoundaryConditions.f90:84-88 */
+          double X[3] = {b->X[0][p], b->X[1][p], b->X[2][p]}, fu[9];
+          mms_eval(&b->d, t, X, fu);
+          for (int c = 0; c < 9; ++c) u[c] = u[c] - 1.0 * fu[c];
+        }
         bc_point(plus, u, rho, mu, lambda, l3, m3, n3, norm, Zs, Zp, r, ubc);
         for (int c = 0; c < 9; ++c) b->work[f][c][fp] = ubc[c];
       }
@@ -1081,6 +1142,7 @@ static void do_stage(odom *D, int stage, double dt, double t0, int sample, doubl
     rhs_interior(b);
     rhs_near_boundaries(b);
     if (b->nsrc > 0) set_moment_tensor(b, D->t);
+    if (b->d.mms) mms_forcing(b, D->t);
   }
   if (D->nb == 2) { /* exchange_fields_interface, src/domain.f90:696-726 (serial copy) */
     copy_fields_to_boundary(D->B[0]);
@@ -1093,10 +1155,10 @@ static void do_stage(odom *D, int stage, double dt, double t0, int sample, doubl
       }
   }
   /* enforce_bound_iface_conditions, src/domain.f90:615-644 */
-  impose_boundary_condition(D->B[0]);
+  impose_boundary_condition(D->B[0], D->t);
   if (D->nb == 2) orc_iface_couple(D, 2, D->t, stage);
   if (D->nb == 2) {
-    impose_boundary_condition(D->B[1]);
+    impose_boundary_condition(D->B[1], D->t);
     orc_iface_couple(D, 1, D->t, stage);
   }
   if (sample) {
@@ -1247,6 +1309,19 @@ void orc_get_iface(void *dv, double *out) {
     out[7 * k + 5] = sqrt(D->I->Svel[1][k] * D->I->Svel[1][k] + D->I->Svel[2][k] * D->I->Svel[2][k]);
     out[7 * k + 6] = D->I->trup[k];
   }
+}
+void orc_mms_exact(void *dv, int bi, double t, double *out) {
+  oblk *b = ((odom *)dv)->B[bi];
+  long n1 = (long)b->nx * b->ny * b->nz;
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) {
+        long p = ID(b, x, y, z);
+        double X[3] = {b->X[0][p], b->X[1][p], b->X[2][p]}, u[9];
+        mms_eval(&b->d, t, X, u);
+        long q = (x - 1) + (long)b->nx * ((y - 1) + (long)b->ny * (z - 1));
+        for (int c = 0; c < 9; ++c) out[c * n1 + q] = u[c];
+      }
 }
 void orc_receiver_index(void *dv, int bi, int *idx) {
   oblk *b = ((odom *)dv)->B[bi];

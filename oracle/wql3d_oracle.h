@@ -54,6 +54,10 @@ typedef struct {
   const double *src_par;   /* per source 11 values: duration t_init mxx myy mzz mxy mxz myz x y z */
   int nrec;
   const double *rec_xyz;   /* per receiver 3 values */
+  /* manufactured solution (src/mms.f90:136-235): forcing added to the rates and
+     exact boundary data in the face SATs when mms != 0 */
+  int mms;
+  double mms_nt, mms_nx, mms_ny, mms_nz;
 } orc_desc;
 
 typedef struct {
@@ -95,6 +99,8 @@ void orc_get_iface(void *d, double *out);               /* per point: S(4) W(1) 
 int orc_get_fault(void *d, int kind, double *out);
 void orc_receiver_index(void *d, int b, int *idx);      /* 3 per receiver */
 void orc_final_state(void *d, double *maxF, double *maxEta, double *maxB);
+/* manufactured solution at time t on block b's grid: 9*nq*nr*ns (src/mms.f90:136-148) */
+void orc_mms_exact(void *d, int b, double t, double *out);
 
 /* coefficient builders, src/anelastic_q4_model.f90:97-111, src/anelastic_q8_model.f90:100-116 */
 void orc_q4_coefficients(double fmin, double fmax, double *tau, double *weight);

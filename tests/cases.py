@@ -159,3 +159,36 @@ def two_block_case(mesh="cartesian", coupling="locked", response="elastic", n=(1
     an = AnelasticParams(Qs0=40.0, Qp0=80.0, fref=1.0, fmin=0.05, fmax=20.0)
     return Problem(blocks=blocks, response=response, type_of_mesh=mesh, t_final=0.2, CFL=0.4, source_order=4,
                    anelastic=an, interface=ip)
+
+
+def mms_case(n=21, mesh="cartesian", bc=((2, 1, 3), (1, 3, 1)), t_final=0.1, hetero=False, seed=6):
+    """Manufactured-solution problem (src/mms.f90:136-235, nt = 2, nx = ny = nz = 1)
+    on the box [0.1, 1.1] x [0.2, 1.2] x [0.15, 1.15]: forcing in the rates,
+    exact boundary data in the face SATs.  'curvilinear' perturbs the interior
+    of the mesh smoothly (faces stay planar)."""
+    from waveqlab3d_q_gpu_b200.problem import MMSParams
+    kw = {}
+    a, bq = (0.1, 0.2, 0.15), (1.1, 1.2, 1.15)
+    if mesh == "curvilinear":
+        q = np.linspace(0.0, 1.0, n)[None, None, :]
+        r = np.linspace(0.0, 1.0, n)[None, :, None]
+        s = np.linspace(0.0, 1.0, n)[:, None, None]
+        bump = 0.03 * np.sin(np.pi * q) * np.sin(np.pi * r) * np.sin(np.pi * s)
+        shape = (n, n, n)
+        x = a[0] + q * (bq[0] - a[0]) + bump
+        y = a[1] + r * (bq[1] - a[1]) + 0.7 * bump
+        z = a[2] + s * (bq[2] - a[2]) - 0.5 * bump
+        kw["coords"] = np.stack([np.broadcast_to(x, shape), np.broadcast_to(y, shape),
+                                 np.broadcast_to(z, shape)]).copy()
+    if hetero:
+        rng = np.random.default_rng(seed)
+        rho = 2.6 + 0.1 * rng.random((n, n, n))
+        cs = 3.3 + 0.2 * rng.random((n, n, n))
+        cp = np.sqrt(3.0) * cs
+        kw["material"] = np.stack([rho * (cp ** 2 - 2 * cs ** 2), rho * cs ** 2, rho])
+    b = Block(nqrs=(n, n, n), aqrs=a, bqrs=bq, rho_s_p=(2.67, 3.464, 6.0), lqrs=bc[0], rqrs=bc[1], **kw)
+    return Problem(blocks=[b], response="elastic", type_of_mesh=mesh, t_final=t_final, CFL=0.5, mms=MMSParams())
+
+
+def mms_error(fields, exact):
+    return float(np.linalg.norm(fields - exact) / np.linalg.norm(exact))

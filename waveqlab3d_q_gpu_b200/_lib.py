@@ -45,6 +45,8 @@ class DomainDesc(C.Structure):
         ("fs", C.c_double), ("fd", C.c_double), ("Dc", C.c_double),
         ("iface_tau0", dp), ("iface_fs", dp),
         ("max_samples", C.c_int32),
+        ("mms", C.c_int32), ("mms_nt", C.c_double), ("mms_nx", C.c_double), ("mms_ny", C.c_double),
+        ("mms_nz", C.c_double),
         ("block", BlockDesc * 2),
     ]
 

@@ -515,6 +515,15 @@ int setup_block(wql3d_domain *d, int bi) {
     CK(M.get(&Jd, vol));
     rc = put_array<double>(d, h, Xd, 3, h.coords.data(), 0);
     if (rc) return rc;
+    b.X = Xd;
+    b.mms = d->desc.mms ? 1 : 0;
+    if (b.mms) {
+      const double pi = 3.141592653589793;
+      b.mms_k[0] = d->desc.mms_nt * pi;
+      b.mms_k[1] = d->desc.mms_nx * pi;
+      b.mms_k[2] = d->desc.mms_ny * pi;
+      b.mms_k[3] = d->desc.mms_nz * pi;
+    }
     dim3 th(32, 4, 2), gr((h.nq + 31) / 32, (h.nr + 3) / 4, (h.ns + 1) / 2);
     k_metrics<T><<<gr, th, 0, d->stream>>>(b, Xd, metd, Jd);
     CK(cudaGetLastError());
@@ -791,7 +800,7 @@ template <typename T>
 void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = false) {
   Blk<T> &b = blk<T>(d, bi);
   int mesh = d->hb[bi].mesh;
-  if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !tuning().generic) {
+  if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !tuning().generic && !b.mms) {
     // strict interior (z-marching kernel) + near-boundary shell
     switch (d->response) {
       case 0: launch_interior_cart<T, RESP_EL>(d, b, a); launch_shell<T, MESH_CART, RESP_EL>(d, b, a); break;
@@ -802,7 +811,7 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
     return;
   }
   dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
-  if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !tuning().generic) {
+  if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !tuning().generic && !b.mms) {
     // derivative pass, then the point update of every point
     if (a.flags & F_RHS) {
       const int gbx = tuning().grad_bx, gby = 256 / gbx / 2;

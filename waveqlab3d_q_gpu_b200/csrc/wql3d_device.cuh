@@ -74,6 +74,9 @@ struct Blk {
   T *FC;                // FP32 path: Kahan compensation for F (9 components)
   T *G;                 // curvilinear: 18 derivative terms per point from k_curv_grad (see there)
   T *S6;                // curvilinear anelastic: per stress component the sum of the memory variables
+  const double *X;      // physical coordinates x, y, z (FP64, field layout)
+  int mms;              // manufactured-solution forcing and boundary data
+  double mms_k[4];      // nt*pi, nx*pi, ny*pi, nz*pi
   T *M;                 // lambda, mu, rho
   // Cartesian: per-axis diagonal metric 1/X_a(i) (index 1..n)
   const T *mq, *mr, *ms;
@@ -294,13 +297,65 @@ __device__ __forceinline__ void cart_basis(int axis, T l[3], T m[3], T n[3]) {
   else { n[2] = 1; m[1] = 1; l[0] = -1; }
 }
 
+// ---------------------------------------------------------------------------
+// Manufactured solution (src/mms.f90:136-235): v = cos(nt pi t) sin sin sin,
+// sigma = cos(nt pi t) cos cos cos
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ void mms_exact(const Blk<T> &b, double t, long long p, double u[9]) {
+  const double X0 = b.X[p], X1 = b.X[b.vol + p], X2 = b.X[2 * b.vol + p];
+  const double ct = cos(b.mms_k[0] * t);
+  const double a = sin(b.mms_k[1] * X0) * sin(b.mms_k[2] * X1) * sin(b.mms_k[3] * X2);
+  const double c = cos(b.mms_k[1] * X0) * cos(b.mms_k[2] * X1) * cos(b.mms_k[3] * X2);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) u[k] = ct * a;
+#pragma unroll
+  for (int k = 3; k < 9; ++k) u[k] = ct * c;
+}
+
+// rates -= L(u*) - u*_t (mms_forcing, src/mms.f90:77-134)
+template <typename T>
+__device__ void mms_forcing(const Blk<T> &b, double t, long long p, T df[9]) {
+  const double X0 = b.X[p], X1 = b.X[b.vol + p], X2 = b.X[2 * b.vol + p];
+  const double kt = b.mms_k[0], kx = b.mms_k[1], ky = b.mms_k[2], kz = b.mms_k[3];
+  const double ct = cos(kt * t), st = sin(kt * t);
+  const double sx = sin(kx * X0), cx = cos(kx * X0), sy = sin(ky * X1), cy = cos(ky * X1);
+  const double sz = sin(kz * X2), cz = cos(kz * X2);
+  // velocity components 0-2 share one profile, stresses 3-8 another
+  const double vt = -kt * st * sx * sy * sz, vx = kx * ct * cx * sy * sz, vy = ky * ct * sx * cy * sz,
+               vz = kz * ct * sx * sy * cz;
+  const double st_ = -kt * st * cx * cy * cz, sx_ = -kx * ct * sx * cy * cz, sy_ = -ky * ct * cx * sy * cz,
+               sz_ = -kz * ct * cx * cy * sz;
+  const double lam = (double)b.M[p], mu = (double)b.M[b.vol + p], rho = (double)b.M[2 * b.vol + p];
+  double f[9];
+  f[0] = (1.0 / rho) * (sx_ + sy_ + sz_);
+  f[1] = (1.0 / rho) * (sx_ + sy_ + sz_);
+  f[2] = (1.0 / rho) * (sx_ + sy_ + sz_);
+  f[3] = (2.0 * mu + lam) * vx + lam * vy + lam * vz;
+  f[4] = lam * vx + (2.0 * mu + lam) * vy + lam * vz;
+  f[5] = lam * vx + lam * vy + (2.0 * mu + lam) * vz;
+  f[6] = mu * (vy + vx);
+  f[7] = mu * (vz + vx);
+  f[8] = mu * (vz + vy);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) df[c] = df[c] - (T)(f[c] - (c < 3 ? vt : st_));
+}
+
 template <typename T, int MESH, bool SEP>
-__device__ void add_face_sats(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T df[9], bool pml_point) {
+__device__ void add_face_sats(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T df[9], bool pml_point,
+                              double t) {
   const int pos[3] = {x, y, z};
   const int nn[3] = {b.nx, b.ny, b.nz};
   T u[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) u[c] = F[c * b.vol + p];
+  if (b.mms) {
+    // u - switch * fu with the exact solution (src/BoundaryConditions.f90:84-88)
+    double fu[9];
+    mms_exact<T>(b, t, p, fu);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) u[c] = (T)((double)u[c] - fu[c]);
+  }
   const T lam = b.M[p], mu = b.M[b.vol + p], rho = b.M[2 * b.vol + p];
   for (int f = 0; f < 6; ++f) {
     int type = b.bc[f];
@@ -859,8 +914,9 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
   if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
       z >= b.sbox[4] && z <= b.sbox[5])
     add_sources<T, MESH>(b, tst, x, y, z, p, df);
+  if (b.mms && (a.flags & F_SOURCE)) mms_forcing<T>(b, tst, p, df);
   if ((a.flags & F_SAT) && (x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz))
-    add_face_sats<T, MESH, SEP>(b, F, x, y, z, p, df, in_pml);
+    add_face_sats<T, MESH, SEP>(b, F, x, y, z, p, df, in_pml, tst);
   if ((a.flags & F_ISAT)) {
     // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
     int side = x == 1 ? 0 : (x == b.nx ? 1 : -1);
@@ -1354,7 +1410,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
     add_sources<T, MESH_CURV>(b, tst, x, y, z, p, df);
   }
-  if ((a.flags & F_SAT) && face_pt) add_face_sats<T, MESH_CURV, false>(b, F, x, y, z, p, df, in_pml);
+  if ((a.flags & F_SAT) && face_pt) add_face_sats<T, MESH_CURV, false>(b, F, x, y, z, p, df, in_pml, 0.0);
   if (defer && (a.flags & F_UPDATE)) {
     slab_integrate<T, 2>(b, a, x, y, z, sz);
     slab_integrate<T, 1>(b, a, x, y, z, sy);

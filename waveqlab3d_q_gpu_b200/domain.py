@@ -108,6 +108,9 @@ class Domain:
             nt = nsteps_hint if nsteps_hint is not None else problem.nt()
             max_samples = max(1, (nt + max(problem.w_stride, 1) - 1) // max(problem.w_stride, 1) + 1)
         d.max_samples = int(max_samples)
+        if problem.mms is not None:
+            d.mms = 1
+            d.mms_nt, d.mms_nx, d.mms_ny, d.mms_nz = problem.mms.nt, problem.mms.nx, problem.mms.ny, problem.mms.nz
         for i, b in enumerate(problem.blocks):
             bd = d.block[i]
             bd.nq, bd.nr, bd.ns = b.nqrs

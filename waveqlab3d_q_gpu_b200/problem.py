@@ -164,6 +164,19 @@ class InterfaceParams:
 
 
 @dataclass
+class MMSParams:
+    """Manufactured solution of src/mms.f90:136-235: v = cos(nt pi t) sin sin sin,
+    sigma = cos(nt pi t) cos cos cos (wavenumbers nx, ny, nz times pi).  When a
+    problem carries one, the rates get the forcing u*_t - L(u*) and the face
+    SATs the exact boundary data (src/BoundaryConditions.f90:84-88)."""
+
+    nt: float = 2.0
+    nx: float = 1.0
+    ny: float = 1.0
+    nz: float = 1.0
+
+
+@dataclass
 class Problem:
     """``&problem_list`` plus blocks."""
 
@@ -182,6 +195,7 @@ class Problem:
     anelastic: AnelasticParams = field(default_factory=AnelasticParams)
     interface: InterfaceParams = field(default_factory=InterfaceParams)
     tau0: float = TAU0_TRADITIONAL6
+    mms: Optional[MMSParams] = None
 
     def dt(self) -> float:
         """Global time step, src/domain.f90:150-171 and src/block.f90:495-510.
