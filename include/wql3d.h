@@ -145,6 +145,11 @@ typedef struct wql3d_domain_desc {
      generic per-point kernel */
   int32_t mms;
   double mms_nt, mms_nx, mms_ny, mms_nz;
+  /* one block per process (the reference's one-rank-per-block run): with
+     nblocks = 1, remote_side = 1 makes this block side 1 of a q-interface
+     (its q-max face), 2 side 2 (its q-min face); the other side's face trace
+     arrives through the interface buffers every stage */
+  int32_t remote_side;
   wql3d_block_desc block[2];
 } wql3d_domain_desc;
 
@@ -175,6 +180,26 @@ int wql3d_get_time(wql3d_domain *d, double *t);
 int wql3d_stage(wql3d_domain *d, int stage, double dt);
 int wql3d_time_step(wql3d_domain *d, double dt, int n, int w_stride);
 int wql3d_run(wql3d_domain *d, double dt, int n_first, int nsteps, int w_stride);
+
+/* stage-by-stage driving (domains with a remote interface side, or any
+   domain): wql3d_begin_step sets the step counter n and takes the stage-1
+   receiver sample (time_step.f90:137); wql3d_stage then runs the stages, the
+   fifth advancing the domain time. */
+int wql3d_begin_step(wql3d_domain *d, int n, int w_stride);
+
+/* remote interface side (remote_side != 0; src/domain.f90:696-754,
+   exchange_fields_interface / exchange_materials_interface): device buffers
+   of this block's face trace (send) and the other side's (recv), each
+   9 x ns x nr components of elem_bytes (field precision), y fastest;
+   wql3d_pack_interface fills send from the current fields on the domain
+   stream; the caller moves send to the peer's recv before each wql3d_stage.
+   The face material (lambda, mu, rho; 3 x ns x nr doubles) is exchanged once:
+   wql3d_get_interface_material gives this side's, wql3d_set_interface_remote_material
+   takes the peer's.  wql3d_time_step / wql3d_run are refused (WQL3D_ESTATE). */
+int wql3d_interface_buffers(wql3d_domain *d, void **send, void **recv, int64_t *count, int32_t *elem_bytes);
+int wql3d_pack_interface(wql3d_domain *d);
+int wql3d_get_interface_material(wql3d_domain *d, double *M);
+int wql3d_set_interface_remote_material(wql3d_domain *d, const double *M);
 
 /* split stage operations (bring-up path, same arithmetic as wql3d_stage) */
 int wql3d_scale_rates(wql3d_domain *d, double A);                         /* domain.f90:922-949 */

@@ -47,6 +47,7 @@ class DomainDesc(C.Structure):
         ("max_samples", C.c_int32),
         ("mms", C.c_int32), ("mms_nt", C.c_double), ("mms_nx", C.c_double), ("mms_ny", C.c_double),
         ("mms_nz", C.c_double),
+        ("remote_side", C.c_int32),
         ("block", BlockDesc * 2),
     ]
 
@@ -68,6 +69,12 @@ SIGNATURES = {
     "wql3d_stage": [C.c_void_p, C.c_int, C.c_double],
     "wql3d_time_step": [C.c_void_p, C.c_double, C.c_int, C.c_int],
     "wql3d_run": [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int],
+    "wql3d_begin_step": [C.c_void_p, C.c_int, C.c_int],
+    "wql3d_interface_buffers": [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                C.POINTER(C.c_int32)],
+    "wql3d_pack_interface": [C.c_void_p],
+    "wql3d_get_interface_material": [C.c_void_p, dp],
+    "wql3d_set_interface_remote_material": [C.c_void_p, dp],
     "wql3d_scale_rates": [C.c_void_p, C.c_double],
     "wql3d_set_rates_rhs": [C.c_void_p],
     "wql3d_enforce_bound_iface_conditions": [C.c_void_p, C.c_int],

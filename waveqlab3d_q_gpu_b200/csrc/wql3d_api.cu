@@ -1037,6 +1037,17 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     rc = d->fp32 ? setup_block<float>(d, i) : setup_block<double>(d, i);
     if (rc) return cleanup(rc);
   }
+  if (d->nblocks == 1 && d->desc.remote_side != 0) {
+    const int side = d->desc.remote_side;
+    rc = d->fp32 ? setup_iface_remote<float>(d->iface, d->desc, d->bf[0], d->hb[0].coords, side, d->mem, d->stream)
+                 : setup_iface_remote<double>(d->iface, d->desc, d->bd[0], d->hb[0].coords, side, d->mem, d->stream);
+    if (rc) return cleanup(fail(rc, "remote interface setup failed"));
+    d->has_iface = true;
+    if (d->fp32) d->bf[0].isat[side == 1 ? 1 : 0] = (float *)(side == 1 ? d->iface.sat_m : d->iface.sat_p);
+    else d->bd[0].isat[side == 1 ? 1 : 0] = (double *)(side == 1 ? d->iface.sat_m : d->iface.sat_p);
+  } else if (d->desc.remote_side != 0) {
+    return cleanup(fail(WQL3D_EINVAL, "remote_side needs nblocks = 1"));
+  }
   if (d->nblocks == 2) {
     rc = d->fp32 ? setup_iface<float>(d->iface, d->desc, d->bf[0], d->bf[1], d->hb[0].coords, d->hb[1].coords,
                                       d->mem, d->stream)
@@ -1203,8 +1214,75 @@ int wql3d_stage(wql3d_domain *d, int stage, double dt) {
   return WQL3D_OK;
 }
 
+int wql3d_begin_step(wql3d_domain *d, int n, int w_stride) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  h.n = n;
+  CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
+  int rc = d->fp32 ? enqueue_sample<float>(d, w_stride) : enqueue_sample<double>(d, w_stride);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_interface_buffers(wql3d_domain *d, void **send, void **recv, int64_t *count, int32_t *elem_bytes) {
+  if (!d || !d->has_iface || !d->iface.remote) return fail(WQL3D_EINVAL, "no remote interface side");
+  if (send) *send = d->iface.send;
+  if (recv) *recv = d->iface.recv;
+  if (count) *count = (int64_t)9 * d->iface.ny * d->iface.nz;
+  if (elem_bytes) *elem_bytes = d->fp32 ? 4 : 8;
+  return WQL3D_OK;
+}
+
+int wql3d_pack_interface(wql3d_domain *d) {
+  if (!d || !d->has_iface || !d->iface.remote) return fail(WQL3D_EINVAL, "no remote interface side");
+  const int n = d->iface.ny * d->iface.nz;
+  if (d->fp32) k_pack_face<float><<<(n + 127) / 128, 128, 0, d->stream>>>(d->bf[0], d->cur, d->iface.remote, (float *)d->iface.send);
+  else k_pack_face<double><<<(n + 127) / 128, 128, 0, d->stream>>>(d->bd[0], d->cur, d->iface.remote, (double *)d->iface.send);
+  d->launches++;
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_get_interface_material(wql3d_domain *d, double *M) {
+  if (!d || !d->has_iface || !d->iface.remote || !M) return fail(WQL3D_EINVAL, "no remote interface side");
+  const int n = d->iface.ny * d->iface.nz;
+  // the receive buffer is free between stages: stage the material through it
+  if (d->fp32) {
+    k_pack_face_material<float><<<(n + 127) / 128, 128, 0, d->stream>>>(d->bf[0], d->iface.remote, (float *)d->iface.recv);
+    std::vector<float> h((size_t)3 * n);
+    CK(cudaMemcpyAsync(h.data(), d->iface.recv, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    for (size_t i = 0; i < h.size(); ++i) M[i] = h[i];
+  } else {
+    k_pack_face_material<double><<<(n + 127) / 128, 128, 0, d->stream>>>(d->bd[0], d->iface.remote, (double *)d->iface.recv);
+    CK(cudaMemcpyAsync(M, d->iface.recv, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  return WQL3D_OK;
+}
+
+int wql3d_set_interface_remote_material(wql3d_domain *d, const double *M) {
+  if (!d || !d->has_iface || !d->iface.remote || !M) return fail(WQL3D_EINVAL, "no remote interface side");
+  const int n = d->iface.ny * d->iface.nz;
+  if (d->fp32) {
+    std::vector<float> h((size_t)3 * n);
+    for (size_t i = 0; i < h.size(); ++i) h[i] = (float)M[i];
+    CK(cudaMemcpyAsync(d->iface.oppM, h.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  } else {
+    CK(cudaMemcpyAsync(d->iface.oppM, M, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  return WQL3D_OK;
+}
+
 int wql3d_time_step(wql3d_domain *d, double dt, int n, int w_stride) {
   if (!d) return fail(WQL3D_EINVAL, "null domain");
+  if (d->has_iface && d->iface.remote)
+    return fail(WQL3D_ESTATE, "remote interface side: drive with wql3d_begin_step / pack / exchange / wql3d_stage");
   DevTime h;
   CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
@@ -1218,6 +1296,8 @@ int wql3d_time_step(wql3d_domain *d, double dt, int n, int w_stride) {
 
 int wql3d_run(wql3d_domain *d, double dt, int n_first, int nsteps, int w_stride) {
   if (!d) return fail(WQL3D_EINVAL, "null domain");
+  if (d->has_iface && d->iface.remote)
+    return fail(WQL3D_ESTATE, "remote interface side: drive with wql3d_begin_step / pack / exchange / wql3d_stage");
   if (nsteps < 0) return fail(WQL3D_EINVAL, "nsteps");
   DevTime h;
   CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));

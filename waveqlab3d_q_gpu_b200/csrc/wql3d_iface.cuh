@@ -43,6 +43,13 @@ struct IfaceDev {
   double *fs[2] = {nullptr, nullptr};     // per side: n static friction
   void *sat_m = nullptr;   // SAT vector added at block 1's q-max face (F_x)
   void *sat_p = nullptr;   // SAT vector added at block 2's q-min face (G_x)
+  // remote interface side: this domain holds one block, side `remote` (1: its
+  // q-max face, 2: its q-min face); the other side's face trace and material
+  // arrive in recv / oppM
+  int remote = 0;
+  void *send = nullptr;    // this block's face trace, 9 x n (field precision)
+  void *recv = nullptr;    // the other side's face trace, 9 x n
+  void *oppM = nullptr;    // the other side's lambda, mu, rho at the face, 3 x n
 };
 
 // boxcar of unit amplitude on (-w, w), 1/2 within 100 eps of the edges
@@ -122,6 +129,60 @@ int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, co
       return WQL3D_ECUDA;
   }
   // the host vectors above go out of scope: finish the copies first
+  if (cudaStreamSynchronize(s) != cudaSuccess) return WQL3D_ECUDA;
+  return WQL3D_OK;
+}
+
+// Remote side: buffers, state and this side's prestress / strength map.
+template <typename T, typename AllocT>
+int setup_iface_remote(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b, const std::vector<double> &coords,
+                       int side, AllocT &mem, cudaStream_t s) {
+  if (side != 1 && side != 2) return WQL3D_EINVAL;
+  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_LINEAR) return WQL3D_EINVAL;
+  if (desc.fault_problem != WQL3D_FAULT_MAPS && desc.fault_problem != WQL3D_FAULT_TPV5) return WQL3D_EINVAL;
+  const int ny = b.ny, nz = b.nz;
+  const long long n = (long long)ny * nz;
+  I.ny = ny;
+  I.nz = nz;
+  I.coupling = desc.coupling;
+  I.serial = 0;
+  I.fd = desc.fd;
+  I.Dc = desc.Dc;
+  I.remote = side;
+  if (mem.get(&I.S, 4 * n) || mem.get(&I.DS, 4 * n) || mem.get(&I.W, n) || mem.get(&I.DW, n) ||
+      mem.get(&I.Svel, 3 * n) || mem.get(&I.Uhat, 6 * n) || mem.get(&I.Vhat, 6 * n) || mem.get(&I.trup, n))
+    return WQL3D_ENOMEM;
+  T *sat = nullptr, *snd = nullptr, *rcv = nullptr, *om = nullptr;
+  if (mem.get(&sat, 9 * n) || mem.get(&snd, 9 * n) || mem.get(&rcv, 9 * n) || mem.get(&om, 3 * n))
+    return WQL3D_ENOMEM;
+  if (side == 1) I.sat_m = sat;
+  else I.sat_p = sat;
+  I.send = snd;
+  I.recv = rcv;
+  I.oppM = om;
+  std::vector<double> tr((size_t)n, 1.0e9);
+  if (cudaMemcpyAsync(I.trup, tr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return WQL3D_ECUDA;
+  std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs);
+  const int xend = side == 1 ? b.nx : 1;
+  const long long nb = (long long)b.nx * ny * nz;
+  for (int z = 1; z <= nz; ++z)
+    for (int y = 1; y <= ny; ++y) {
+      long long k = (long long)(y - 1) + (long long)ny * (z - 1);
+      if (desc.fault_problem == WQL3D_FAULT_TPV5) {
+        long long q = (long long)(xend - 1) + (long long)b.nx * ((y - 1) + (long long)ny * (z - 1));
+        double x[3] = {coords[(size_t)q], coords[(size_t)(nb + q)], coords[(size_t)(2 * nb + q)]};
+        tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
+      } else {
+        if (desc.iface_tau0)
+          for (int c = 0; c < 3; ++c) t0[(size_t)(c * n + k)] = desc.iface_tau0[c * n + k];
+        if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
+      }
+    }
+  if (mem.get(&I.t0[side - 1], 3 * n) || mem.get(&I.fs[side - 1], n)) return WQL3D_ENOMEM;
+  if (cudaMemcpyAsync(I.t0[side - 1], t0.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(I.fs[side - 1], f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return WQL3D_ECUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return WQL3D_ECUDA;
   return WQL3D_OK;
 }
@@ -405,10 +466,133 @@ __global__ void k_iface_scale(IfaceDev I, double A) {
   I.DW[k] = __dmul_rn(A, I.DW[k]);
 }
 
+// this block's interface face trace into the send buffer (copy_fields_to_boundary,
+// src/block.f90:466-482)
+template <typename T>
+__global__ void k_pack_face(Blk<T> b, int cur, int side, T *send) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = b.ny * b.nz;
+  if (k >= n) return;
+  const int y = k % b.ny + 1, z = k / b.ny + 1;
+  const T *F = cur ? b.F1 : b.F0;
+  const long long p = pidx(b, side == 1 ? b.nx : 1, y, z);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) send[c * n + k] = F[c * b.vol + p];
+}
+
+// One side of the interface (the other block lives in another process): the
+// same law, outputs and SAT vector as k_iface's side I.remote, with the
+// other side's trace and material from recv / oppM.  Each process keeps its
+// own slip state and adds to it once per stage (src/domain.f90:615-644 on
+// one rank per block).
+template <typename T>
+__global__ void __launch_bounds__(128) k_iface_remote(Blk<T> b, IfaceDev I, StageArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = I.ny * I.nz;
+  if (k >= n) return;
+  const int side = I.remote;
+  if (a.flags & F_ISAT) {
+    const int y = k % I.ny + 1, z = k / I.ny + 1;
+    const T *F = a.cur ? b.F1 : b.F0;
+    const long long p = pidx(b, side == 1 ? b.nx : 1, y, z);
+    const T *R = (const T *)I.recv;
+    const T *OM = (const T *)I.oppM;
+    double own[9], opp[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      own[c] = (double)F[c * b.vol + p];
+      opp[c] = (double)R[c * n + k];
+    }
+    const double *uF = side == 1 ? own : opp;
+    const double *vF = side == 1 ? opp : own;
+    const double lo = (double)b.M[p], mo = (double)b.M[b.vol + p], ro = (double)b.M[2 * b.vol + p];
+    const double lr = (double)OM[k], mr = (double)OM[n + k], rr = (double)OM[2 * n + k];
+    const double lam1 = side == 1 ? lo : lr, mu1 = side == 1 ? mo : mr, rho1 = side == 1 ? ro : rr;
+    const double lam2 = side == 1 ? lr : lo, mu2 = side == 1 ? mr : mo, rho2 = side == 1 ? rr : ro;
+    const double c1p = sqrt(__dadd_rn(__dmul_rn(2.0, mu1), lam1) / rho1), c1s = sqrt(mu1 / rho1);
+    const double c2p = sqrt(__dadd_rn(__dmul_rn(2.0, mu2), lam2) / rho2), c2s = sqrt(mu2 / rho2);
+    const double Z1s = __dmul_rn(rho1, c1s), Z2s = __dmul_rn(rho2, c2s);
+    const double Z1p = __dmul_rn(rho1, c1p), Z2p = __dmul_rn(rho2, c2p);
+    const double S4 = I.S[3 * n + k];
+    double ds[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      ds[c] = I.DS[c * n + k];
+      if (a.flags & F_SCALE) ds[c] = __dmul_rn(a.A, ds[c]);
+    }
+    const T *B = b.nrm[side == 1 ? 1 : 0];
+    double n3[3], m3[3], l3[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      l3[c] = (double)B[(0 + c) * n + k];
+      m3[c] = (double)B[(3 + c) * n + k];
+      n3[c] = (double)B[(6 + c) * n + k];
+    }
+    double u[6], v[6];
+    u[0] = uF[0]; u[1] = uF[1]; u[2] = uF[2];
+    v[0] = vF[0]; v[1] = vF[1]; v[2] = vF[2];
+    {
+      const double su[3] = {uF[3], uF[6], uF[7]}, su2[3] = {uF[6], uF[4], uF[8]}, su3[3] = {uF[7], uF[8], uF[5]};
+      const double sv[3] = {vF[3], vF[6], vF[7]}, sv2[3] = {vF[6], vF[4], vF[8]}, sv3[3] = {vF[7], vF[8], vF[5]};
+      u[3] = dot3(n3, su); u[4] = dot3(n3, su2); u[5] = dot3(n3, su3);
+      v[3] = dot3(n3, sv); v[4] = dot3(n3, sv2); v[5] = dot3(n3, sv3);
+    }
+    rot_in(u, n3, m3, l3);
+    rot_in(v, n3, m3, l3);
+    const double T0[3] = {I.t0[side - 1][k], I.t0[side - 1][n + k], I.t0[side - 1][2 * n + k]};
+    double P[6], Q[6];
+    iface_law(I, u, v, Z1s, Z2s, Z1p, Z2p, T0, I.fs[side - 1][k], S4, P, Q);
+    const double Vel = sqrt(__dadd_rn(__dmul_rn(__dsub_rn(Q[1], P[1]), __dsub_rn(Q[1], P[1])),
+                                      __dmul_rn(__dsub_rn(Q[2], P[2]), __dsub_rn(Q[2], P[2]))));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ds[c] = __dsub_rn(__dadd_rn(ds[c], Q[c]), P[c]);
+    ds[3] = __dadd_rn(ds[3], Vel);
+    if (a.stage == 1) {
+      const double Tn = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[0];
+      const double Tm = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[1];
+      const double Tl = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double sv = __dsub_rn(Q[c], P[c]);
+        I.Uhat[c * n + k] = sv;
+        I.Vhat[c * n + k] = sv;
+        I.Svel[c * n + k] = sv;
+      }
+      I.Uhat[3 * n + k] = __dadd_rn(P[3], Tn); I.Vhat[3 * n + k] = __dadd_rn(Q[3], Tn);
+      I.Uhat[4 * n + k] = __dadd_rn(P[4], Tm); I.Vhat[4 * n + k] = __dadd_rn(Q[4], Tm);
+      I.Uhat[5 * n + k] = __dadd_rn(P[5], Tl); I.Vhat[5 * n + k] = __dadd_rn(Q[5], Tl);
+      const double s1 = __dsub_rn(Q[1], P[1]), s2 = __dsub_rn(Q[2], P[2]);
+      if (sqrt(__dadd_rn(__dmul_rn(s1, s1), __dmul_rn(s2, s2))) > 1.0e-3) I.trup[k] = fmin(I.trup[k], a.time->t);
+    }
+    rot_back(u, n3, m3, l3);
+    rot_back(v, n3, m3, l3);
+    rot_back(P, n3, m3, l3);
+    rot_back(Q, n3, m3, l3);
+    const double qx = (double)b.met[(long long)0 * b.vol + p];
+    const double qy = (double)b.met[(long long)3 * b.vol + p];
+    const double qz = (double)b.met[(long long)6 * b.vol + p];
+    double sat[9];
+    if (side == 1) iface_sat(1, u, P, lam1, mu1, rho1, n3, m3, l3, qx, qy, qz, sat);
+    else iface_sat(2, v, Q, lam2, mu2, rho2, n3, m3, l3, qx, qy, qz, sat);
+    T *out = (T *)(side == 1 ? I.sat_m : I.sat_p);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) out[c * n + k] = (T)sat[c];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) I.DS[c * n + k] = ds[c];
+    if (a.flags & F_SCALE) I.DW[k] = __dmul_rn(a.A, I.DW[k]);
+  }
+  if (a.flags & F_UPDATE) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) I.S[c * n + k] = __dadd_rn(I.S[c * n + k], __dmul_rn(a.Bdt, I.DS[c * n + k]));
+    I.W[k] = __dadd_rn(I.W[k], __dmul_rn(a.Bdt, I.DW[k]));
+  }
+}
+
 template <typename T>
 void launch_iface(IfaceDev &I, const Blk<T> &b0, const Blk<T> &b1, const StageArgs &a, cudaStream_t s) {
   const int n = I.ny * I.nz;
-  k_iface<T><<<(n + 127) / 128, 128, 0, s>>>(b0, b1, I, a);
+  if (I.remote) k_iface_remote<T><<<(n + 127) / 128, 128, 0, s>>>(b0, I, a);
+  else k_iface<T><<<(n + 127) / 128, 128, 0, s>>>(b0, b1, I, a);
 }
 
 template <typename T>
@@ -422,7 +606,20 @@ void launch_iface_update(IfaceDev &I, const Blk<T> &b0, const Blk<T> &b1, double
   a.dt = 0.0;
   a.time = nullptr;
   const int n = I.ny * I.nz;
-  k_iface<T><<<(n + 127) / 128, 128, 0, s>>>(b0, b1, I, a);
+  if (I.remote) k_iface_remote<T><<<(n + 127) / 128, 128, 0, s>>>(b0, I, a);
+  else k_iface<T><<<(n + 127) / 128, 128, 0, s>>>(b0, b1, I, a);
+}
+
+// this block's face material (lambda, mu, rho) into a 3 x n device buffer
+template <typename T>
+__global__ void k_pack_face_material(Blk<T> b, int side, T *out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = b.ny * b.nz;
+  if (k >= n) return;
+  const int y = k % b.ny + 1, z = k / b.ny + 1;
+  const long long p = pidx(b, side == 1 ? b.nx : 1, y, z);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c * n + k] = b.M[c * b.vol + p];
 }
 
 inline void iface_scale(IfaceDev &I, double A, cudaStream_t s) {

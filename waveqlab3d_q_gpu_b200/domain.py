@@ -59,19 +59,30 @@ class Domain:
     """One or two blocks resident on the current CUDA device."""
 
     def __init__(self, problem: Problem, precision: str = "fp64", max_samples: Optional[int] = None,
-                 nsteps_hint: Optional[int] = None):
+                 nsteps_hint: Optional[int] = None, remote_block: Optional[int] = None):
+        """``remote_block`` = r holds only block r of a two-block problem; the
+        other block lives in another process and the interface face is
+        exchanged every stage (see :mod:`waveqlab3d_q_gpu_b200.distributed`)."""
         from . import anelastic as an
 
         L = _lib.load()
         self.problem = problem
         self.precision = precision
         self._keep: List[np.ndarray] = []
-        nb = len(problem.blocks)
+        if remote_block is not None:
+            if len(problem.blocks) != 2 or remote_block not in (0, 1):
+                raise ValueError("remote_block needs a two-block problem and r in (0, 1)")
+            self.blocks = [problem.blocks[remote_block]]
+        else:
+            self.blocks = list(problem.blocks)
+        self.remote_block = remote_block
+        nb = len(self.blocks)
         if nb not in (1, 2):
             raise ValueError("one or two blocks")
         d = _lib.DomainDesc()
         d.abi_version = _lib.ABI_VERSION
         d.nblocks = nb
+        d.remote_side = 0 if remote_block is None else remote_block + 1
         d.precision = 0 if precision == "fp64" else 1
         d.response = RESPONSES[problem.response]
         d.coarse_grain = 1 if (problem.response == "anelastic-fQ8" and problem.anelastic.coarse_grain == 2) else 0
@@ -91,7 +102,7 @@ class Domain:
         d.serial_shared = 1 if ip.serial_shared else 0
         d.fault_problem = FAULT_PROBLEMS[ip.problem]
         d.fs, d.fd, d.Dc = ip.fs, ip.fd, ip.Dc
-        if nb == 2:
+        if nb == 2 or remote_block is not None:
             nq, nr, ns = problem.blocks[0].nqrs
             if ip.tau0_n is not None or ip.tau0_m is not None or ip.tau0_l is not None:
                 t0 = np.zeros((3, ns, nr))
@@ -111,7 +122,7 @@ class Domain:
         if problem.mms is not None:
             d.mms = 1
             d.mms_nt, d.mms_nx, d.mms_ny, d.mms_nz = problem.mms.nt, problem.mms.nx, problem.mms.ny, problem.mms.nz
-        for i, b in enumerate(problem.blocks):
+        for i, b in enumerate(self.blocks):
             bd = d.block[i]
             bd.nq, bd.nr, bd.ns = b.nqrs
             bd.mesh = 1 if problem.type_of_mesh == "curvilinear" else 0
@@ -231,7 +242,7 @@ class Domain:
 
     # ------------------------------------------------------------------ data
     def _shape(self, b: int, ncomp: int, host_nb: int = 0):
-        nq, nr, ns = self.problem.blocks[b].nqrs
+        nq, nr, ns = self.blocks[b].nqrs
         return (ncomp, ns + 2 * host_nb, nr + 2 * host_nb, nq + 2 * host_nb)
 
     def fields(self, b: int = 0, host_nb: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
@@ -254,7 +265,7 @@ class Domain:
 
     def eta(self, b: int = 0) -> np.ndarray:
         nm = self.problem.nmech
-        nq, nr, ns = self.problem.blocks[b].nqrs
+        nq, nr, ns = self.blocks[b].nqrs
         a = np.zeros((6, nm, ns, nr, nq))
         _lib.check(_lib.load().wql3d_get_memory_variables(self.handle, b, _ptr(a)), "wql3d_get_memory_variables")
         return a
@@ -265,10 +276,38 @@ class Domain:
         return a
 
     def interface(self) -> np.ndarray:
-        nq, nr, ns = self.problem.blocks[0].nqrs
+        nq, nr, ns = self.blocks[0].nqrs
         a = np.zeros((ns, nr, 7))
         _lib.check(_lib.load().wql3d_get_interface(self.handle, _ptr(a)), "wql3d_get_interface")
         return a
+
+    # stage-by-stage driving and the remote interface side
+    def begin_step(self, n: Optional[int] = None):
+        """Step counter and stage-1 receiver sample (time_step.f90:137) before wql3d_stage calls."""
+        n = self.n if n is None else n
+        _lib.check(_lib.load().wql3d_begin_step(self.handle, int(n), int(self.problem.w_stride)), "wql3d_begin_step")
+
+    def interface_buffers(self):
+        """(send_ptr, recv_ptr, count, elem_bytes) of a remote interface side."""
+        snd, rcv = C.c_void_p(), C.c_void_p()
+        cnt, eb = C.c_int64(), C.c_int32()
+        _lib.check(_lib.load().wql3d_interface_buffers(self.handle, C.byref(snd), C.byref(rcv), C.byref(cnt),
+                                                       C.byref(eb)), "wql3d_interface_buffers")
+        return snd.value, rcv.value, cnt.value, eb.value
+
+    def pack_interface(self):
+        _lib.check(_lib.load().wql3d_pack_interface(self.handle), "wql3d_pack_interface")
+
+    def interface_material(self) -> np.ndarray:
+        nq, nr, ns = self.blocks[0].nqrs
+        a = np.zeros((3, ns, nr))
+        _lib.check(_lib.load().wql3d_get_interface_material(self.handle, _ptr(a)), "wql3d_get_interface_material")
+        return a
+
+    def set_interface_remote_material(self, M: np.ndarray):
+        a = np.ascontiguousarray(M, dtype=np.float64)
+        _lib.check(_lib.load().wql3d_set_interface_remote_material(self.handle, _ptr(a)),
+                   "wql3d_set_interface_remote_material")
 
     FAULT_KINDS = {"S": (0, 4), "Svel": (1, 3), "Uhat": (2, 6), "Vhat": (3, 6), "state": (4, 1), "trup": (5, 1)}
 
@@ -277,13 +316,13 @@ class Domain:
         (ncomp, ns, nr), the layout of the reference's ``_interface.*`` files
         (src/fault_output.f90:73-122); ``Uface`` / ``Vface`` come from :meth:`fields`."""
         kind, nc = self.FAULT_KINDS[name]
-        nq, nr, ns = self.problem.blocks[0].nqrs
+        nq, nr, ns = self.blocks[0].nqrs
         a = np.zeros((nc, ns, nr))
         _lib.check(_lib.load().wql3d_get_fault_output(self.handle, kind, _ptr(a)), "wql3d_get_fault_output")
         return a
 
     def seismograms(self, b: int = 0) -> np.ndarray:
-        blk = self.problem.blocks[b]
+        blk = self.blocks[b]
         nrec = 0 if blk.receivers is None else len(blk.receivers)
         ns = C.c_int32()
         _lib.check(_lib.load().wql3d_get_seismograms(self.handle, b, None, C.byref(ns)), "wql3d_get_seismograms")
@@ -294,7 +333,7 @@ class Domain:
         return a[:ns.value, :nrec]
 
     def receiver_index(self, b: int = 0) -> np.ndarray:
-        blk = self.problem.blocks[b]
+        blk = self.blocks[b]
         n = 0 if blk.receivers is None else len(blk.receivers)
         a = np.zeros((max(n, 1), 3), dtype=np.int32)
         _lib.check(_lib.load().wql3d_receiver_index(self.handle, b, a.ctypes.data_as(_lib.ip)), "wql3d_receiver_index")
