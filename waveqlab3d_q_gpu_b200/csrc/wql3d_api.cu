@@ -443,6 +443,23 @@ int setup_block(wql3d_domain *d, int bi) {
   if (d->fp32) CK(M.get(&b.FC, 9 * vol));
   if (bd.mesh == WQL3D_MESH_CURVILINEAR) CK(M.get(&b.G, 18 * vol, false));
   if (bd.mesh == WQL3D_MESH_CURVILINEAR && d->response != 0) CK(M.get(&b.S6, 6 * vol, false));
+  if (bd.mesh == WQL3D_MESH_CURVILINEAR) {
+    // face-SAT buffers of the lean path: faces with a physical boundary condition
+    int off = 0;
+    for (int f = 0; f < 6; ++f) {
+      const int axis = f / 2;
+      const int fn = axis == 0 ? h.nr * h.ns : axis == 1 ? h.nq * h.ns : h.nq * h.nr;
+      b.foff[f] = off;
+      b.fsat[f] = nullptr;
+      b.fdq[f] = nullptr;
+      if (bd.bc[f] > 0) {
+        CK(M.get(&b.fsat[f], (size_t)9 * fn, false));
+        if (bd.pml[f] && bd.npml > 0) CK(M.get(&b.fdq[f], (size_t)9 * fn, false));
+        off += fn;
+      }
+    }
+    b.foff[6] = off;
+  }
   {
     // rates start at the reference's 1e40 sentinel (src/fields.f90:39) in FP64;
     // the first stage scales them by A(1) = 0.  FP32 cannot hold 1e40: zero.
@@ -835,6 +852,10 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
           case 3: launch_curv_anelastic<T, 3>(d, b, a, agr, ath); break;
           default: launch_curv_anelastic<T, 4>(d, b, a, agr, ath); break;
         }
+        d->launches++;
+      }
+      if ((a.flags & F_SAT) && b.foff[6] > 0) {
+        k_curv_face_sat<T><<<(b.foff[6] + 127) / 128, 128, 0, d->stream>>>(b, a.cur);
         d->launches++;
       }
       switch (tuning().curv_lb) {

@@ -111,6 +111,10 @@ struct Blk {
   const T *nrm[6];      // curvilinear face bases n_l(3) n_m(3) n_n(3), face-local
   // interface SAT vectors (q-min face: isat[0], q-max face: isat[1]), 9 x ny*nz
   T *isat[2];
+  // curvilinear lean path: face-SAT terms per face (tau0/h * structure(ubc) for
+  // the rates, tau0/h * ubc for the face's PML slab), face-local (see k_curv_face_sat)
+  T *fsat[6], *fdq[6];
+  int foff[7];          // face offsets of the concatenated face launch
   // sources
   int nsrc, src_order, src_alpha, src_half;
   const DevSource *src;
@@ -1098,6 +1102,21 @@ __device__ __forceinline__ T slab_damping(const Blk<T> &b, int x, int y, int z) 
   return b.d0 * fabs(v / (T)b.npml);
 }
 
+// face-local index of (x, y, z) on face F
+template <typename T, int F>
+__device__ __forceinline__ int face_index(const Blk<T> &b, int x, int y, int z) {
+  constexpr int axis = F >> 1;
+  return axis == 0 ? (y - 1) + b.ny * (z - 1) : axis == 1 ? (x - 1) + b.nx * (z - 1) : (x - 1) + b.nx * (y - 1);
+}
+
+template <typename T, int F>
+__device__ __forceinline__ bool on_face(const Blk<T> &b, int x, int y, int z) {
+  constexpr int axis = F >> 1;
+  const int i = axis == 0 ? x : axis == 1 ? y : z;
+  const int n = axis == 0 ? b.nx : axis == 1 ? b.ny : b.nz;
+  return (F & 1) ? i == n : i == 1;
+}
+
 // One PML slab per axis: the point lies in at most one of the axis's two
 // slabs (the host sends blocks whose two slabs on an axis overlap to the
 // generic update).  Only the membership is kept; the slab index, damping and
@@ -1121,8 +1140,8 @@ __device__ __forceinline__ AxisSlab axis_slab(const Blk<T> &b, int x, int y, int
 // the derivative scratch Gp), store DQ and integrate Q (integrate)
 template <typename T, int F>
 __device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int x, int y, int z, bool rhs,
-                                        bool integrate, const T *Gp, long long V, T rhoJ_inv, T lambda2mu, T lam,
-                                        T mu, T J, T df[9]) {
+                                        bool integrate, bool sat, const T *Gp, long long V, T rhoJ_inv,
+                                        T lambda2mu, T lam, T mu, T J, T df[9]) {
   constexpr int AX = F >> 1;
   const long long q = slab_index<T, F>(b, x, y, z);
   const long long PV = b.pvol[F];
@@ -1162,6 +1181,13 @@ __device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int
 #pragma unroll
     for (int c = 0; c < 9; ++c) DQ[c] = DQ[c] + src[c] - (d + cfs) * Q[c];
   }
+  if (sat && b.fdq[F] && on_face<T, F>(b, x, y, z)) {
+    // the face SAT's share of this slab (impose_boundary_condition, PML DQ)
+    const int fn = b.foff[F + 1] - b.foff[F];
+    const T *q = b.fdq[F] + face_index<T, F>(b, x, y, z);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) DQ[c] = DQ[c] - q[c * fn];
+  }
   const T Bdt = (T)a.Bdt;
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
@@ -1172,28 +1198,10 @@ __device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int
 
 template <typename T, int AX>
 __device__ __forceinline__ void slab_pass(const Blk<T> &b, const StageArgs &a, int x, int y, int z, AxisSlab s,
-                                          bool rhs, bool integrate, const T *Gp, long long V, T rhoJ_inv,
+                                          bool rhs, bool integrate, bool sat, const T *Gp, long long V, T rhoJ_inv,
                                           T lambda2mu, T lam, T mu, T J, T df[9]) {
-  if (s.hi) slab_do<T, 2 * AX + 1>(b, a, x, y, z, rhs, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-  else if (s.lo) slab_do<T, 2 * AX>(b, a, x, y, z, rhs, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-}
-
-// Q <- Q + B dt DQ for a slab whose DQ the face SAT changed after slab_pass
-template <typename T, int F>
-__device__ __forceinline__ void slab_int(const Blk<T> &b, const StageArgs &a, int x, int y, int z) {
-  const long long q = slab_index<T, F>(b, x, y, z);
-  const long long PV = b.pvol[F];
-  T *Qp = b.Q[F] + q;
-  const T *DQp = b.DQ[F] + q;
-  const T Bdt = (T)a.Bdt;
-#pragma unroll
-  for (int c = 0; c < 9; ++c) Qp[c * PV] = Qp[c * PV] + Bdt * DQp[c * PV];
-}
-
-template <typename T, int AX>
-__device__ __forceinline__ void slab_integrate(const Blk<T> &b, const StageArgs &a, int x, int y, int z, AxisSlab s) {
-  if (s.hi) slab_int<T, 2 * AX + 1>(b, a, x, y, z);
-  else if (s.lo) slab_int<T, 2 * AX>(b, a, x, y, z);
+  if (s.hi) slab_do<T, 2 * AX + 1>(b, a, x, y, z, rhs, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+  else if (s.lo) slab_do<T, 2 * AX>(b, a, x, y, z, rhs, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
 }
 
 // PML strain correction term d * Q[c] of the slab of one axis (0 outside)
@@ -1340,6 +1348,86 @@ __global__ void __launch_bounds__(128, MINB) k_curv_anelastic(Blk<T> b, StageArg
   }
 }
 
+// Face SATs of the curvilinear lean path (impose_boundary_condition,
+// src/RHS_Interior.f90:1584-1768, with BC_* and BCm/BCp of
+// src/BoundaryConditions.f90): one thread per point of every face with a
+// physical boundary condition; the terms the reference subtracts are stored
+// face-locally and k_curv_point subtracts them in the reference's face order.
+template <typename T>
+__global__ void __launch_bounds__(128) k_curv_face_sat(Blk<T> b, int cur) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= b.foff[6]) return;
+  int f = 0;
+#pragma unroll
+  for (int g = 1; g < 6; ++g)
+    if (j >= b.foff[g]) f = g;
+  const int k = j - b.foff[f];
+  const int axis = f >> 1, plus = f & 1;
+  const int d0 = axis == 0 ? b.ny : b.nx;
+  const int a1 = k / d0, a0 = k - a1 * d0;
+  const int fixed = plus ? (axis == 0 ? b.nx : axis == 1 ? b.ny : b.nz) : 1;
+  int x, y, z;
+  if (axis == 0) { x = fixed; y = a0 + 1; z = a1 + 1; }
+  else if (axis == 1) { x = a0 + 1; y = fixed; z = a1 + 1; }
+  else { x = a0 + 1; y = a1 + 1; z = fixed; }
+  const long long p = pidx(b, x, y, z);
+  const T *F = cur ? b.F1 : b.F0;
+  T u[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) u[c] = F[c * b.vol + p];
+  const T lam = b.M[p], mu = b.M[b.vol + p], rho = b.M[2 * b.vol + p];
+  const int type = b.bc[f];
+  const T r = type == 1 ? (T)0 : type == 2 ? (T)1 : (T)-1;
+  const T c_p = sqrt(((T)2 * mu + lam) / rho);
+  const T c_s = sqrt(mu / rho);
+  const T Zp = rho * c_p, Zs = rho * c_s;
+  const T qx = ld(b.met + (long long)(0 + axis) * b.vol + p);
+  const T qy = ld(b.met + (long long)(3 + axis) * b.vol + p);
+  const T qz = ld(b.met + (long long)(6 + axis) * b.vol + p);
+  const T norm = sqrt(qx * qx + qy * qy + qz * qz);
+  const int fn = b.foff[f + 1] - b.foff[f];
+  const T *B = b.nrm[f];
+  T l[3], m[3], n[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    l[c] = ld(B + (0 + c) * fn + k);
+    m[c] = ld(B + (3 + c) * fn + k);
+    n[c] = ld(B + (6 + c) * fn + k);
+  }
+  T ubc[9], Ux[9];
+  bc_vector<T>(plus, u, Zs, Zp, r, l, m, n, norm, ubc);
+  // structure(), src/RHS_Interior.f90:2267-2287
+  const T irho = (T)1 / rho;
+  Ux[0] = irho * ubc[0];
+  Ux[1] = irho * ubc[1];
+  Ux[2] = irho * ubc[2];
+  Ux[3] = ((T)2 * mu + lam) * ubc[3] + lam * (ubc[4] + ubc[5]);
+  Ux[4] = ((T)2 * mu + lam) * ubc[4] + lam * (ubc[3] + ubc[5]);
+  Ux[5] = ((T)2 * mu + lam) * ubc[5] + lam * (ubc[3] + ubc[4]);
+  Ux[6] = mu * ubc[6];
+  Ux[7] = mu * ubc[7];
+  Ux[8] = mu * ubc[8];
+  const T h = axis == 0 ? b.hq : axis == 1 ? b.hr : b.hs;
+  const T pen = b.tau0 / h;
+  T *o = b.fsat[f] + k;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) o[c * fn] = pen * Ux[c];
+  if (b.fdq[f]) {
+    T *q = b.fdq[f] + k;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) q[c * fn] = pen * ubc[c];
+  }
+}
+
+template <typename T, int F>
+__device__ __forceinline__ void face_sat_add(const Blk<T> &b, int x, int y, int z, T df[9]) {
+  if (!b.fsat[F] || !on_face<T, F>(b, x, y, z)) return;
+  const int fn = b.foff[F + 1] - b.foff[F];
+  const T *o = b.fsat[F] + face_index<T, F>(b, x, y, z);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) df[c] = df[c] - o[c * fn];
+}
+
 template <typename T, int RESP, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a) {
   int x, y, z;
@@ -1362,11 +1450,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     sz = axis_slab<T, 2>(b, x, y, z);
   }
   const bool in_pml = sx.in() || sy.in() || sz.in();
-  // a face point's SAT also changes DQ of its slab (add_face_sats), so its
-  // slabs are integrated after the SATs
   const bool face_pt = x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz;
-  const bool defer = in_pml && face_pt && (a.flags & F_SAT);
-  const bool integrate = (a.flags & F_UPDATE) && !defer;
+  const bool integrate = (a.flags & F_UPDATE) != 0;
+  const bool sat = (a.flags & F_SAT) != 0;
   const T *Gp = b.G + p;
   if (a.flags & F_RHS) {
     const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
@@ -1395,14 +1481,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     }
     // PML damping and auxiliary fields, reference slab order z, y, x
     if (in_pml) {
-      slab_pass<T, 2>(b, a, x, y, z, sz, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-      slab_pass<T, 1>(b, a, x, y, z, sy, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-      slab_pass<T, 0>(b, a, x, y, z, sx, true, integrate, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 2>(b, a, x, y, z, sz, true, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 1>(b, a, x, y, z, sy, true, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 0>(b, a, x, y, z, sx, true, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
     }
-  } else if (in_pml && (a.flags & (F_SCALE | F_UPDATE))) {
-    slab_pass<T, 2>(b, a, x, y, z, sz, false, integrate, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
-    slab_pass<T, 1>(b, a, x, y, z, sy, false, integrate, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
-    slab_pass<T, 0>(b, a, x, y, z, sx, false, integrate, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+  } else if (in_pml && (a.flags & (F_SCALE | F_UPDATE | F_SAT))) {
+    slab_pass<T, 2>(b, a, x, y, z, sz, false, integrate, sat, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 1>(b, a, x, y, z, sy, false, integrate, sat, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 0>(b, a, x, y, z, sx, false, integrate, sat, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
   }
   if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
       z >= b.sbox[4] && z <= b.sbox[5]) {
@@ -1410,11 +1496,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
     add_sources<T, MESH_CURV>(b, tst, x, y, z, p, df);
   }
-  if ((a.flags & F_SAT) && face_pt) add_face_sats<T, MESH_CURV, false>(b, F, x, y, z, p, df, in_pml, 0.0);
-  if (defer && (a.flags & F_UPDATE)) {
-    slab_integrate<T, 2>(b, a, x, y, z, sz);
-    slab_integrate<T, 1>(b, a, x, y, z, sy);
-    slab_integrate<T, 0>(b, a, x, y, z, sx);
+  if (sat && face_pt) {
+    // face SATs in the reference's order Lx, Rx, Ly, Ry, Lz, Rz
+    face_sat_add<T, 0>(b, x, y, z, df);
+    face_sat_add<T, 1>(b, x, y, z, df);
+    face_sat_add<T, 2>(b, x, y, z, df);
+    face_sat_add<T, 3>(b, x, y, z, df);
+    face_sat_add<T, 4>(b, x, y, z, df);
+    face_sat_add<T, 5>(b, x, y, z, df);
   }
   if (a.flags & F_ISAT) {
     // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
