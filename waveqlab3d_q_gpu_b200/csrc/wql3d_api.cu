@@ -727,7 +727,9 @@ struct Tuning {
   int generic = 0;   // 1: every point through the generic per-point kernel
   int split = 1;     // interior: two warp groups (velocity / stress rates) with register z-queues
   int lean = 1;      // curvilinear update: k_curv_point (0: generic point update k_curv_update)
-  int curv_lb = 0;   // k_curv_point threads x min blocks: 0 = 256x2, 1 = 128x3, 2 = 256x1
+  int curv_lb = -1;  // k_curv_point threads x min blocks: 0 = 256x2, 1 = 128x3, 2 = 256x1, 3 = 256x3,
+                     // 4 = 256x4; -1: 256x2 (FP64), 256x4 (FP32)
+  int grad_minb = 2; // k_curv_grad resident 256-thread blocks per SM (2, 3, 4)
   int grad_bx = 32;  // k_curv_grad tile width along x (32, 64)
   int an_minb = 3;   // k_curv_anelastic: resident 128-thread blocks per SM (3, 4 or 6)
 };
@@ -737,7 +739,8 @@ Tuning tuning() {
     Tuning r;
     if (const char *e = getenv("WQL3D_TY")) r.ty = atoi(e) == 8 ? 8 : 4;
     if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = std::max(1, atoi(e));
-    if (const char *e = getenv("WQL3D_CURV_LB")) r.curv_lb = std::min(2, std::max(0, atoi(e)));
+    if (const char *e = getenv("WQL3D_CURV_LB")) r.curv_lb = std::min(4, std::max(0, atoi(e)));
+    if (const char *e = getenv("WQL3D_GRAD_MINB")) r.grad_minb = atoi(e);
     if (const char *e = getenv("WQL3D_AN_MINB")) r.an_minb = atoi(e);
     if (const char *e = getenv("WQL3D_GRAD_BX")) r.grad_bx = atoi(e) == 64 ? 64 : 32;
     if (const char *e = getenv("WQL3D_KERNEL")) {
@@ -833,7 +836,11 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
     if (a.flags & F_RHS) {
       const int gbx = tuning().grad_bx, gby = 256 / gbx / 2;
       dim3 gth(gbx, gby, 2), ggr((b.nx + gbx - 1) / gbx, (b.ny + gby - 1) / gby, (b.nz + 1) / 2);
-      k_curv_grad<T><<<ggr, gth, 0, d->stream>>>(b, a.cur);
+      switch (tuning().grad_minb) {
+        case 3: k_curv_grad<T, 3><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+        case 4: k_curv_grad<T, 4><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+        default: k_curv_grad<T, 2><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+      }
       d->launches++;
     }
     // the lean kernel keeps one PML slab per axis: blocks whose two slabs on
@@ -858,9 +865,12 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
         k_curv_face_sat<T><<<(b.foff[6] + 127) / 128, 128, 0, d->stream>>>(b, a.cur);
         d->launches++;
       }
-      switch (tuning().curv_lb) {
+      const int lb = tuning().curv_lb >= 0 ? tuning().curv_lb : (sizeof(T) == 4 ? 4 : 0);
+      switch (lb) {
         case 1: launch_curv_point<T, 128, 3>(d, b, a); break;
         case 2: launch_curv_point<T, 256, 1>(d, b, a); break;
+        case 3: launch_curv_point<T, 256, 3>(d, b, a); break;
+        case 4: launch_curv_point<T, 256, 4>(d, b, a); break;
         default: launch_curv_point<T, 256, 2>(d, b, a); break;
       }
     } else {

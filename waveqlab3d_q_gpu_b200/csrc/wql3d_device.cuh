@@ -984,8 +984,8 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
 //   0-8   dv_x/dx, dv_y/dx, dv_z/dx, dv_x/dy, ..., dv_z/dz   (Ux, Uy, Uz 1:3)
 //   9-17  Ux4, Ux7, Ux8, Uy7, Uy5, Uy9, Uz8, Uz9, Uz6        (1-based JJU_x6 slots)
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(256, 2) k_curv_grad(Blk<T> b, int cur) {
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
