@@ -729,9 +729,10 @@ struct Tuning {
   int lean = 1;      // curvilinear update: k_curv_point (0: generic point update k_curv_update)
   int curv_lb = -1;  // k_curv_point threads x min blocks: 0 = 256x2, 1 = 128x3, 2 = 256x1, 3 = 256x3,
                      // 4 = 256x4; -1: 256x2 (FP64), 256x4 (FP32)
-  int grad_minb = 2; // k_curv_grad resident 256-thread blocks per SM (2, 3, 4)
-  int grad_bx = 32;  // k_curv_grad tile width along x (32, 64)
-  int an_minb = 3;   // k_curv_anelastic: resident 128-thread blocks per SM (3, 4 or 6)
+  int grad_minb = 2; // k_curv_grad resident 256-thread blocks per SM (2, 3; 4 with 3-D tiles)
+  int grad_bx = 32;  // k_curv_grad 3-D tile width along x (32, 64)
+  int grad_flat = 1; // k_curv_grad over a flattened point index (0: 3-D tiles)
+  int an_minb = 0;   // k_curv_anelastic: resident 128-thread blocks per SM (3, 4, 6, 8); 0: 3 (FP64), 8 (FP32)
 };
 
 Tuning tuning() {
@@ -743,6 +744,7 @@ Tuning tuning() {
     if (const char *e = getenv("WQL3D_GRAD_MINB")) r.grad_minb = atoi(e);
     if (const char *e = getenv("WQL3D_AN_MINB")) r.an_minb = atoi(e);
     if (const char *e = getenv("WQL3D_GRAD_BX")) r.grad_bx = atoi(e) == 64 ? 64 : 32;
+    if (const char *e = getenv("WQL3D_GRAD_FLAT")) r.grad_flat = atoi(e) != 0;
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
       if (strcmp(e, "ring") == 0) r.split = 0;
@@ -836,10 +838,19 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
     if (a.flags & F_RHS) {
       const int gbx = tuning().grad_bx, gby = 256 / gbx / 2;
       dim3 gth(gbx, gby, 2), ggr((b.nx + gbx - 1) / gbx, (b.ny + gby - 1) / gby, (b.nz + 1) / 2);
-      switch (tuning().grad_minb) {
-        case 3: k_curv_grad<T, 3><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
-        case 4: k_curv_grad<T, 4><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
-        default: k_curv_grad<T, 2><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+      if (tuning().grad_flat) {
+        const long long np = (long long)b.nx * b.ny * b.nz;
+        const unsigned fgr = (unsigned)((np + 255) / 256);
+        if (tuning().grad_minb == 3)
+          k_curv_grad<T, 3, 1><<<fgr, 256, 0, d->stream>>>(b, a.cur);
+        else
+          k_curv_grad<T, 2, 1><<<fgr, 256, 0, d->stream>>>(b, a.cur);
+      } else {
+        switch (tuning().grad_minb) {
+          case 3: k_curv_grad<T, 3, 0><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+          case 4: k_curv_grad<T, 4, 0><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+          default: k_curv_grad<T, 2, 0><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
+        }
       }
       d->launches++;
     }
@@ -854,10 +865,12 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
         // memory variables first: k_curv_point subtracts their sums
         const long long npts = (long long)b.nx * b.ny * b.nz;
         const unsigned ath = 128, agr = (unsigned)((npts + 127) / 128);
-        switch (tuning().an_minb) {
+        const int am = tuning().an_minb > 0 ? tuning().an_minb : (sizeof(T) == 4 ? 8 : 3);
+        switch (am) {
+          case 8: launch_curv_anelastic<T, 8>(d, b, a, agr, ath); break;
           case 6: launch_curv_anelastic<T, 6>(d, b, a, agr, ath); break;
-          case 3: launch_curv_anelastic<T, 3>(d, b, a, agr, ath); break;
-          default: launch_curv_anelastic<T, 4>(d, b, a, agr, ath); break;
+          case 4: launch_curv_anelastic<T, 4>(d, b, a, agr, ath); break;
+          default: launch_curv_anelastic<T, 3>(d, b, a, agr, ath); break;
         }
         d->launches++;
       }

@@ -984,12 +984,22 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
 //   0-8   dv_x/dx, dv_y/dx, dv_z/dx, dv_x/dy, ..., dv_z/dz   (Ux, Uy, Uz 1:3)
 //   9-17  Ux4, Ux7, Ux8, Uy7, Uy5, Uy9, Uz8, Uz9, Uz6        (1-based JJU_x6 slots)
 // ---------------------------------------------------------------------------
-template <typename T, int MINB>
+template <typename T>
+__device__ __forceinline__ bool flat_point(const Blk<T> &b, int &x, int &y, int &z);
+
+// FLAT: one thread per point of a flattened (x fastest) 1-D launch, every lane
+// busy; otherwise 3-D tiles of blockDim points.
+template <typename T, int MINB, int FLAT>
 __global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int z = blockIdx.z * blockDim.z + threadIdx.z + 1;
-  if (x > b.nx || y > b.ny || z > b.nz) return;
+  int x, y, z;
+  if (FLAT) {
+    if (!flat_point(b, x, y, z)) return;
+  } else {
+    x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (x > b.nx || y > b.ny || z > b.nz) return;
+  }
   const long long p = pidx(b, x, y, z);
   const long long V = b.vol;
   const T *F = cur ? b.F1 : b.F0;
@@ -1233,8 +1243,8 @@ __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs 
   T qs = 0, qp = 0;
   if (RESP != RESP_FQ8) { qs = ld(b.qs + p); qp = ld(b.qp + p); }
   const int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
-  T *ep = b.eta + p;
-  T *dp = b.deta + p;
+  T *__restrict__ ep = b.eta + p;
+  T *__restrict__ dp = b.deta + p;
   const T A = (T)a.A, Bdt = (T)a.Bdt;
   const T two_mu = (T)2 * mu, l2m = lam + (T)2 * mu;
   // per-point factors of the rates
