@@ -979,8 +979,9 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
 // form, src/JU_xJU_yJU_z6.f90:16177-16424, is the same operator with the
 // central row, summed in another order).  Per axis a with row coefficients
 // c_k: velocities X_r(p) * (1/h_a) sum_k c_k v(k), stresses
-// (1/h_a) sum_k ((c_k s(k)) J(k)) X_r(k) for the nine (stress, metric row)
-// pairs the rates need.  G holds, component-major with the field stride:
+// sum_k (s(k) ((c_k / h_a) J(k))) X_r(k) for the nine (stress, metric row)
+// pairs the rates need, summed over the three axes in one accumulator each
+// (the reference scales each axis sum by 1/h_a: rounding-level difference).  G holds, component-major with the field stride:
 //   0-8   dv_x/dx, dv_y/dx, dv_z/dx, dv_x/dy, ..., dv_z/dz   (Ux, Uy, Uz 1:3)
 //   9-17  Ux4, Ux7, Ux8, Uy7, Uy5, Uy9, Uz8, Uz9, Uz6        (1-based JJU_x6 slots)
 // ---------------------------------------------------------------------------
@@ -1013,23 +1014,23 @@ __global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
 #pragma unroll 1
   for (int ax = 0; ax < 3; ++ax) {
     T sv[3] = {0, 0, 0};
-    T acc[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) acc[k] = 0;
+    const T h = ih[ax];
     const T *X0 = b.met + (long long)(0 * 3 + ax) * V;
     const T *X1 = b.met + (long long)(1 * 3 + ax) * V;
     const T *X2 = b.met + (long long)(2 * 3 + ax) * V;
+    // stress fluxes straight into S with 1/h folded into the tap weight (no
+    // per-axis accumulators: registers go to loads in flight)
     auto tap = [&](long long q, T c) {
-      const T Jq = ld(b.J + q);
+      const T cJ = (h * c) * ld(b.J + q);
       const T x0 = ld(X0 + q), x1 = ld(X1 + q), x2 = ld(X2 + q);
 #pragma unroll
       for (int f = 0; f < 3; ++f) sv[f] = sv[f] + c * ld(F + f * V + q);
-      const T sxx = c * ld(F + 3 * V + q) * Jq, syy = c * ld(F + 4 * V + q) * Jq;
-      const T szz = c * ld(F + 5 * V + q) * Jq, sxy = c * ld(F + 6 * V + q) * Jq;
-      const T sxz = c * ld(F + 7 * V + q) * Jq, syz = c * ld(F + 8 * V + q) * Jq;
-      acc[0] = acc[0] + sxx * x0; acc[1] = acc[1] + sxy * x0; acc[2] = acc[2] + sxz * x0;
-      acc[3] = acc[3] + sxy * x1; acc[4] = acc[4] + syy * x1; acc[5] = acc[5] + syz * x1;
-      acc[6] = acc[6] + sxz * x2; acc[7] = acc[7] + syz * x2; acc[8] = acc[8] + szz * x2;
+      const T sxx = ld(F + 3 * V + q) * cJ, syy = ld(F + 4 * V + q) * cJ;
+      const T szz = ld(F + 5 * V + q) * cJ, sxy = ld(F + 6 * V + q) * cJ;
+      const T sxz = ld(F + 7 * V + q) * cJ, syz = ld(F + 8 * V + q) * cJ;
+      S[0] = S[0] + sxx * x0; S[1] = S[1] + sxy * x0; S[2] = S[2] + sxz * x0;
+      S[3] = S[3] + sxy * x1; S[4] = S[4] + syy * x1; S[5] = S[5] + syz * x1;
+      S[6] = S[6] + sxz * x2; S[7] = S[7] + syz * x2; S[8] = S[8] + szz * x2;
     };
     const int i = pos[ax], n = nn[ax];
     if (i >= 7 && i <= n - 6) {
@@ -1051,9 +1052,7 @@ __global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int f = 0; f < 3; ++f) U[r * 3 + f] = U[r * 3 + f] + ih[ax] * (xp[r] * sv[f]);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) S[k] = S[k] + ih[ax] * acc[k];
+      for (int f = 0; f < 3; ++f) U[r * 3 + f] = U[r * 3 + f] + h * (xp[r] * sv[f]);
   }
   T *Gp = b.G + p;
 #pragma unroll
