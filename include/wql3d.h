@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define WQL3D_ABI_VERSION 1
+#define WQL3D_ABI_VERSION 2
 
 /* status codes */
 #define WQL3D_OK 0
@@ -150,6 +150,19 @@ typedef struct wql3d_domain_desc {
      (its q-max face), 2 side 2 (its q-min face); the other side's face trace
      arrives through the interface buffers every stage */
   int32_t remote_side;
+  /* one s-slab of a block per process (the reference's spatial decomposition
+     with ghost-layer exchange, src/mpi3dcomm.f90:459-528, src/fields.f90:306-321):
+     with nblocks = 1 and slab_ns_global > 0, block 0 holds the global s-planes
+     slab_z0 + 1 .. slab_z0 + ns of a block of slab_ns_global planes (aqrs / bqrs
+     are the whole block's).  Its s faces inside the block are open: no boundary
+     condition or PML there, the central SBP row up to the face, and 3 ghost
+     planes per open face that wql3d_unpack_halo fills with the neighbour's
+     planes.  Curvilinear slabs pass in slab_ghost_coords the coordinates of the
+     3 planes below and the 3 above the slab, (3, 6, nr, nq) with q fastest
+     (the rows of a side that is a face of the whole block are ignored). */
+  int32_t slab_z0;
+  int32_t slab_ns_global;
+  const double *slab_ghost_coords;
   wql3d_block_desc block[2];
 } wql3d_domain_desc;
 
@@ -200,6 +213,23 @@ int wql3d_interface_buffers(wql3d_domain *d, void **send, void **recv, int64_t *
 int wql3d_pack_interface(wql3d_domain *d);
 int wql3d_get_interface_material(wql3d_domain *d, double *M);
 int wql3d_set_interface_remote_material(wql3d_domain *d, const double *M);
+
+/* ghost-plane exchange of an s-slab domain (slab_ns_global > 0;
+   src/mpi3dcomm.f90:459-528): device buffers of 2 faces x count elements of
+   elem_bytes (field precision), the lower face first, each face
+   ncomp x 3 planes x nr x nq with q fastest (ncomp 9 for WQL3D_HALO_FIELDS,
+   10 for WQL3D_HALO_METRIC).  wql3d_pack_halo fills send with the 3 planes
+   next to each open face; the caller moves send's lower face to the lower
+   neighbour's recv upper face and send's upper face to the upper neighbour's
+   recv lower face; wql3d_unpack_halo writes recv into the ghost planes.  The
+   metric (metricx, metricy, metricz, J) is exchanged once after
+   wql3d_domain_create; the fields before every wql3d_stage (after
+   wql3d_begin_step).  wql3d_time_step / wql3d_run are refused (WQL3D_ESTATE). */
+#define WQL3D_HALO_FIELDS 0
+#define WQL3D_HALO_METRIC 1
+int wql3d_halo_buffers(wql3d_domain *d, int kind, void **send, void **recv, int64_t *count, int32_t *elem_bytes);
+int wql3d_pack_halo(wql3d_domain *d, int kind);
+int wql3d_unpack_halo(wql3d_domain *d, int kind);
 
 /* split stage operations (bring-up path, same arithmetic as wql3d_stage) */
 int wql3d_scale_rates(wql3d_domain *d, double A);                         /* domain.f90:922-949 */

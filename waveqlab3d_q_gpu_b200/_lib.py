@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libwql3d.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 OK = 0
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENONFINITE", -5: "ESTATE"}
 
@@ -48,6 +48,7 @@ class DomainDesc(C.Structure):
         ("mms", C.c_int32), ("mms_nt", C.c_double), ("mms_nx", C.c_double), ("mms_ny", C.c_double),
         ("mms_nz", C.c_double),
         ("remote_side", C.c_int32),
+        ("slab_z0", C.c_int32), ("slab_ns_global", C.c_int32), ("slab_ghost_coords", dp),
         ("block", BlockDesc * 2),
     ]
 
@@ -73,6 +74,10 @@ SIGNATURES = {
     "wql3d_interface_buffers": [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int32)],
     "wql3d_pack_interface": [C.c_void_p],
+    "wql3d_halo_buffers": [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                           C.POINTER(C.c_int32)],
+    "wql3d_pack_halo": [C.c_void_p, C.c_int],
+    "wql3d_unpack_halo": [C.c_void_p, C.c_int],
     "wql3d_get_interface_material": [C.c_void_p, dp],
     "wql3d_set_interface_remote_material": [C.c_void_p, dp],
     "wql3d_scale_rates": [C.c_void_p, C.c_double],

@@ -162,6 +162,9 @@ struct wql3d_domain {
   int64_t launches = 0;
   double *red = nullptr;
   int *flag = nullptr;
+  // s-slab ghost-plane exchange buffers (2 faces x up to 10 x 3 x nr x nq)
+  bool slab = false;
+  void *halo_send = nullptr, *halo_recv = nullptr;
 };
 
 namespace {
@@ -258,11 +261,12 @@ __global__ void k_metrics(Blk<T> b, const double *X, double *met, double *Jout) 
   const int pos[3] = {q, r, s};
   const int nn[3] = {b.nx, b.ny, b.nz};
   const long long st[3] = {1, b.sy, b.sz};
+  const int ng[3] = {b.nx, b.ny, b.nzg};
   double D[3][3];  // D[axis][comp]
   for (int a = 0; a < 3; ++a) {
     Row row;
-    sbp_row(pos[a], nn[a], b.lit, row);
-    double h = 1.0 / (double)(nn[a] - 1);
+    sbp_row(pos[a], nn[a], b.lit, row, b.open_lo[a], b.open_hi[a]);
+    double h = 1.0 / (double)(ng[a] - 1);
     for (int c = 0; c < 3; ++c) {
       double sum = 0.0;
       for (int k = 0; k < row.cnt; ++k) sum = __dadd_rn(sum, __dmul_rn(row.c[k], X[c * V + p + row.off[k] * st[a]]));
@@ -390,17 +394,24 @@ int setup_block(wql3d_domain *d, int bi) {
   b.o1 = h.XOFF + b.sy * NB + b.sz * NB;
   b.vol = vol;
   b.lit = bd.f32_literal ? 1 : 0;
+  // an s-slab of a larger block: global plane offset z0, nsg planes in all
+  const bool slab = d->slab;
+  const int z0 = slab ? d->desc.slab_z0 : 0;
+  const int nsg = slab ? d->desc.slab_ns_global : h.ns;
+  b.open_lo[2] = slab && z0 > 0 ? 1 : 0;
+  b.open_hi[2] = slab && z0 + h.ns < nsg ? 1 : 0;
+  b.nzg = nsg;
   b.hq = (T)(1.0 / (double)(h.nq - 1));
   b.hr = (T)(1.0 / (double)(h.nr - 1));
-  b.hs = (T)(1.0 / (double)(h.ns - 1));
+  b.hs = (T)(1.0 / (double)(nsg - 1));
   b.ihq = (T)(1.0 / (1.0 / (double)(h.nq - 1)));
   b.ihr = (T)(1.0 / (1.0 / (double)(h.nr - 1)));
-  b.ihs = (T)(1.0 / (1.0 / (double)(h.ns - 1)));
+  b.ihs = (T)(1.0 / (1.0 / (double)(nsg - 1)));
   const double cc[3] = {0.75, -0.15, 1.0 / 60.0};
   for (int s = 0; s < 3; ++s) {
     b.cx[s] = (T)(cc[s] / (1.0 / (double)(h.nq - 1)));
     b.cy[s] = (T)(cc[s] / (1.0 / (double)(h.nr - 1)));
-    b.cz[s] = (T)(cc[s] / (1.0 / (double)(h.ns - 1)));
+    b.cz[s] = (T)(cc[s] / (1.0 / (double)(nsg - 1)));
   }
   b.tau0 = (T)bd.tau0;
   for (int f = 0; f < 6; ++f) b.bc[f] = bd.bc[f];
@@ -431,6 +442,8 @@ int setup_block(wql3d_domain *d, int bi) {
   int ix = bd.pml[0] ? std::max(np, 6) : 6, fx = bd.pml[1] ? std::max(np, 6) : 6;
   int iy = bd.pml[2] ? std::max(np, 6) : 6, fy = bd.pml[3] ? std::max(np, 6) : 6;
   int iz = bd.pml[4] ? std::max(np, 6) : 6, fz = bd.pml[5] ? std::max(np, 6) : 6;
+  if (b.open_lo[2]) iz = 0;   // open faces: the central row reaches the face
+  if (b.open_hi[2]) fz = 0;
   b.lo[0] = ix + 1; b.hi[0] = h.nq - fx;
   b.lo[1] = iy + 1; b.hi[1] = h.nr - fy;
   b.lo[2] = iz + 1; b.hi[2] = h.ns - fz;
@@ -478,11 +491,12 @@ int setup_block(wql3d_domain *d, int bi) {
   if (rc) return rc;
 
   // coordinates (host copy for lookups)
+  std::vector<double> ghost;   // s-slab: coordinates of the 3 planes beyond each side, (3, 6, nr, nq)
   long long n1 = (long long)h.nq * h.nr * h.ns;
   h.coords.assign((size_t)(3 * n1), 0.0);
   if (bd.mesh == WQL3D_MESH_CARTESIAN) {
     double bh[3];
-    int nn[3] = {h.nq, h.nr, h.ns};
+    int nn[3] = {h.nq, h.nr, nsg};
     for (int c = 0; c < 3; ++c) bh[c] = (bd.bqrs[c] - bd.aqrs[c]) / (double)(nn[c] - 1);
     for (int z = 1; z <= h.ns; ++z)
       for (int y = 1; y <= h.nr; ++y)
@@ -490,18 +504,35 @@ int setup_block(wql3d_domain *d, int bi) {
           long long i = (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1));
           h.coords[i] = bd.aqrs[0] + (double)(x - 1) * bh[0];
           h.coords[n1 + i] = bd.aqrs[1] + (double)(y - 1) * bh[1];
-          h.coords[2 * n1 + i] = bd.aqrs[2] + (double)(z - 1) * bh[2];
+          h.coords[2 * n1 + i] = bd.aqrs[2] + (double)(z0 + z - 1) * bh[2];
         }
+    if (slab) {
+      // the 3 planes below and above the slab, for the metric's central rows
+      const long long pl = (long long)h.nq * h.nr;
+      ghost.assign((size_t)(3 * 6 * pl), 0.0);
+      for (int k = 0; k < 6; ++k) {
+        const int zg = k < 3 ? z0 - 2 + k : z0 + h.ns + 1 + (k - 3);
+        for (int y = 1; y <= h.nr; ++y)
+          for (int x = 1; x <= h.nq; ++x) {
+            long long i = (x - 1) + (long long)h.nq * (y - 1) + pl * k;
+            ghost[i] = bd.aqrs[0] + (double)(x - 1) * bh[0];
+            ghost[6 * pl + i] = bd.aqrs[1] + (double)(y - 1) * bh[1];
+            ghost[12 * pl + i] = bd.aqrs[2] + (double)(zg - 1) * bh[2];
+          }
+      }
+    }
     // per-axis metric of the separable Cartesian mesh: 1 / (D6 x)(i), with
     // the SBP operator applied to the coordinate line exactly as
     // src/grid.f90:398-471 does (row-4 literal included)
     for (int a = 0; a < 3; ++a) {
-      std::vector<T> m((size_t)nn[a] + 1, (T)0);
+      const int off = a == 2 ? z0 : 0;   // global index of the slab's planes
+      const int nl = a == 0 ? h.nq : a == 1 ? h.nr : h.ns;
+      std::vector<T> m((size_t)nl + 1, (T)0);
       double hh = 1.0 / (double)(nn[a] - 1);
-      for (int i = 1; i <= nn[a]; ++i) {
+      for (int i = 1; i <= nl; ++i) {
         int cnt, idx[8];
         double c[8];
-        host_row(i, nn[a], b.lit, cnt, idx, c);
+        host_row(i + off, nn[a], b.lit, cnt, idx, c);
         double s = 0.0;
         for (int k = 0; k < cnt; ++k) s = s + c[k] * (bd.aqrs[a] + (double)(idx[k] - 1) * bh[a]);
         double Xa = (1.0 / hh) * s;
@@ -522,6 +553,10 @@ int setup_block(wql3d_domain *d, int bi) {
             long long hi = (x - 1 + H) + (long long)(h.nq + 2 * H) * ((y - 1 + H) + (long long)(h.nr + 2 * H) * (z - 1 + H));
             h.coords[c * n1 + (x - 1) + (long long)h.nq * ((y - 1) + (long long)h.nr * (z - 1))] = bd.coords[c * hn + hi];
           }
+    if (slab && (b.open_lo[2] || b.open_hi[2])) {
+      if (!d->desc.slab_ghost_coords) return fail(WQL3D_EINVAL, "curvilinear slab needs slab_ghost_coords");
+      ghost.assign(d->desc.slab_ghost_coords, d->desc.slab_ghost_coords + (size_t)3 * 6 * h.nq * h.nr);
+    }
   }
   {
     // full metric and Jacobian of both mesh kinds from the coordinates
@@ -532,6 +567,25 @@ int setup_block(wql3d_domain *d, int bi) {
     CK(M.get(&Jd, vol));
     rc = put_array<double>(d, h, Xd, 3, h.coords.data(), 0);
     if (rc) return rc;
+    if (!ghost.empty()) {
+      // ghost planes of the open sides (device planes -2..0 and ns+1..ns+3)
+      for (int side = 0; side < 2; ++side) {
+        if (!(side ? b.open_hi[2] : b.open_lo[2])) continue;
+        for (int c = 0; c < 3; ++c) {
+          cudaMemcpy3DParms q;
+          memset(&q, 0, sizeof(q));
+          q.srcPtr = make_cudaPitchedPtr((void *)(ghost.data() + (size_t)c * 6 * h.nq * h.nr), (size_t)h.nq * sizeof(double),
+                                         h.nq, h.nr);
+          q.srcPos = make_cudaPos(0, 0, side ? 3 : 0);
+          q.dstPtr = make_cudaPitchedPtr((void *)(Xd + (long long)c * vol), (size_t)h.PX * sizeof(double), h.PX, h.PY);
+          q.dstPos = make_cudaPos((size_t)h.XOFF * sizeof(double), NB, side ? NB + h.ns : 0);
+          q.extent = make_cudaExtent((size_t)h.nq * sizeof(double), h.nr, 3);
+          q.kind = cudaMemcpyHostToDevice;
+          CK(cudaMemcpy3DAsync(&q, d->stream));
+        }
+      }
+      CK(cudaStreamSynchronize(d->stream));
+    }
     b.X = Xd;
     b.mms = d->desc.mms ? 1 : 0;
     if (b.mms) {
@@ -1037,6 +1091,21 @@ wql3d_domain *checked(wql3d_domain *d) { return d; }
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// ghost-plane pack / unpack of an s-slab domain on its stream
+template <typename T>
+int halo_launch(wql3d_domain *d, Blk<T> &b, int kind, int unpack) {
+  T *buf = (T *)(unpack ? d->halo_recv : d->halo_send);
+  const int ncomp = kind == WQL3D_HALO_FIELDS ? 9 : 10;
+  T *a0 = kind == WQL3D_HALO_FIELDS ? (d->cur ? b.F1 : b.F0) : const_cast<T *>(b.met);
+  T *a1 = kind == WQL3D_HALO_FIELDS ? a0 : const_cast<T *>(b.J);
+  const int n0 = 9;
+  const long long n = (long long)2 * ncomp * 3 * b.nx * b.ny;
+  k_halo<T><<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(b, buf, a0, n0, a1, ncomp, unpack);
+  d->launches++;
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
 extern "C" {
 
 const char *wql3d_last_error(void) { return g_err.c_str(); }
@@ -1077,6 +1146,25 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     return cleanup(fail(WQL3D_ECUDA, "time init"));
   if (d->mem.get(&d->red, 592) != cudaSuccess || d->mem.get(&d->flag, 1) != cudaSuccess)
     return cleanup(fail(WQL3D_ENOMEM, "reduction scratch"));
+  if (desc->slab_ns_global > 0) {
+    // one s-slab of a larger block: open faces carry no boundary condition or PML
+    const wql3d_block_desc &b0 = desc->block[0];
+    if (desc->nblocks != 1 || desc->remote_side != 0 || desc->mms)
+      return cleanup(fail(WQL3D_EINVAL, "an s-slab domain holds one block without interface or MMS"));
+    if (desc->slab_z0 < 0 || desc->slab_z0 + b0.ns > desc->slab_ns_global)
+      return cleanup(fail(WQL3D_EINVAL, "slab planes outside the block"));
+    d->slab = true;
+    if (desc->slab_z0 > 0) { d->desc.block[0].bc[4] = 0; d->desc.block[0].pml[4] = 0; }
+    if (desc->slab_z0 + b0.ns < desc->slab_ns_global) { d->desc.block[0].bc[5] = 0; d->desc.block[0].pml[5] = 0; }
+    for (int f = 4; f < 6; ++f)
+      if (d->desc.block[0].pml[f] && b0.npml > b0.ns)
+        return cleanup(fail(WQL3D_EINVAL, "an s-face PML slab must lie inside one slab"));
+    const size_t hn = (size_t)2 * 10 * 3 * b0.nq * b0.nr;
+    const size_t eb = d->fp32 ? sizeof(float) : sizeof(double);
+    if (d->mem.get((char **)&d->halo_send, hn * eb) != cudaSuccess ||
+        d->mem.get((char **)&d->halo_recv, hn * eb) != cudaSuccess)
+      return cleanup(fail(WQL3D_ENOMEM, "halo buffers"));
+  }
   for (int i = 0; i < d->nblocks; ++i) {
     rc = d->fp32 ? setup_block<float>(d, i) : setup_block<double>(d, i);
     if (rc) return cleanup(rc);
@@ -1290,6 +1378,29 @@ int wql3d_pack_interface(wql3d_domain *d) {
   return WQL3D_OK;
 }
 
+int wql3d_halo_buffers(wql3d_domain *d, int kind, void **send, void **recv, int64_t *count, int32_t *elem_bytes) {
+  if (!d || !d->slab) return fail(WQL3D_EINVAL, "not an s-slab domain");
+  if (kind != WQL3D_HALO_FIELDS && kind != WQL3D_HALO_METRIC) return fail(WQL3D_EINVAL, "halo kind");
+  const int ncomp = kind == WQL3D_HALO_FIELDS ? 9 : 10;
+  if (send) *send = d->halo_send;
+  if (recv) *recv = d->halo_recv;
+  if (count) *count = (int64_t)ncomp * 3 * d->hb[0].nq * d->hb[0].nr;
+  if (elem_bytes) *elem_bytes = d->fp32 ? 4 : 8;
+  return WQL3D_OK;
+}
+
+int wql3d_pack_halo(wql3d_domain *d, int kind) {
+  if (!d || !d->slab) return fail(WQL3D_EINVAL, "not an s-slab domain");
+  if (kind != WQL3D_HALO_FIELDS && kind != WQL3D_HALO_METRIC) return fail(WQL3D_EINVAL, "halo kind");
+  return d->fp32 ? halo_launch<float>(d, d->bf[0], kind, 0) : halo_launch<double>(d, d->bd[0], kind, 0);
+}
+
+int wql3d_unpack_halo(wql3d_domain *d, int kind) {
+  if (!d || !d->slab) return fail(WQL3D_EINVAL, "not an s-slab domain");
+  if (kind != WQL3D_HALO_FIELDS && kind != WQL3D_HALO_METRIC) return fail(WQL3D_EINVAL, "halo kind");
+  return d->fp32 ? halo_launch<float>(d, d->bf[0], kind, 1) : halo_launch<double>(d, d->bd[0], kind, 1);
+}
+
 int wql3d_get_interface_material(wql3d_domain *d, double *M) {
   if (!d || !d->has_iface || !d->iface.remote || !M) return fail(WQL3D_EINVAL, "no remote interface side");
   const int n = d->iface.ny * d->iface.nz;
@@ -1327,6 +1438,8 @@ int wql3d_time_step(wql3d_domain *d, double dt, int n, int w_stride) {
   if (!d) return fail(WQL3D_EINVAL, "null domain");
   if (d->has_iface && d->iface.remote)
     return fail(WQL3D_ESTATE, "remote interface side: drive with wql3d_begin_step / pack / exchange / wql3d_stage");
+  if (d->slab)
+    return fail(WQL3D_ESTATE, "s-slab domain: drive with wql3d_begin_step / halo pack / exchange / unpack / wql3d_stage");
   DevTime h;
   CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
@@ -1342,6 +1455,8 @@ int wql3d_run(wql3d_domain *d, double dt, int n_first, int nsteps, int w_stride)
   if (!d) return fail(WQL3D_EINVAL, "null domain");
   if (d->has_iface && d->iface.remote)
     return fail(WQL3D_ESTATE, "remote interface side: drive with wql3d_begin_step / pack / exchange / wql3d_stage");
+  if (d->slab)
+    return fail(WQL3D_ESTATE, "s-slab domain: drive with wql3d_begin_step / halo pack / exchange / unpack / wql3d_stage");
   if (nsteps < 0) return fail(WQL3D_EINVAL, "nsteps");
   DevTime h;
   CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));

@@ -91,6 +91,10 @@ struct Blk {
   int sep;              // Cartesian block whose metric is diagonal to roundoff (separable shell)
   const double *rowc;   // closure rows 0..11 (left 1..6, right n..n-5): 8 signed coefficients each
   const int *rowo;      // matching tap offsets relative to the point
+  // open faces of an s-slab of a larger block (ghost planes hold the
+  // neighbour's data): the central row applies up to the face on that axis
+  int open_lo[3], open_hi[3];
+  int nzg;              // s-planes of the whole block (nz unless a slab)
   // PML slabs (faces 0..5): box and Q / DQ (9 components each, slab-local)
   int npml;
   int pml_on[6];
@@ -142,6 +146,13 @@ __device__ __forceinline__ long long pidx(const Blk<T> &b, int x, int y, int z) 
 template <typename T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
 
+// central (interior) SBP row at 1-based i of n points on axis a: 7 <= i <= n-6,
+// or up to an open face of a slab
+template <typename T>
+__device__ __forceinline__ bool central_row(const Blk<T> &b, int a, int i, int n) {
+  return (i >= 7 || b.open_lo[a]) && (i <= n - 6 || b.open_hi[a]);
+}
+
 // ---------------------------------------------------------------------------
 // SBP stencil row at 1-based index i of an axis with n points: taps as
 // relative offsets and signed coefficients, in the reference's summation
@@ -154,8 +165,8 @@ struct Row {
   double c[8];
 };
 
-__device__ __forceinline__ void sbp_row(int i, int n, int lit, Row &r) {
-  if (i >= 7 && i <= n - 6) {
+__device__ __forceinline__ void sbp_row(int i, int n, int lit, Row &r, bool open_lo = false, bool open_hi = false) {
+  if ((i >= 7 || open_lo) && (i <= n - 6 || open_hi)) {
     r.cnt = 6;
     r.off[0] = -3; r.off[1] = -2; r.off[2] = -1; r.off[3] = 1; r.off[4] = 2; r.off[5] = 3;
     r.c[0] = -1.0 / 60.0; r.c[1] = 0.15; r.c[2] = -0.75; r.c[3] = 0.75; r.c[4] = -0.15; r.c[5] = 1.0 / 60.0;
@@ -592,7 +603,7 @@ __device__ void jju6_row(const Blk<T> &b, const T *F, int x, int y, int z, long 
   for (int f = 0; f < 9; ++f) Ju[f] = 0;
   for (int a = 0; a < 3; ++a) {
     Row r;
-    sbp_row(pos[a], nn[a], b.lit, r);
+    sbp_row(pos[a], nn[a], b.lit, r, b.open_lo[a], b.open_hi[a]);
     const T *X = b.met + (long long)(mrow * 3 + a) * b.vol;
     T sv[3] = {0, 0, 0};
     T ss[6] = {0, 0, 0, 0, 0, 0};
@@ -656,7 +667,7 @@ __device__ void jju6_all(const Blk<T> &b, const T *F, int x, int y, int z, long 
 #pragma unroll
       for (int f = 0; f < 6; ++f) acc[r][f] = 0;
     const int i = pos[a], n = nn[a];
-    if (i >= 7 && i <= n - 6) {
+    if (central_row(b, a, i, n)) {
       const T cc[6] = {(T)(-1.0 / 60.0), (T)0.15, (T)-0.75, (T)0.75, (T)-0.15, (T)(1.0 / 60.0)};
       const int off[6] = {-3, -2, -1, 1, 2, 3};
 #pragma unroll
@@ -687,11 +698,12 @@ __device__ void jju6_all(const Blk<T> &b, const T *F, int x, int y, int z, long 
 // is diagonal to roundoff, J*X_a is constant along the axis, so this equals
 // JJU_x6's conservative form divided by J (src/JU_xJU_yJU_z6.f90:12-809).
 template <typename T>
-__device__ void sep_axis(const Blk<T> &b, const T *F, int i, int n, long long p, long long stride, T m, T ih, T U[9]) {
+__device__ void sep_axis(const Blk<T> &b, const T *F, int a, int i, int n, long long p, long long stride, T m, T ih,
+                         T U[9]) {
   T s[9];
 #pragma unroll
   for (int f = 0; f < 9; ++f) s[f] = 0;
-  if (i >= 7 && i <= n - 6) {
+  if (central_row(b, a, i, n)) {
     const T cc[6] = {(T)(-1.0 / 60.0), (T)0.15, (T)-0.75, (T)0.75, (T)-0.15, (T)(1.0 / 60.0)};
     const int off[6] = {-3, -2, -1, 1, 2, 3};
 #pragma unroll
@@ -852,9 +864,9 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
       J = ld(b.J + p);
       rhoJ_inv = (T)1 / (rho * J);
     } else if (SEP) {
-      sep_axis<T>(b, F, x, b.nx, p, 1, ld(b.mq + x), b.ihq, Ux);
-      sep_axis<T>(b, F, y, b.ny, p, b.sy, ld(b.mr + y), b.ihr, Uy);
-      sep_axis<T>(b, F, z, b.nz, p, b.sz, ld(b.ms + z), b.ihs, Uz);
+      sep_axis<T>(b, F, 0, x, b.nx, p, 1, ld(b.mq + x), b.ihq, Ux);
+      sep_axis<T>(b, F, 1, y, b.ny, p, b.sy, ld(b.mr + y), b.ihr, Uy);
+      sep_axis<T>(b, F, 2, z, b.nz, p, b.sz, ld(b.ms + z), b.ihs, Uz);
       J = (T)1;
       rhoJ_inv = (T)1 / rho;
     } else {
@@ -1033,7 +1045,7 @@ __global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
       S[6] = S[6] + sxz * x2; S[7] = S[7] + syz * x2; S[8] = S[8] + szz * x2;
     };
     const int i = pos[ax], n = nn[ax];
-    if (i >= 7 && i <= n - 6) {
+    if (central_row(b, ax, i, n)) {
       const T cc[6] = {(T)(-1.0 / 60.0), (T)0.15, (T)-0.75, (T)0.75, (T)-0.15, (T)(1.0 / 60.0)};
       const int off[6] = {-3, -2, -1, 1, 2, 3};
 #pragma unroll
@@ -1355,6 +1367,32 @@ __global__ void __launch_bounds__(128, MINB) k_curv_anelastic(Blk<T> b, StageArg
 #pragma unroll
     for (int c = 0; c < 6; ++c) b.S6[c * V + p] = s[3 + c];
   }
+}
+
+// Ghost planes of an s-slab (src/mpi3dcomm.f90:459-528): pack the 3 planes
+// next to each open face into buf (lower face first; each face ncomp x 3 x
+// ny x nx, x fastest), or unpack buf into the 3 ghost planes beyond each open
+// face.  Components c < n0 live at a0 + c * vol, the rest at a1.
+template <typename T>
+__global__ void k_halo(Blk<T> b, T *buf, T *a0, int n0, T *a1, int ncomp, int unpack) {
+  const long long plane = (long long)b.nx * b.ny;
+  const long long face = (long long)ncomp * 3 * plane;
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= 2 * face) return;
+  const int hi = j >= face;
+  if (hi ? !b.open_hi[2] : !b.open_lo[2]) return;
+  long long r = j - hi * face;
+  const int c = (int)(r / (3 * plane));
+  r -= (long long)c * 3 * plane;
+  const int k = (int)(r / plane);
+  r -= (long long)k * plane;
+  const int y = (int)(r / b.nx) + 1;
+  const int x = (int)(r - (long long)(y - 1) * b.nx) + 1;
+  const int z = unpack ? (hi ? b.nz + 1 + k : k - 2) : (hi ? b.nz - 2 + k : 1 + k);
+  T *a = c < n0 ? a0 + (long long)c * b.vol : a1 + (long long)(c - n0) * b.vol;
+  const long long p = pidx(b, x, y, z);
+  if (unpack) a[p] = buf[j];
+  else buf[j] = a[p];
 }
 
 // Face SATs of the curvilinear lean path (impose_boundary_condition,

@@ -1,4 +1,4 @@
-"""One block per process for two-block problems.
+"""One block (or one s-slab of a block) per process.
 
 The reference runs a two-block problem with one MPI rank per block and
 exchanges the interface face every RK stage (exchange_fields_interface and
@@ -122,6 +122,104 @@ class BlockRank:
         """Release the exchange buffers while the domain's stream exists (torch
         records an event on it when a pinned buffer used there is freed), then
         the domain."""
+        import gc
+
+        import torch
+        self.domain.synchronize()
+        self.xch = None
+        gc.collect()
+        torch.cuda.synchronize()
+        self.domain.close()
+
+
+def swap_faces(send, recv, count: int, rank: int, nranks: int):
+    """Ghost-plane swap of s-slab ``rank``: the lower face of ``send`` goes to
+    rank - 1, whose upper face arrives in the lower face of ``recv``, and the
+    upper face to rank + 1 (buffers [lower face | upper face] of ``count``
+    elements each)."""
+    import torch.distributed as dist
+    c = count
+    ops = []
+    if rank > 0:
+        ops += [dist.P2POp(dist.isend, send[0:c], rank - 1), dist.P2POp(dist.irecv, recv[0:c], rank - 1)]
+    if rank < nranks - 1:
+        ops += [dist.P2POp(dist.isend, send[c:2 * c], rank + 1), dist.P2POp(dist.irecv, recv[c:2 * c], rank + 1)]
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+
+
+class HaloExchange:
+    """The per-stage ghost-plane swap of one s-slab process with its lower
+    (rank - 1) and upper (rank + 1) neighbours; buffers are [lower face |
+    upper face] (wql3d_halo_buffers)."""
+
+    def __init__(self, domain, rank: int, nranks: int, backend: str, kind: int):
+        import torch
+        self.domain, self.rank, self.nranks, self.backend, self.kind = domain, rank, nranks, backend, kind
+        snd, rcv, count, eb = domain.halo_buffers(kind)
+        self.count = count
+        dtype = torch.float64 if eb == 8 else torch.float32
+        self.send = torch.as_tensor(_DeviceArray(snd, 2 * count, eb), device="cuda")
+        self.recv = torch.as_tensor(_DeviceArray(rcv, 2 * count, eb), device="cuda")
+        self.stream = torch.cuda.ExternalStream(domain.stream_handle())
+        if backend == "gloo":
+            self.hsend = torch.empty(2 * count, dtype=dtype, pin_memory=True)
+            self.hrecv = torch.empty(2 * count, dtype=dtype, pin_memory=True)
+
+    def _swap(self, send, recv):
+        swap_faces(send, recv, self.count, self.rank, self.nranks)
+
+    def exchange(self):
+        import torch
+        d = self.domain
+        d.pack_halo(self.kind)
+        if self.backend == "nccl":
+            with torch.cuda.stream(self.stream):
+                self._swap(self.send, self.recv)
+        else:
+            with torch.cuda.stream(self.stream):
+                self.hsend.copy_(self.send, non_blocking=True)
+            self.stream.synchronize()
+            self._swap(self.hsend, self.hrecv)
+            with torch.cuda.stream(self.stream):
+                self.recv.copy_(self.hrecv, non_blocking=True)
+        d.unpack_halo(self.kind)
+
+
+def slab_step(domain, xch, n: int, dt: float):
+    """Time step n of an s-slab domain: the stage-1 receiver sample, then per
+    RK stage the ghost-plane exchange and the stage."""
+    domain.begin_step(n)
+    for s in range(1, 6):
+        xch.exchange()
+        domain.stage(s, dt)
+
+
+class SlabRank:
+    """s-slab ``rank`` of ``nranks`` of a one-block problem on this process
+    (one slab per GPU, torch.distributed for the ghost planes)."""
+
+    def __init__(self, problem, rank: int, nranks: int, backend: str = "nccl", precision: str = "fp64",
+                 nsteps_hint: Optional[int] = None, cuts=None):
+        from .domain import Domain
+        from .slabs import HALO_FIELDS, HALO_METRIC, split_s
+        self.rank, self.nranks = rank, nranks
+        self.part = split_s(problem, nranks, cuts)[rank]
+        self.domain = Domain(self.part.problem, precision=precision, nsteps_hint=nsteps_hint, slab=self.part)
+        HaloExchange(self.domain, rank, nranks, backend, HALO_METRIC).exchange()
+        self.xch = HaloExchange(self.domain, rank, nranks, backend, HALO_FIELDS)
+        self.n = 1
+
+    def step(self):
+        slab_step(self.domain, self.xch, self.n, self.domain.dt)
+        self.n += 1
+
+    def run(self, nsteps: int):
+        for _ in range(nsteps):
+            self.step()
+
+    def close(self):
         import gc
 
         import torch

@@ -59,10 +59,13 @@ class Domain:
     """One or two blocks resident on the current CUDA device."""
 
     def __init__(self, problem: Problem, precision: str = "fp64", max_samples: Optional[int] = None,
-                 nsteps_hint: Optional[int] = None, remote_block: Optional[int] = None):
+                 nsteps_hint: Optional[int] = None, remote_block: Optional[int] = None, slab=None):
         """``remote_block`` = r holds only block r of a two-block problem; the
         other block lives in another process and the interface face is
-        exchanged every stage (see :mod:`waveqlab3d_q_gpu_b200.distributed`)."""
+        exchanged every stage (see :mod:`waveqlab3d_q_gpu_b200.distributed`).
+        ``slab`` (a :class:`waveqlab3d_q_gpu_b200.slabs.SlabPart`) makes this
+        domain one s-slab of a larger block whose ghost planes are exchanged
+        every stage (see :mod:`waveqlab3d_q_gpu_b200.slabs`)."""
         from . import anelastic as an
 
         L = _lib.load()
@@ -119,6 +122,14 @@ class Domain:
             nt = nsteps_hint if nsteps_hint is not None else problem.nt()
             max_samples = max(1, (nt + max(problem.w_stride, 1) - 1) // max(problem.w_stride, 1) + 1)
         d.max_samples = int(max_samples)
+        self.slab = slab
+        if slab is not None:
+            d.slab_z0 = int(slab.z0)
+            d.slab_ns_global = int(slab.ns_global)
+            if slab.ghost_coords is not None:
+                gc = np.ascontiguousarray(slab.ghost_coords, dtype=np.float64)
+                self._keep.append(gc)
+                d.slab_ghost_coords = _ptr(gc)
         if problem.mms is not None:
             d.mms = 1
             d.mms_nt, d.mms_nx, d.mms_ny, d.mms_nz = problem.mms.nt, problem.mms.nx, problem.mms.ny, problem.mms.nz
@@ -167,7 +178,7 @@ class Domain:
         _lib.check(L.wql3d_domain_create(C.byref(d), C.byref(h)), "wql3d_domain_create")
         self.handle = h
         self.nblocks = nb
-        self.dt = problem.dt()
+        self.dt = problem.dt() if slab is None else slab.dt
         self.RK = init_RK()
         self.n = 1
 
@@ -297,6 +308,21 @@ class Domain:
 
     def pack_interface(self):
         _lib.check(_lib.load().wql3d_pack_interface(self.handle), "wql3d_pack_interface")
+
+    # ghost planes of an s-slab domain (kind 0: fields, 1: metric)
+    def halo_buffers(self, kind: int = 0):
+        """(send_ptr, recv_ptr, count per face, elem_bytes) of the ghost-plane buffers."""
+        snd, rcv = C.c_void_p(), C.c_void_p()
+        cnt, eb = C.c_int64(), C.c_int32()
+        _lib.check(_lib.load().wql3d_halo_buffers(self.handle, int(kind), C.byref(snd), C.byref(rcv), C.byref(cnt),
+                                                  C.byref(eb)), "wql3d_halo_buffers")
+        return snd.value, rcv.value, cnt.value, eb.value
+
+    def pack_halo(self, kind: int = 0):
+        _lib.check(_lib.load().wql3d_pack_halo(self.handle, int(kind)), "wql3d_pack_halo")
+
+    def unpack_halo(self, kind: int = 0):
+        _lib.check(_lib.load().wql3d_unpack_halo(self.handle, int(kind)), "wql3d_unpack_halo")
 
     def interface_material(self) -> np.ndarray:
         nq, nr, ns = self.blocks[0].nqrs
