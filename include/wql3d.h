@@ -69,12 +69,15 @@ extern "C" {
 #define WQL3D_IFACE_LOCKED 0
 #define WQL3D_IFACE_SLIP_WEAKENING 1
 #define WQL3D_IFACE_LINEAR 2
+#define WQL3D_IFACE_RATE_STATE 3      /* rate-and-state, Regula-Falsi slip rate (src/Interface_Condition.f90:918-1263) */
 
 /* fault prestress and static friction: per-point maps (iface_tau0, iface_fs)
    or the reference's TPV5 formulas (src/Interface_Condition.f90:1283-1294,
    1822-1830) evaluated at the face coordinates */
 #define WQL3D_FAULT_MAPS 0
 #define WQL3D_FAULT_TPV5 1
+#define WQL3D_FAULT_TPV101 2          /* rate-and-state TPV101 / TPV102 prestress and parameters */
+#define WQL3D_FAULT_TPV102 3
 
 /* fault outputs of wql3d_get_fault_output (src/domain.f90:782-845,
    src/fault_output.f90:73-122): [component][ns][nr] doubles */

@@ -1173,6 +1173,8 @@ static void do_stage(odom *D, int stage, double dt, double t0, int sample, doubl
 /* ------------------------------------------------------------------------ */
 /* Public API                                                                */
 /* ------------------------------------------------------------------------ */
+static void rs_init_vel_state(odom *D);
+
 void *orc_create(int nblocks, const orc_desc *blocks, const orc_iface_desc *iface) {
   odom *D = (odom *)calloc(1, sizeof(odom));
   D->nb = nblocks;
@@ -1203,6 +1205,7 @@ void *orc_create(int nblocks, const orc_desc *blocks, const orc_iface_desc *ifac
       }
     }
     D->I = I;
+    if (I->d.coupling == ORC_IFACE_RATE_STATE) rs_init_vel_state(D);
   }
   D->t = 0.0;
   return D;
@@ -1512,6 +1515,142 @@ static void slip_weakening(const oiface *I, long k, const double x[3], const dou
   P[4] = tm_hat; P[5] = tl_hat; Q[4] = tm_hat; Q[5] = tl_hat;
 }
 
+/* smooth_boxcar, src/Interface_Condition.f90:2460-2476 */
+static double smooth_boxcar(double x, double w, double wr) {
+  if (-w <= x && x <= w) return 1.0;
+  if (fabs(x) > w && fabs(x) < w + wr) return 0.5 * (1.0 + tanh(wr / (fabs(x) - w - wr) + wr / (fabs(x) - w)));
+  return 0.0;
+}
+
+/* TPV101 / TPV102 rate-and-state parameters, src/Interface_Condition.f90:386-401 */
+#define RS_L0 0.02
+#define RS_F0 0.6
+#define RS_B 0.012
+#define RS_V0 1.0e-6
+static double rs_a(const double x[3]) {
+  return 0.008 + 0.008 * (1.0 - smooth_boxcar(x[1], 15.0, 3.0) * smooth_boxcar(x[2], 15.0, 3.0));
+}
+
+/* TPV101 / TPV102 prestress in the face basis at time t: the initial stress of
+   src/initial_stress_condition.f90:114-120 as tractions on n, rotated onto
+   n, m, l, plus the nucleation ramp 25 F(r) G(t) on T0_l
+   (src/Interface_Condition.f90:2324-2385) */
+static void rs_prestress(const double x[3], double t, const double n[3], const double m[3], const double l[3],
+                         double *T0n, double *T0m, double *T0l) {
+  const double sxx = -120.0, syy = 0.0, szz = -120.0, sxy = 0.0, sxz = 75.0, syz = 0.0;
+  double Tx = n[0] * sxx + n[1] * sxy + n[2] * sxz;
+  double Ty = n[0] * sxy + n[1] * syy + n[2] * syz;
+  double Tz = n[0] * sxz + n[1] * syz + n[2] * szz;
+  *T0n = n[0] * Tx + n[1] * Ty + n[2] * Tz;
+  *T0m = m[0] * Tx + m[1] * Ty + m[2] * Tz;
+  *T0l = l[0] * Tx + l[1] * Ty + l[2] * Tz;
+  double r = sqrt((x[1] - 7.5) * (x[1] - 7.5) + x[2] * x[2]);
+  double F = 0.0;
+  if (r < 3.0) F = exp(r * r / (r * r - 9.0));
+  double G = 0.0;
+  if (t > 0.0 && t < 1.0) G = exp((t - 1.0) * (t - 1.0) / (t * (t - 2.0)));
+  if (t >= 1.0) G = 1.0;
+  *T0l = *T0l + 25.0 * F * G;
+}
+
+/* f(V) = V + a sigma_n / eta asinh(V / (2 V0) exp(psi / a)) - Phi / eta,
+   src/Interface_Condition.f90:1242-1263 */
+static double rs_f(double V, double Phi, double eta, double sn, double psi, double a) {
+  return V + a * sn / eta * asinh(0.5 * V / RS_V0 * exp(psi / a)) - Phi / eta;
+}
+
+/* Regula_Falsi, src/Interface_Condition.f90:1170-1239: bracket [0, Phi/eta],
+   absolute tolerance 1e-12, at most 5000 iterations */
+static double rs_regula_falsi(double V, double Phi, double eta, double sn, double psi, double a) {
+  const double tol = 1.0e-12;
+  double Vl = 0.0, Vr = Phi / eta;
+  double fv = rs_f(V, Phi, eta, sn, psi, a);
+  double fl = rs_f(Vl, Phi, eta, sn, psi, a);
+  double fr = rs_f(Vr, Phi, eta, sn, psi, a);
+  if (fabs(fv) <= tol) return V;
+  if (fabs(fl) <= tol) return Vl;
+  if (fabs(fr) <= tol) return Vr;
+  double err = 1.0;
+  for (int k = 1; k <= 5000 && err >= tol; ++k) {
+    double V1 = V;
+    if (fv * fl > tol) {
+      Vl = V;
+      V = Vr - (Vr - Vl) * fr / (fr - fl);
+      fl = fv;
+    } else if (fv * fr > tol) {
+      Vr = V;
+      V = Vr - (Vr - Vl) * fr / (fr - fl);
+      fr = fv;
+    }
+    fv = rs_f(V, Phi, eta, sn, psi, a);
+    err = fabs(V - V1);
+  }
+  return V;
+}
+
+/* rate_state_friction + solve('rate-and-state_friction'),
+   src/Interface_Condition.f90:918-1067, 1095-1168; *Vrs: the solved slip rate */
+static void rate_state(const double x[3], double t, const double n[3], const double m[3], const double l[3],
+                       const double *U, const double *V, double *P, double *Q, double Z1s, double Z2s, double Z1p,
+                       double Z2p, double psi, double *Vrs) {
+  char_t c;
+  characteristics(U, V, Z1s, Z2s, Z1p, Z2p, &c);
+  double T0n, T0m, T0l;
+  rs_prestress(x, t, n, m, l, &T0n, &T0m, &T0l);
+  P[0] = (c.q[0] - c.phi[0]) / Z2p; P[3] = c.phi[0];
+  Q[0] = (c.p[0] + c.phi[0]) / Z1p; Q[3] = c.phi[0];
+  double sigma_n = fmax(0.0, -(T0n + c.phi[0]));
+  double a = rs_a(x);
+  double vm = V[1] - U[1], vl = V[2] - U[2];
+  double phi1 = T0m + c.phi[1], phi2 = T0l + c.phi[2];
+  double Phi = sqrt(phi1 * phi1 + phi2 * phi2);
+  double Vs = sqrt(vm * vm + vl * vl);
+  if (Vs > Phi) Vs = 0.5 * Phi / c.eta_s;
+  Vs = rs_regula_falsi(Vs, Phi, c.eta_s, sigma_n, psi, a);
+  double fv = sigma_n * a * asinh(0.5 * Vs / RS_V0 * exp(psi / a));
+  vm = phi1 / (c.eta_s + fv / Vs);
+  vl = phi2 / (c.eta_s + fv / Vs);
+  double tm = (phi1 - c.eta_s * vm) - T0m;
+  double tl = (phi2 - c.eta_s * vl) - T0l;
+  Q[1] = (tm + c.p[1]) / Z1s + vm;
+  Q[2] = (tl + c.p[2]) / Z1s + vl;
+  P[1] = (c.q[1] - tm) / Z2s - vm;
+  P[2] = (c.q[2] - tl) / Z2s - vl;
+  P[4] = tm; P[5] = tl; Q[4] = tm; Q[5] = tl;
+  *Vrs = Vs;
+}
+
+/* init_vel_state for TPV101 / TPV102 as the one-process run calls it
+   (src/domain.f90:273, src/Interface_Condition.f90:2722-2786): block 1's v_z
+   set to -Vin/2 (Vin = 1e-12), and the state W from block 1's q-max face
+   traction at t = 0: theta = L0/V0 exp((a log(2 sinh(T0_l/(a sigma_n))) - f0
+   - a log(Vin/V0))/b), W = f0 + b log(V0/L0 theta).  V0 there is an
+   unsuffixed literal: single precision unless the reals are promoted, so it
+   follows the block's closure-literal switch. */
+static void rs_init_vel_state(odom *D) {
+  oblk *b = D->B[0];
+  oiface *I = D->I;
+  const double Vin = 1.0e-12;
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) b->F[2][ID(b, x, y, z)] = -(0.5 * Vin);
+  const double V0 = b->d.f32lit ? (double)1.0e-6f : 1.0e-6;
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y) {
+      long k = (long)(y - 1) + (long)b->ny * (z - 1);
+      long p = ID(b, b->nx, y, z);
+      double x[3] = {b->X[0][p], b->X[1][p], b->X[2][p]};
+      double n[3], m[3], l[3];
+      for (int c = 0; c < 3; ++c) { n[c] = b->nn[1][c][k]; m[c] = b->nm[1][c][k]; l[c] = b->nl[1][c][k]; }
+      double T0n, T0m, T0l;
+      rs_prestress(x, 0.0, n, m, l, &T0n, &T0m, &T0l);
+      double a = rs_a(x);
+      double sigma_n = -T0n;
+      double theta = RS_L0 / V0 * exp(((a * log(2.0 * sinh(T0l / (a * sigma_n)))) - RS_F0 - a * log(Vin / V0)) / RS_B);
+      I->W[k] = RS_F0 + RS_B * log(V0 / RS_L0 * theta);
+    }
+}
+
 static void rotate_in(double *w, const double n[3], const double m[3], const double l[3]) {
   /* src/CouplingForcing.f90:466-520 */
   double a[6];
@@ -1622,7 +1761,11 @@ void orc_iface_couple(odom *D, int ib, double t, int stage) {
       double Z1s = rho1 * c1s, Z2s = rho2 * c2s, Z1p = rho1 * c1p, Z2p = rho2 * c2p;
       double x[3] = {b->X[0][p], b->X[1][p], b->X[2][p]};
       double P[6], Q[6];
+      double Vrs = 0.0;
       switch (I->d.coupling) {
+        case ORC_IFACE_RATE_STATE:
+          rate_state(x, t, n, m, l, u, v, P, Q, Z1s, Z2s, Z1p, Z2p, I->W[k], &Vrs);
+          break;
         case ORC_IFACE_SLIP_WEAKENING:
           slip_weakening(I, k, x, u, v, P, Q, Z1s, Z2s, Z1p, Z2p, I->S[3][k]);
           break;
@@ -1637,10 +1780,14 @@ void orc_iface_couple(odom *D, int ib, double t, int stage) {
       if (accumulate) {
         for (int c = 0; c < 3; ++c) I->DS[c][k] = I->DS[c][k] + Q[c] - P[c];
         I->DS[3][k] = I->DS[3][k] + Vel;
+        /* rate of state, TPV101 / TPV102 (src/Interface_Condition.f90:431-436) */
+        if (I->d.coupling == ORC_IFACE_RATE_STATE)
+          I->DW[k] = I->DW[k] + RS_B * RS_V0 / RS_L0 * exp(-(I->W[k] - RS_F0) / RS_B) - Vrs * RS_B / RS_L0;
       }
       if (stage == 1 && record) {
         double T0n = 0.0, T0m = 0.0, T0l = 0.0;
-        if (I->d.coupling != ORC_IFACE_LOCKED) fault_prestress(I, k, x, &T0n, &T0m, &T0l);
+        if (I->d.coupling == ORC_IFACE_RATE_STATE) rs_prestress(x, t, n, m, l, &T0n, &T0m, &T0l);
+        else if (I->d.coupling != ORC_IFACE_LOCKED) fault_prestress(I, k, x, &T0n, &T0m, &T0l);
         /* Couple_Interface_x overwrites components 1:3 with v_hat - u_hat */
         for (int c = 0; c < 3; ++c) {
           double sv = Q[c] - P[c];

@@ -27,8 +27,8 @@ enum {
 };
 
 /* interface coupling laws, src/Interface_Condition.f90 */
-enum { ORC_IFACE_LOCKED = 0, ORC_IFACE_SLIP_WEAKENING = 1, ORC_IFACE_LINEAR = 2 };
-enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1 };
+enum { ORC_IFACE_LOCKED = 0, ORC_IFACE_SLIP_WEAKENING = 1, ORC_IFACE_LINEAR = 2, ORC_IFACE_RATE_STATE = 3 };
+enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1, ORC_FAULT_TPV101 = 2, ORC_FAULT_TPV102 = 3 };
 /* fault outputs, src/domain.f90:782-845 and src/fault_output.f90:73-122; layout [comp][ns][nr] */
 enum { ORC_FO_S = 0, ORC_FO_SVEL = 1, ORC_FO_UHAT = 2, ORC_FO_VHAT = 3, ORC_FO_STATE = 4, ORC_FO_TRUP = 5 };
 

@@ -192,3 +192,15 @@ def mms_case(n=21, mesh="cartesian", bc=((2, 1, 3), (1, 3, 1)), t_final=0.1, het
 
 def mms_error(fields, exact):
     return float(np.linalg.norm(fields - exact) / np.linalg.norm(exact))
+
+
+def tpv101_case(serial_shared=False, n=21, t_final=0.5, problem="TPV101"):
+    """The TPV5 geometry with the reference's rate-and-state law and TPV101 /
+    TPV102 prestress (src/Interface_Condition.f90:386-436, 918-1263,
+    2324-2385): uniform background stress (-120, 0, -120, 0, 75, 0), a
+    nucleation patch of radius 3 at (y, z) = (7.5, 0) ramped in over 1 s, the
+    state starting at 0 as the reference leaves it."""
+    from waveqlab3d_q_gpu_b200.problem import InterfaceParams
+    p = tpv5_case(serial_shared=serial_shared, n=n, t_final=t_final)
+    p.interface = InterfaceParams(coupling="rate-and-state_friction", problem=problem, serial_shared=serial_shared)
+    return p

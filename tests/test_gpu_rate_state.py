@@ -1,0 +1,118 @@
+"""Rate-and-state interface (TPV101 / TPV102) on the CUDA path against the
+CPU oracle: both blocks' fields, the fault outputs (slip, slip rate, hat
+tractions, state, rupture time) after every step.
+
+Tolerances (1e-12 relative for the other laws).  While the fault creeps at
+the initial 1e-12 m/s, the Regula-Falsi solve stops on an absolute step of
+1e-12 m/s, of the order of the slip rate itself, and evaluates exp / asinh,
+whose device and host implementations may differ in the last bit: the
+slip rate is then defined only to about that step, and the two solves
+differ by up to 7e-16 m/s after 12 steps.  Slip rates, slip and the fields
+they drive are held to 1e-8 of their size or an absolute 1e-13 m/s (a
+tenth of the solver's step; 1e-12 MPa for stresses), tractions and state to
+1e-12 relative.  Once the ramped
+nucleation has raised the slip rate by orders of magnitude (60 steps),
+everything agrees to 1e-9 relative L2."""
+import numpy as np
+import pytest
+
+from cases import rel_l2, tpv101_case, two_block_case
+
+pytestmark = pytest.mark.gpu
+
+FAULT = ("S", "Svel", "Uhat", "Vhat", "state")
+
+
+def _close(a, b, rtol, atol):
+    """max |a - b| within rtol of max |b|, or within atol."""
+    err = np.abs(np.asarray(a) - np.asarray(b)).max()
+    return err <= max(rtol * np.abs(b).max(), atol), err
+
+
+def _compare(g, o):
+    for name, rtol in (("S", 1e-8), ("Svel", 1e-8), ("Uhat", 1e-12), ("Vhat", 1e-12), ("state", 1e-12)):
+        ok, err = _close(g.fault(name), o.fault(name), rtol, 1e-13)
+        assert ok, (name, err)
+    assert np.array_equal(g.fault("trup"), o.fault("trup"))
+    for b in (0, 1):
+        Fg, Fo = g.fields(b), o.fields(b)
+        ok, err = _close(Fg[:3], Fo[:3], 1e-8, 1e-13)      # velocities, m/s
+        assert ok, (b, "v", err)
+        ok, err = _close(Fg[3:], Fo[3:], 1e-8, 1e-12)      # stresses, MPa (Z ~ 10 x velocities)
+        assert ok, (b, "sigma", err)
+
+
+@pytest.mark.parametrize("serial", [False, True])
+def test_tpv101_steps_match_oracle(wql3d_lib, oracle_lib, serial):
+    from waveqlab3d_q_gpu_b200.domain import Domain
+    p = tpv101_case(serial_shared=serial)
+    o = oracle_lib.OracleDomain(p)
+    g = Domain(p, nsteps_hint=12)
+    # the initial state and velocity of init_vel_state
+    assert rel_l2(g.fault("state"), o.fault("state")) < 1e-14
+    assert np.array_equal(g.fields(0)[2], o.fields(0)[2])
+    for n in range(1, 13):
+        o.run(1)
+        g.time_step_RK(n)
+        _compare(g, o)
+
+
+def test_tpv101_graph_run_equals_steps(wql3d_lib):
+    from waveqlab3d_q_gpu_b200.domain import Domain
+    p = tpv101_case()
+    a = Domain(p, nsteps_hint=20)
+    b = Domain(p, nsteps_hint=20)
+    for n in range(1, 11):
+        a.time_step_RK(n)
+    b.run(10)
+    for k in (0, 1):
+        assert np.array_equal(a.fields(k), b.fields(k))
+    assert np.array_equal(a.fault("state"), b.fault("state"))
+
+
+def test_rate_state_curvilinear_q8_pml(wql3d_lib, oracle_lib):
+    """Curvilinear two-block Q8 + PML with the rate-and-state law (per-side
+    normals from each block's metric)."""
+    from waveqlab3d_q_gpu_b200.domain import Domain
+    from waveqlab3d_q_gpu_b200.problem import InterfaceParams
+    p = two_block_case(mesh="curvilinear", coupling="locked", response="anelastic-Q8", pml=True)
+    p.interface = InterfaceParams(coupling="rate-and-state_friction", problem="TPV101")
+    o = oracle_lib.OracleDomain(p)
+    g = Domain(p, nsteps_hint=8)
+    for n in range(1, 9):
+        o.run(1)
+        g.time_step_RK(n)
+    _compare(g, o)
+
+
+def test_fp32_rate_state_tracks_fp64(wql3d_lib):
+    """The FP32 path through the nucleation (60 steps): fields and slip rate
+    within 1e-3 of FP64 (the law and the slip run in FP64 on both paths)."""
+    from waveqlab3d_q_gpu_b200.domain import Domain
+    p = tpv101_case(t_final=1.0)
+    a = Domain(p, nsteps_hint=60)
+    b = Domain(p, precision="fp32", nsteps_hint=60)
+    a.run(60)
+    b.run(60)
+    for k in (0, 1):
+        assert rel_l2(b.fields(k), a.fields(k)) < 1e-3, (k, rel_l2(b.fields(k), a.fields(k)))
+    assert rel_l2(b.fault("Svel"), a.fault("Svel")) < 1e-3, rel_l2(b.fault("Svel"), a.fault("Svel"))
+    assert rel_l2(b.fault("state"), a.fault("state")) < 1e-6
+
+
+def test_tpv101_nucleation_matches_oracle(wql3d_lib, oracle_lib):
+    """60 steps (t = 0.64 s): the ramped nucleation stress (G(0.64) = 0.87)
+    drives the patch above its steady friction and the slip rate grows by
+    orders of magnitude; fields and fault outputs still agree."""
+    from waveqlab3d_q_gpu_b200.domain import Domain
+    p = tpv101_case(t_final=1.0)
+    o = oracle_lib.OracleDomain(p)
+    g = Domain(p, nsteps_hint=60)
+    o.run(60)
+    g.run(60)
+    sv = g.fault("Svel")
+    assert np.sqrt(sv[1] ** 2 + sv[2] ** 2).max() > 1e3 * 1e-12
+    for name in FAULT:
+        assert rel_l2(g.fault(name), o.fault(name)) < 1e-9, (name, rel_l2(g.fault(name), o.fault(name)))
+    for b in (0, 1):
+        assert rel_l2(g.fields(b), o.fields(b)) < 1e-9, (b, rel_l2(g.fields(b), o.fields(b)))

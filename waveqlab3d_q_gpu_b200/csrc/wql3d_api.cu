@@ -292,6 +292,14 @@ __global__ void k_metrics(Blk<T> b, const double *X, double *met, double *Jout) 
   Jout[p] = J;
 }
 
+// one field component set to v at every point of a block (init_vel_state)
+template <typename T>
+__global__ void k_fill_component(Blk<T> b, T *F, int c, T v) {
+  int x, y, z;
+  if (!flat_point(b, x, y, z)) return;
+  F[(long long)c * b.vol + pidx(b, x, y, z)] = v;
+}
+
 template <typename T>
 __global__ void k_convert(const double *src, T *dst, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1091,6 +1099,14 @@ wql3d_domain *checked(wql3d_domain *d) { return d; }
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// v_z of block bi set to v everywhere (the current field buffer)
+void init_velocity(wql3d_domain *d, int bi, double v) {
+  const long long np = (long long)d->hb[bi].nq * d->hb[bi].nr * d->hb[bi].ns;
+  const unsigned gr = (unsigned)((np + 255) / 256);
+  if (d->fp32) k_fill_component<float><<<gr, 256, 0, d->stream>>>(d->bf[bi], d->cur ? d->bf[bi].F1 : d->bf[bi].F0, 2, (float)v);
+  else k_fill_component<double><<<gr, 256, 0, d->stream>>>(d->bd[bi], d->cur ? d->bd[bi].F1 : d->bd[bi].F0, 2, v);
+}
+
 // ghost-plane pack / unpack of an s-slab domain on its stream
 template <typename T>
 int halo_launch(wql3d_domain *d, Blk<T> &b, int kind, int unpack) {
@@ -1177,6 +1193,8 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     d->has_iface = true;
     if (d->fp32) d->bf[0].isat[side == 1 ? 1 : 0] = (float *)(side == 1 ? d->iface.sat_m : d->iface.sat_p);
     else d->bd[0].isat[side == 1 ? 1 : 0] = (double *)(side == 1 ? d->iface.sat_m : d->iface.sat_p);
+    // init_vel_state: v_z = -Vin/2 on block 1's rank, +Vin/2 on block 2's (src/domain.f90:273-274)
+    if (rs_problem(d->desc.fault_problem)) init_velocity(d, 0, side == 1 ? -0.5e-12 : 0.5e-12);
   } else if (d->desc.remote_side != 0) {
     return cleanup(fail(WQL3D_EINVAL, "remote_side needs nblocks = 1"));
   }
@@ -1189,6 +1207,8 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     d->has_iface = true;
     if (d->fp32) { d->bf[0].isat[1] = (float *)d->iface.sat_m; d->bf[1].isat[0] = (float *)d->iface.sat_p; }
     else { d->bd[0].isat[1] = (double *)d->iface.sat_m; d->bd[1].isat[0] = (double *)d->iface.sat_p; }
+    // init_vel_state of the one-process run: block 1's v_z = -Vin/2 (src/domain.f90:273)
+    if (rs_problem(d->desc.fault_problem)) init_velocity(d, 0, -0.5e-12);
   }
   if (cudaStreamSynchronize(d->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
     return cleanup(fail(WQL3D_ECUDA, "setup kernels failed"));

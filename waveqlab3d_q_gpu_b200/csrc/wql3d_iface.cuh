@@ -50,7 +50,34 @@ struct IfaceDev {
   void *send = nullptr;    // this block's face trace, 9 x n (field precision)
   void *recv = nullptr;    // the other side's face trace, 9 x n
   void *oppM = nullptr;    // the other side's lambda, mu, rho at the face, 3 x n
+  // rate-and-state (TPV101 / TPV102): per side the direct-effect map a and the
+  // nucleation amplitude 25 F(r) of the time-ramped prestress
+  double *ra[2] = {nullptr, nullptr};
+  double *nuc[2] = {nullptr, nullptr};
 };
+
+// TPV101 / TPV102 rate-and-state parameters, src/Interface_Condition.f90:386-401
+constexpr double kRsL0 = 0.02, kRsF0 = 0.6, kRsB = 0.012, kRsV0 = 1.0e-6;
+
+// smooth_boxcar, src/Interface_Condition.f90:2460-2476
+inline double host_smooth_boxcar(double x, double w, double wr) {
+  if (-w <= x && x <= w) return 1.0;
+  if (std::fabs(x) > w && std::fabs(x) < w + wr)
+    return 0.5 * (1.0 + std::tanh(wr / (std::fabs(x) - w - wr) + wr / (std::fabs(x) - w)));
+  return 0.0;
+}
+
+// per-point direct-effect parameter a and nucleation amplitude 25 F(r)
+// (src/Interface_Condition.f90:386-401, 2340-2352)
+inline void rs_point(const double x[3], double *a, double *nuc) {
+  *a = 0.008 + 0.008 * (1.0 - host_smooth_boxcar(x[1], 15.0, 3.0) * host_smooth_boxcar(x[2], 15.0, 3.0));
+  const double r = std::sqrt((x[1] - 7.5) * (x[1] - 7.5) + x[2] * x[2]);
+  double F = 0.0;
+  if (r < 3.0) F = std::exp(r * r / (r * r - 9.0));
+  *nuc = 25.0 * F;
+}
+
+inline bool rs_problem(int p) { return p == WQL3D_FAULT_TPV101 || p == WQL3D_FAULT_TPV102; }
 
 // boxcar of unit amplitude on (-w, w), 1/2 within 100 eps of the edges
 // (src/Interface_Condition.f90:2438-2457)
@@ -74,6 +101,53 @@ inline void tpv5_point(const double x[3], double *T0n, double *T0m, double *T0l,
   *fs = 0.677 + 1.0e10 * (1.0 - host_boxcar(x[1], 15.0) * host_boxcar(x[2], 15.0));
 }
 
+// init_vel_state's state for TPV101 / TPV102 (src/Interface_Condition.f90:2722-2786):
+// W from the t = 0 traction on one block's interface face (basis of face
+// `face`, coordinates at q = xend): theta = L0/V0 exp((a log(2 sinh(T0_l/(a
+// sigma_n))) - f0 - a log(Vin/V0))/b), W = f0 + b log(V0/L0 theta).  V0 is an
+// unsuffixed literal there: single precision unless reals are promoted (lit).
+template <typename T>
+int rs_init_state(IfaceDev &I, const Blk<T> &b, int face, const std::vector<double> &coords, int xend, cudaStream_t s) {
+  const int ny = I.ny, nz = I.nz;
+  const long long n = (long long)ny * nz;
+  std::vector<T> B((size_t)(9 * n));
+  if (cudaMemcpyAsync(B.data(), b.nrm[face], sizeof(T) * 9 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return WQL3D_ECUDA;
+  const double Vin = 1.0e-12, V0 = b.lit ? (double)1.0e-6f : 1.0e-6;
+  const double sxx = -120.0, syy = 0.0, szz = -120.0, sxy = 0.0, sxz = 75.0, syz = 0.0;
+  const long long nb = (long long)b.nx * ny * nz;
+  std::vector<double> W((size_t)n);
+  for (int z = 1; z <= nz; ++z)
+    for (int y = 1; y <= ny; ++y) {
+      const long long k = (long long)(y - 1) + (long long)ny * (z - 1);
+      const long long q = (long long)(xend - 1) + (long long)b.nx * ((y - 1) + (long long)ny * (z - 1));
+      const double x[3] = {coords[(size_t)q], coords[(size_t)(nb + q)], coords[(size_t)(2 * nb + q)]};
+      double l[3], m[3], nv[3];
+      for (int c = 0; c < 3; ++c) {
+        l[c] = (double)B[(size_t)((0 + c) * n + k)];
+        m[c] = (double)B[(size_t)((3 + c) * n + k)];
+        nv[c] = (double)B[(size_t)((6 + c) * n + k)];
+      }
+      const double Tx = nv[0] * sxx + nv[1] * sxy + nv[2] * sxz;
+      const double Ty = nv[0] * sxy + nv[1] * syy + nv[2] * syz;
+      const double Tz = nv[0] * sxz + nv[1] * syz + nv[2] * szz;
+      const double T0n = nv[0] * Tx + nv[1] * Ty + nv[2] * Tz;
+      const double T0l = l[0] * Tx + l[1] * Ty + l[2] * Tz;
+      (void)m;
+      double a, nuc;
+      rs_point(x, &a, &nuc);
+      const double sigma_n = -T0n;
+      const double theta = kRsL0 / V0 *
+                           std::exp(((a * std::log(2.0 * std::sinh(T0l / (a * sigma_n)))) - kRsF0 - a * std::log(Vin / V0)) / kRsB);
+      W[(size_t)k] = kRsF0 + kRsB * std::log(V0 / kRsL0 * theta);
+    }
+  if (cudaMemcpyAsync(I.W, W.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return WQL3D_ECUDA;
+  return WQL3D_OK;
+}
+
 // Allocate the interface state and build the per-side prestress / strength
 // maps.  coords0 / coords1: host coordinates of the two blocks (3 x nq*nr*ns,
 // x fastest); nq0 is block 1's q extent.
@@ -82,8 +156,9 @@ int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, co
                 const std::vector<double> &coords0, const std::vector<double> &coords1, AllocT &mem,
                 cudaStream_t s) {
   if (b0.ny != b1.ny || b0.nz != b1.nz) return WQL3D_EINVAL;
-  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_LINEAR) return WQL3D_EINVAL;
-  if (desc.fault_problem != WQL3D_FAULT_MAPS && desc.fault_problem != WQL3D_FAULT_TPV5) return WQL3D_EINVAL;
+  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_RATE_STATE) return WQL3D_EINVAL;
+  if (desc.fault_problem < WQL3D_FAULT_MAPS || desc.fault_problem > WQL3D_FAULT_TPV102) return WQL3D_EINVAL;
+  if ((desc.coupling == WQL3D_IFACE_RATE_STATE) != rs_problem(desc.fault_problem)) return WQL3D_EINVAL;
   const int ny = b0.ny, nz = b0.nz;
   const long long n = (long long)ny * nz;
   I.ny = ny;
@@ -107,15 +182,17 @@ int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, co
   const int nq[2] = {b0.nx, b1.nx};
   const std::vector<double> *cs[2] = {&coords0, &coords1};
   for (int side = 0; side < 2; ++side) {
-    std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs);
+    std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs), ra((size_t)n, 0.0), nuc((size_t)n, 0.0);
     const int xend = side == 0 ? nq[0] : 1;
     const long long nb = (long long)nq[side] * ny * nz;
     for (int z = 1; z <= nz; ++z)
       for (int y = 1; y <= ny; ++y) {
         long long k = (long long)(y - 1) + (long long)ny * (z - 1);
-        if (desc.fault_problem == WQL3D_FAULT_TPV5) {
-          long long q = (long long)(xend - 1) + (long long)nq[side] * ((y - 1) + (long long)ny * (z - 1));
-          double x[3] = {(*cs[side])[(size_t)q], (*cs[side])[(size_t)(nb + q)], (*cs[side])[(size_t)(2 * nb + q)]};
+        long long q = (long long)(xend - 1) + (long long)nq[side] * ((y - 1) + (long long)ny * (z - 1));
+        double x[3] = {(*cs[side])[(size_t)q], (*cs[side])[(size_t)(nb + q)], (*cs[side])[(size_t)(2 * nb + q)]};
+        if (rs_problem(desc.fault_problem)) {
+          rs_point(x, &ra[(size_t)k], &nuc[(size_t)k]);
+        } else if (desc.fault_problem == WQL3D_FAULT_TPV5) {
           tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
         } else {
           if (desc.iface_tau0)
@@ -123,13 +200,20 @@ int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, co
           if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
         }
       }
-    if (mem.get(&I.t0[side], 3 * n) || mem.get(&I.fs[side], n)) return WQL3D_ENOMEM;
+    if (mem.get(&I.t0[side], 3 * n) || mem.get(&I.fs[side], n) || mem.get(&I.ra[side], n) || mem.get(&I.nuc[side], n))
+      return WQL3D_ENOMEM;
     if (cudaMemcpyAsync(I.t0[side], t0.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(I.fs[side], f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        cudaMemcpyAsync(I.fs[side], f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(I.ra[side], ra.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(I.nuc[side], nuc.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
       return WQL3D_ECUDA;
+    // the host vectors go out of scope at the end of this iteration
+    if (cudaStreamSynchronize(s) != cudaSuccess) return WQL3D_ECUDA;
   }
   // the host vectors above go out of scope: finish the copies first
   if (cudaStreamSynchronize(s) != cudaSuccess) return WQL3D_ECUDA;
+  // the one-process run initialises the state from block 1 (src/domain.f90:273)
+  if (rs_problem(desc.fault_problem)) return rs_init_state<T>(I, b0, 1, coords0, b0.nx, s);
   return WQL3D_OK;
 }
 
@@ -138,8 +222,9 @@ template <typename T, typename AllocT>
 int setup_iface_remote(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b, const std::vector<double> &coords,
                        int side, AllocT &mem, cudaStream_t s) {
   if (side != 1 && side != 2) return WQL3D_EINVAL;
-  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_LINEAR) return WQL3D_EINVAL;
-  if (desc.fault_problem != WQL3D_FAULT_MAPS && desc.fault_problem != WQL3D_FAULT_TPV5) return WQL3D_EINVAL;
+  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_RATE_STATE) return WQL3D_EINVAL;
+  if (desc.fault_problem < WQL3D_FAULT_MAPS || desc.fault_problem > WQL3D_FAULT_TPV102) return WQL3D_EINVAL;
+  if ((desc.coupling == WQL3D_IFACE_RATE_STATE) != rs_problem(desc.fault_problem)) return WQL3D_EINVAL;
   const int ny = b.ny, nz = b.nz;
   const long long n = (long long)ny * nz;
   I.ny = ny;
@@ -163,15 +248,17 @@ int setup_iface_remote(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> 
   std::vector<double> tr((size_t)n, 1.0e9);
   if (cudaMemcpyAsync(I.trup, tr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return WQL3D_ECUDA;
-  std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs);
+  std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs), ra((size_t)n, 0.0), nuc((size_t)n, 0.0);
   const int xend = side == 1 ? b.nx : 1;
   const long long nb = (long long)b.nx * ny * nz;
   for (int z = 1; z <= nz; ++z)
     for (int y = 1; y <= ny; ++y) {
       long long k = (long long)(y - 1) + (long long)ny * (z - 1);
-      if (desc.fault_problem == WQL3D_FAULT_TPV5) {
-        long long q = (long long)(xend - 1) + (long long)b.nx * ((y - 1) + (long long)ny * (z - 1));
-        double x[3] = {coords[(size_t)q], coords[(size_t)(nb + q)], coords[(size_t)(2 * nb + q)]};
+      long long q = (long long)(xend - 1) + (long long)b.nx * ((y - 1) + (long long)ny * (z - 1));
+      double x[3] = {coords[(size_t)q], coords[(size_t)(nb + q)], coords[(size_t)(2 * nb + q)]};
+      if (rs_problem(desc.fault_problem)) {
+        rs_point(x, &ra[(size_t)k], &nuc[(size_t)k]);
+      } else if (desc.fault_problem == WQL3D_FAULT_TPV5) {
         tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
       } else {
         if (desc.iface_tau0)
@@ -179,11 +266,18 @@ int setup_iface_remote(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> 
         if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
       }
     }
-  if (mem.get(&I.t0[side - 1], 3 * n) || mem.get(&I.fs[side - 1], n)) return WQL3D_ENOMEM;
+  if (mem.get(&I.t0[side - 1], 3 * n) || mem.get(&I.fs[side - 1], n) || mem.get(&I.ra[side - 1], n) ||
+      mem.get(&I.nuc[side - 1], n))
+    return WQL3D_ENOMEM;
   if (cudaMemcpyAsync(I.t0[side - 1], t0.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(I.fs[side - 1], f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      cudaMemcpyAsync(I.fs[side - 1], f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(I.ra[side - 1], ra.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(I.nuc[side - 1], nuc.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return WQL3D_ECUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return WQL3D_ECUDA;
+  // one block per rank: each rank initialises the state from its own face
+  // (src/domain.f90:273-274)
+  if (rs_problem(desc.fault_problem)) return rs_init_state<T>(I, b, side == 1 ? 1 : 0, coords, xend, s);
   return WQL3D_OK;
 }
 
@@ -214,17 +308,99 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
   return __dadd_rn(__dadd_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1])), __dmul_rn(a[2], b[2]));
 }
 
+// TPV101 / TPV102 prestress in the face basis at time t: the initial stress
+// (-120, 0, -120, 0, 75, 0) of src/initial_stress_condition.f90:114-120 as
+// tractions on n, rotated onto n, m, l, plus the nucleation 25 F(r) G(t) on
+// T0_l (src/Interface_Condition.f90:2324-2385)
+__device__ __forceinline__ void rs_prestress(double t, double nuc, const double n[3], const double m[3],
+                                             const double l[3], double T0[3]) {
+  const double sxx = -120.0, syy = 0.0, szz = -120.0, sxy = 0.0, sxz = 75.0, syz = 0.0;
+  const double Tx = __dadd_rn(__dadd_rn(__dmul_rn(n[0], sxx), __dmul_rn(n[1], sxy)), __dmul_rn(n[2], sxz));
+  const double Ty = __dadd_rn(__dadd_rn(__dmul_rn(n[0], sxy), __dmul_rn(n[1], syy)), __dmul_rn(n[2], syz));
+  const double Tz = __dadd_rn(__dadd_rn(__dmul_rn(n[0], sxz), __dmul_rn(n[1], syz)), __dmul_rn(n[2], szz));
+  const double Tv[3] = {Tx, Ty, Tz};
+  T0[0] = dot3(n, Tv);
+  T0[1] = dot3(m, Tv);
+  T0[2] = dot3(l, Tv);
+  double G = 0.0;
+  if (t > 0.0 && t < 1.0) G = exp(__dmul_rn(__dsub_rn(t, 1.0), __dsub_rn(t, 1.0)) / __dmul_rn(t, __dsub_rn(t, 2.0)));
+  if (t >= 1.0) G = 1.0;
+  T0[2] = __dadd_rn(T0[2], __dmul_rn(nuc, G));
+}
+
+// f(V) = V + a sigma_n / eta asinh(V / (2 V0) exp(psi / a)) - Phi / eta
+// (src/Interface_Condition.f90:1242-1263)
+__device__ __forceinline__ double rs_f(double V, double Phi, double eta, double sn, double psi, double a) {
+  const double g = asinh(__dmul_rn(__dmul_rn(0.5, V) / kRsV0, exp(psi / a)));
+  return __dsub_rn(__dadd_rn(V, __dmul_rn(__dmul_rn(a, sn) / eta, g)), Phi / eta);
+}
+
+// Regula_Falsi, src/Interface_Condition.f90:1170-1239: bracket [0, Phi/eta],
+// absolute tolerance 1e-12, at most 5000 iterations (the reference's cap)
+__device__ double rs_regula_falsi(double V, double Phi, double eta, double sn, double psi, double a) {
+  const double tol = 1.0e-12;
+  double Vl = 0.0, Vr = Phi / eta;
+  double fv = rs_f(V, Phi, eta, sn, psi, a);
+  double fl = rs_f(Vl, Phi, eta, sn, psi, a);
+  double fr = rs_f(Vr, Phi, eta, sn, psi, a);
+  if (fabs(fv) <= tol) return V;
+  if (fabs(fl) <= tol) return Vl;
+  if (fabs(fr) <= tol) return Vr;
+  double err = 1.0;
+  for (int k = 1; k <= 5000 && err >= tol; ++k) {
+    const double V1 = V;
+    if (__dmul_rn(fv, fl) > tol) {
+      Vl = V;
+      V = __dsub_rn(Vr, __dmul_rn(__dsub_rn(Vr, Vl), fr) / __dsub_rn(fr, fl));
+      fl = fv;
+    } else if (__dmul_rn(fv, fr) > tol) {
+      Vr = V;
+      V = __dsub_rn(Vr, __dmul_rn(__dsub_rn(Vr, Vl), fr) / __dsub_rn(fr, fl));
+      fr = fv;
+    }
+    fv = rs_f(V, Phi, eta, sn, psi, a);
+    err = fabs(__dsub_rn(V, V1));
+  }
+  return V;
+}
+
 // Interface law at one point: P (side-1 hats) and Q (side-2 hats) from the
-// rotated traces U, V.  T0 / fs: this side's prestress and static friction.
+// rotated traces U, V.  T0 / fs: this side's prestress and static friction;
+// rate-and-state: psi the state, ra the direct-effect parameter, *Vrs the
+// solved slip rate (the state-rate input).
 __device__ void iface_law(const IfaceDev &I, const double *U, const double *V, double Z1s, double Z2s, double Z1p,
-                          double Z2p, const double T0[3], double fsk, double slip, double *P, double *Q) {
+                          double Z2p, const double T0[3], double fsk, double slip, double psi, double ra,
+                          double *Vrs, double *P, double *Q) {
   IfacePoint c;
   iface_characteristics(U, V, Z1s, Z2s, Z1p, Z2p, c);
   P[0] = __dsub_rn(c.q[0], c.phi[0]) / Z2p;
   P[3] = c.phi[0];
   Q[0] = __dadd_rn(c.p[0], c.phi[0]) / Z1p;
   Q[3] = c.phi[0];
-  if (I.coupling == WQL3D_IFACE_SLIP_WEAKENING) {
+  if (I.coupling == WQL3D_IFACE_RATE_STATE) {
+    // rate_state_friction + solve('rate-and-state_friction'),
+    // src/Interface_Condition.f90:918-1067, 1095-1168
+    const double T0n = T0[0], T0m = T0[1], T0l = T0[2];
+    const double sigma_n = fmax(0.0, -__dadd_rn(T0n, c.phi[0]));
+    double vm = __dsub_rn(V[1], U[1]), vl = __dsub_rn(V[2], U[2]);
+    const double phi1 = __dadd_rn(T0m, c.phi[1]), phi2 = __dadd_rn(T0l, c.phi[2]);
+    const double Phi = sqrt(__dadd_rn(__dmul_rn(phi1, phi1), __dmul_rn(phi2, phi2)));
+    double Vs = sqrt(__dadd_rn(__dmul_rn(vm, vm), __dmul_rn(vl, vl)));
+    if (Vs > Phi) Vs = __dmul_rn(0.5, Phi) / c.eta_s;
+    Vs = rs_regula_falsi(Vs, Phi, c.eta_s, sigma_n, psi, ra);
+    const double fv = __dmul_rn(__dmul_rn(sigma_n, ra), asinh(__dmul_rn(__dmul_rn(0.5, Vs) / kRsV0, exp(psi / ra))));
+    const double den = __dadd_rn(c.eta_s, fv / Vs);
+    vm = phi1 / den;
+    vl = phi2 / den;
+    const double tm = __dsub_rn(__dsub_rn(phi1, __dmul_rn(c.eta_s, vm)), T0m);
+    const double tl = __dsub_rn(__dsub_rn(phi2, __dmul_rn(c.eta_s, vl)), T0l);
+    Q[1] = __dadd_rn(__dadd_rn(tm, c.p[1]) / Z1s, vm);
+    Q[2] = __dadd_rn(__dadd_rn(tl, c.p[2]) / Z1s, vl);
+    P[1] = __dsub_rn(__dsub_rn(c.q[1], tm) / Z2s, vm);
+    P[2] = __dsub_rn(__dsub_rn(c.q[2], tl) / Z2s, vl);
+    P[4] = tm; P[5] = tl; Q[4] = tm; Q[5] = tl;
+    *Vrs = Vs;
+  } else if (I.coupling == WQL3D_IFACE_SLIP_WEAKENING) {
     // Slip_Weakening_Friction + solve('slip-weakening_friction'),
     // src/Interface_Condition.f90:745-916, 1095-1168
     const double T0n = T0[0], T0m = T0[1], T0l = T0[2];
@@ -373,10 +549,15 @@ __global__ void __launch_bounds__(128) k_iface(Blk<T> b0, Blk<T> b1, IfaceDev I,
     S4 = I.S[3 * n + k];
 #pragma unroll
     for (int c = 0; c < 4; ++c) ds[c] = I.DS[c * n + k];
+    double dw = I.DW[k];
     if (a.flags & F_SCALE) {
 #pragma unroll
       for (int c = 0; c < 4; ++c) ds[c] = __dmul_rn(a.A, ds[c]);
+      dw = __dmul_rn(a.A, dw);
     }
+    // stage time of the interface law (D%t at enforce_bound_iface_conditions)
+    const double ts = a.stage <= 1 ? a.time->t : a.time->t + c_rkC[a.stage - 1] * a.dt;
+    const bool rs = I.coupling == WQL3D_IFACE_RATE_STATE;
     for (int side = 1; side <= 2; ++side) {
       const Blk<T> &b = side == 1 ? b0 : b1;
       const long long p = side == 1 ? p0 : p1;
@@ -400,15 +581,21 @@ __global__ void __launch_bounds__(128) k_iface(Blk<T> b0, Blk<T> b1, IfaceDev I,
       }
       rot_in(u, n3, m3, l3);
       rot_in(v, n3, m3, l3);
-      const double T0[3] = {I.t0[side - 1][k], I.t0[side - 1][n + k], I.t0[side - 1][2 * n + k]};
-      double P[6], Q[6];
-      iface_law(I, u, v, Z1s, Z2s, Z1p, Z2p, T0, I.fs[side - 1][k], S4, P, Q);
+      double T0[3] = {I.t0[side - 1][k], I.t0[side - 1][n + k], I.t0[side - 1][2 * n + k]};
+      if (rs) rs_prestress(ts, I.nuc[side - 1][k], n3, m3, l3, T0);
+      double P[6], Q[6], Vrs = 0.0;
+      iface_law(I, u, v, Z1s, Z2s, Z1p, Z2p, T0, I.fs[side - 1][k], S4, I.W[k], rs ? I.ra[side - 1][k] : 1.0, &Vrs,
+                P, Q);
       const double Vel = sqrt(__dadd_rn(__dmul_rn(__dsub_rn(Q[1], P[1]), __dsub_rn(Q[1], P[1])),
                                         __dmul_rn(__dsub_rn(Q[2], P[2]), __dsub_rn(Q[2], P[2]))));
       if (side == 1 || I.serial) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) ds[c] = __dsub_rn(__dadd_rn(ds[c], Q[c]), P[c]);
         ds[3] = __dadd_rn(ds[3], Vel);
+        // rate of state, TPV101 / TPV102 (src/Interface_Condition.f90:431-436)
+        if (rs)
+          dw = __dsub_rn(__dadd_rn(dw, __dmul_rn(kRsB * kRsV0 / kRsL0, exp(-__dsub_rn(I.W[k], kRsF0) / kRsB))),
+                         __dmul_rn(Vrs, kRsB) / kRsL0);
       }
       if (a.stage == 1 && (side == 1 || I.serial)) {
         // fault outputs, src/Interface_Condition.f90:470-486 and
@@ -447,7 +634,7 @@ __global__ void __launch_bounds__(128) k_iface(Blk<T> b0, Blk<T> b1, IfaceDev I,
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c) I.DS[c * n + k] = ds[c];
-    if (a.flags & F_SCALE) I.DW[k] = __dmul_rn(a.A, I.DW[k]);
+    I.DW[k] = dw;
   }
   if (a.flags & F_UPDATE) {
     // update_fields for the interface (src/iface.f90): S = S + B dt DS
@@ -520,6 +707,10 @@ __global__ void __launch_bounds__(128) k_iface_remote(Blk<T> b, IfaceDev I, Stag
       ds[c] = I.DS[c * n + k];
       if (a.flags & F_SCALE) ds[c] = __dmul_rn(a.A, ds[c]);
     }
+    double dw = I.DW[k];
+    if (a.flags & F_SCALE) dw = __dmul_rn(a.A, dw);
+    const double ts = a.stage <= 1 ? a.time->t : a.time->t + c_rkC[a.stage - 1] * a.dt;
+    const bool rs = I.coupling == WQL3D_IFACE_RATE_STATE;
     const T *B = b.nrm[side == 1 ? 1 : 0];
     double n3[3], m3[3], l3[3];
 #pragma unroll
@@ -539,14 +730,19 @@ __global__ void __launch_bounds__(128) k_iface_remote(Blk<T> b, IfaceDev I, Stag
     }
     rot_in(u, n3, m3, l3);
     rot_in(v, n3, m3, l3);
-    const double T0[3] = {I.t0[side - 1][k], I.t0[side - 1][n + k], I.t0[side - 1][2 * n + k]};
-    double P[6], Q[6];
-    iface_law(I, u, v, Z1s, Z2s, Z1p, Z2p, T0, I.fs[side - 1][k], S4, P, Q);
+    double T0[3] = {I.t0[side - 1][k], I.t0[side - 1][n + k], I.t0[side - 1][2 * n + k]};
+    if (rs) rs_prestress(ts, I.nuc[side - 1][k], n3, m3, l3, T0);
+    double P[6], Q[6], Vrs = 0.0;
+    iface_law(I, u, v, Z1s, Z2s, Z1p, Z2p, T0, I.fs[side - 1][k], S4, I.W[k], rs ? I.ra[side - 1][k] : 1.0, &Vrs, P,
+              Q);
     const double Vel = sqrt(__dadd_rn(__dmul_rn(__dsub_rn(Q[1], P[1]), __dsub_rn(Q[1], P[1])),
                                       __dmul_rn(__dsub_rn(Q[2], P[2]), __dsub_rn(Q[2], P[2]))));
 #pragma unroll
     for (int c = 0; c < 3; ++c) ds[c] = __dsub_rn(__dadd_rn(ds[c], Q[c]), P[c]);
     ds[3] = __dadd_rn(ds[3], Vel);
+    if (rs)
+      dw = __dsub_rn(__dadd_rn(dw, __dmul_rn(kRsB * kRsV0 / kRsL0, exp(-__dsub_rn(I.W[k], kRsF0) / kRsB))),
+                     __dmul_rn(Vrs, kRsB) / kRsL0);
     if (a.stage == 1) {
       const double Tn = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[0];
       const double Tm = I.coupling == WQL3D_IFACE_LOCKED ? 0.0 : T0[1];
@@ -579,7 +775,7 @@ __global__ void __launch_bounds__(128) k_iface_remote(Blk<T> b, IfaceDev I, Stag
     for (int c = 0; c < 9; ++c) out[c * n + k] = (T)sat[c];
 #pragma unroll
     for (int c = 0; c < 4; ++c) I.DS[c * n + k] = ds[c];
-    if (a.flags & F_SCALE) I.DW[k] = __dmul_rn(a.A, I.DW[k]);
+    I.DW[k] = dw;
   }
   if (a.flags & F_UPDATE) {
 #pragma unroll

@@ -34,9 +34,10 @@ STF_CODES = {
 
 RESPONSES = {"elastic": 0, "anelastic-Q4": 1, "anelastic-Q8": 2, "anelastic-fQ8": 3}
 
-COUPLINGS = {"locked": 0, "slip-weakening_friction": 1, "linear_friction": 2}
-# fault prestress / strength: per-point maps, or the reference's TPV5 formulas
-FAULT_PROBLEMS = {None: 0, "maps": 0, "TPV5": 1}
+COUPLINGS = {"locked": 0, "slip-weakening_friction": 1, "linear_friction": 2, "rate-and-state_friction": 3}
+# fault prestress / strength: per-point maps, or the reference's TPV5 formulas;
+# TPV101 / TPV102: prestress and rate-and-state parameters of the reference
+FAULT_PROBLEMS = {None: 0, "maps": 0, "TPV5": 1, "TPV101": 2, "TPV102": 3}
 
 # Kennedy-Carpenter (5,4) low-storage coefficients, src/time_step.f90:53-62
 RK_A = (
