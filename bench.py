@@ -14,7 +14,10 @@ FP32 path with compensated state accumulation is measured on the same
 workload and reported under ``fp32`` with its seismogram error against FP64.
 
 ``--workload cartesian`` times the plain FP64 single Cartesian 101^3 block
-(explosive Ricker source, free surface on the q-min face) instead.
+(explosive Ricker source, free surface on the q-min face) instead;
+``--workload planar`` the two-block 512 x 512 x 384 Cartesian planar
+slip-weakening fault with fQ8 in a von Karman medium (its CPU leg runs a
+128 x 128 x 96 instance of the same workload).
 
 Inputs are synthetic (generated here; there is no dataset).  Prints one JSON
 line (rank 0).  ``--impl reference`` times the CPU restatement of the
@@ -43,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="hill", choices=["hill", "cartesian"])
+    ap.add_argument("--workload", default="hill", choices=["hill", "cartesian", "planar"])
     ap.add_argument("--n", type=int, default=None, help="points per axis (201 hill, 101 cartesian)")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--only-fp32", action="store_true", help="time the FP32 path alone (profiling)")
@@ -51,11 +54,16 @@ def parse():
     return ap.parse_args()
 
 
-def make_problem(args, steps):
-    from waveqlab3d_q_gpu_b200.configs import cartesian_101, hill_two_block_q8
+def make_problem(args, steps, cpu_sample=False):
+    from waveqlab3d_q_gpu_b200.configs import cartesian_101, hill_two_block_q8, planar_fault_fq8
     if args.workload == "cartesian":
         n = args.n or 101
         return cartesian_101(n, steps), f"cartesian-elastic-fp64-{n}^3-traditional6-ricker-10x10rec"
+    if args.workload == "planar":
+        n = 128 if cpu_sample else (args.n or 512)
+        ns = 3 * n // 4
+        return (planar_fault_fq8(n, n, ns, steps=steps),
+                f"planar-fault-2block-{n}x{n}x{ns}-fq8-vonkarman-slipweakening")
     n = args.n or 201
     return (hill_two_block_q8(n, steps=steps),
             f"curvilinear-2block-{n}^3-hill-q8-pml20-locked-ricker3hz-10x10rec")
@@ -188,7 +196,7 @@ def oracle_steps(problem, steps, warmup, budget_s):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    p, name = make_problem(args, max(args.steps, 1))
+    p, name = make_problem(args, max(args.steps, 1), cpu_sample=True)
     value, n, el, cores = oracle_steps(p, args.steps, min(args.warmup, 1), 150.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n,
@@ -339,9 +347,10 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, n, el, cores = oracle_steps(p, 2, 0, 30.0)
+        pc, cname = (p, name) if args.workload != "planar" else make_problem(args, 4, cpu_sample=True)
+        v, n, el, cores = oracle_steps(pc, 2, 0, 30.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{n} RK time step(s) of the same workload in {el:.1f} s (CPU restatement of the "
+               "sample": f"{n} RK time step(s) of {cname} in {el:.1f} s (CPU restatement of the "
                          f"reference solver, OpenMP over z)"}
 
     if rank == 0:

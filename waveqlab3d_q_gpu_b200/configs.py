@@ -166,3 +166,81 @@ def hill_two_block_q8(n: int = 201, h: float = 0.05, npml: int = 20, seed: int =
                 anelastic=an, interface=InterfaceParams(coupling="locked"), w_stride=1)
     p.t_final = steps * p.dt() * (1.0 + 1e-9)
     return p
+
+
+def von_karman_field(shape, h: float, a: float = 1.0, hurst: float = 0.2, std: float = 0.05,
+                     seed: int = 3) -> np.ndarray:
+    """Seeded von Karman random field (3-D power spectrum proportional to
+    (1 + k^2 a^2)^-(H + 3/2), correlation length a, Hurst exponent H) with
+    zero mean and the given standard deviation, on a grid of spacing h."""
+    import scipy.fft as sf
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape).astype(np.float32)
+    W = sf.rfftn(w, workers=-1)
+    del w
+    k = [2.0 * math.pi * sf.fftfreq(n, d=h).astype(np.float32) for n in shape[:-1]]
+    k.append(2.0 * math.pi * sf.rfftfreq(shape[-1], d=h).astype(np.float32))
+    k2 = (k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2)
+    W *= np.power(1.0 + k2 * (a * a), -(hurst + 1.5) / 2.0).astype(np.float32)
+    del k2
+    f = sf.irfftn(W, s=shape, workers=-1)
+    del W
+    f -= f.mean()
+    f *= std / max(float(f.std()), 1e-30)
+    return f.astype(np.float64)
+
+
+def planar_fault_fq8(nq: int = 512, nr: int = 512, ns: int = 384, h: float = 0.1, seed: int = 3,
+                     steps: int = 2000, nrec: int = 4) -> Problem:
+    """Two Cartesian blocks of nq/2 x nr x ns points (q the fault-normal axis)
+    sharing a planar vertical slip-weakening interface.
+
+    * Medium: Vp 6, Vs 3.464, rho 2.67 perturbed by one seeded von Karman
+      field (Hurst 0.2, correlation length 1 km, 5 % standard deviation),
+      continuous across the fault.
+    * fQ8 anelasticity, Q0 = 100 (Qp0 = 200), gamma = 0.6 above 1 Hz.
+    * Linear slip weakening mu_s = 0.70, mu_d = 0.50, Dc = 0.3 m under a
+      normal traction of -120 MPa; shear traction 70 MPa with seeded smooth
+      5 MPa heterogeneity, and a 3 km square nucleation patch at the fault
+      centre loaded to 85 MPa, above the 84 MPa static strength.
+    * Absorbing SATs on the outer faces; nrec x nrec stations on each side of
+      the fault, one grid plane from it.
+    """
+    from .problem import InterfaceParams
+    if nq % 2:
+        raise ValueError("nq must be even: two blocks of nq / 2 points")
+    nb = nq // 2
+    Lq = h * (2 * nb - 2)
+    Lr, Ls = h * (nr - 1), h * (ns - 1)
+    d = von_karman_field((ns, nr, 2 * nb - 1), h, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    # smooth shear heterogeneity on the fault plane (Gaussian filter of white noise)
+    import scipy.ndimage as nd
+    het = nd.gaussian_filter(rng.standard_normal((ns, nr)), sigma=max(1.0, 2.0 / h), mode="wrap")
+    het *= 5.0 / max(float(het.std()), 1e-30)
+    yy = np.arange(nr)[None, :] * h
+    zz = np.arange(ns)[:, None] * h
+    patch = (np.abs(yy - 0.5 * Lr) <= 1.5) & (np.abs(zz - 0.5 * Ls) <= 1.5)
+    tl = np.where(patch, 85.0, 70.0 + het)
+    blocks = []
+    for side in range(2):
+        sl = slice(0, nb) if side == 0 else slice(nb - 1, 2 * nb - 1)
+        db = d[:, :, sl]
+        vp, vs, rho = 6.0 * (1.0 + db), 3.464 * (1.0 + db), 2.67 * (1.0 + db)
+        mat = np.stack([rho * (vp ** 2 - 2 * vs ** 2), rho * vs ** 2, rho])
+        x0 = 0.0 if side == 0 else 0.5 * Lq
+        xr = (0.5 * Lq - h) if side == 0 else (0.5 * Lq + h)
+        ys = np.linspace(0.3 * Lr, 0.7 * Lr, nrec)
+        zs = np.linspace(0.3 * Ls, 0.7 * Ls, nrec)
+        rec = np.array([[xr, y, z] for z in zs for y in ys])
+        blocks.append(Block(nqrs=(nb, nr, ns), aqrs=(x0, 0.0, 0.0), bqrs=(x0 + 0.5 * Lq, Lr, Ls),
+                            rho_s_p=(2.67, 3.464, 6.0), lqrs=(1, 1, 1) if side == 0 else (0, 1, 1),
+                            rqrs=(0, 1, 1) if side == 0 else (1, 1, 1), material=mat, receivers=rec))
+    ip = InterfaceParams(coupling="slip-weakening_friction", fs=0.70, fd=0.50, Dc=0.3,
+                         tau0_n=np.full((ns, nr), -120.0), tau0_m=np.zeros((ns, nr)), tau0_l=tl,
+                         fs_map=np.full((ns, nr), 0.70))
+    an = AnelasticParams(Qs0=100.0, Qp0=200.0, fref=1.0, fmin=0.05, fmax=20.0, gamma=0.6, f_transition=1.0)
+    p = Problem(blocks=blocks, response="anelastic-fQ8", type_of_mesh="cartesian", CFL=0.5, source_order=4,
+                anelastic=an, interface=ip, w_stride=1)
+    p.t_final = steps * p.dt() * (1.0 + 1e-9)
+    return p
