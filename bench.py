@@ -17,7 +17,10 @@ workload and reported under ``fp32`` with its seismogram error against FP64.
 (explosive Ricker source, free surface on the q-min face) instead;
 ``--workload planar`` the two-block 512 x 512 x 384 Cartesian planar
 slip-weakening fault with fQ8 in a von Karman medium (its CPU leg runs a
-128 x 128 x 96 instance of the same workload).
+128 x 128 x 96 instance of the same workload).  ``--workload shots`` runs the batched
+independent shots (48 Cartesian elastic / Q4 problems of 64^3 - 192^3 points,
+seeded media, sources and Ricker frequencies) concurrently on one device in
+FP32, checked against FP64 solves of the same shots.
 
 Inputs are synthetic (generated here; there is no dataset).  Prints one JSON
 line (rank 0).  ``--impl reference`` times the CPU restatement of the
@@ -46,7 +49,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="hill", choices=["hill", "cartesian", "planar"])
+    ap.add_argument("--workload", default="hill", choices=["hill", "cartesian", "planar", "shots"])
+    ap.add_argument("--nshots", type=int, default=48, help="shots of --workload shots")
     ap.add_argument("--n", type=int, default=None, help="points per axis (201 hill, 101 cartesian)")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--only-fp32", action="store_true", help="time the FP32 path alone (profiling)")
@@ -56,6 +60,9 @@ def parse():
 
 def make_problem(args, steps, cpu_sample=False):
     from waveqlab3d_q_gpu_b200.configs import cartesian_101, hill_two_block_q8, planar_fault_fq8
+    if args.workload == "shots":
+        from waveqlab3d_q_gpu_b200.shots import random_shot
+        return random_shot(7000, steps=steps), "batched-shots-one-shot-sample"
     if args.workload == "cartesian":
         n = args.n or 101
         return cartesian_101(n, steps), f"cartesian-elastic-fp64-{n}^3-traditional6-ricker-10x10rec"
@@ -260,10 +267,9 @@ def main():
     from waveqlab3d_q_gpu_b200.domain import Domain
 
     K, W = args.steps, max(args.warmup, 3)
-    p, name = make_problem(args, K + W + 4)
-    npts = sum(b.npoints for b in p.blocks)
-    dt = p.dt()
-    nb = len(p.blocks)
+    p, name = make_problem(args, K + W + 4) if args.workload != "shots" else (None, None)
+    npts = sum(b.npoints for b in p.blocks) if p is not None else 0
+    nb = len(p.blocks) if p is not None else 0
 
     def barrier():
         torch.cuda.synchronize()
@@ -277,6 +283,13 @@ def main():
         t = torch.tensor([x], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.workload == "shots":
+        shots_main(args, rank, world, local, barrier, max_over_ranks)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     peak, peak_kind = load_peaks()
     words = words_per_stage(p)
@@ -299,7 +312,7 @@ def main():
         ms = max_over_ranks(ms)
         seis = g.seismograms(0)
         fields = [g.fields(bi) for bi in range(len(p.blocks))] if "fp32" in precisions else None
-        st_ms = stage_time(g, stream, dt)
+        st_ms = stage_time(g, stream, p.dt())
         w = 8 if prec == "fp64" else 4
         achieved = words * w / (st_ms / 1e3) / 1e9
         results[prec] = {"ms_per_step": ms / K, "value": world * npts * K / (ms / 1e3) / 1e9,
@@ -392,6 +405,109 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def shots_main(args, rank, world, local, barrier, max_over_ranks):
+    """Batched shots: every shot a domain on its own stream, replayed
+    round-robin; the timed region spans all streams (each stream's end event
+    joins the first stream before the stop event)."""
+    import numpy as np
+    import torch
+    from waveqlab3d_q_gpu_b200.shots import ShotBatch, random_shots
+    K, W = args.steps, max(args.warmup, 3)
+    ps = random_shots(args.nshots, seed=7 + rank, steps=K + W + 4)
+    name = f"batched-shots-{args.nshots}x(64..192)^3-elastic-q4-ricker1-4hz"
+    npts = sum(b.npoints for q in ps for b in q.blocks)
+    words = sum(words_per_stage(q) for q in ps)
+    peak, peak_kind = load_peaks()
+
+    def timed(batch, nsteps):
+        streams = [torch.cuda.ExternalStream(d.stream_handle()) for d in batch.domains]
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        for s in streams[1:]:
+            s.wait_event(e0)
+        batch.run(nsteps)
+        for s in streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            streams[0].wait_event(ev)
+        e1.record(streams[0])
+        batch.synchronize()
+        barrier()
+        return e0.elapsed_time(e1)
+
+    res = {}
+    clk = None
+    for prec in ("fp32", "fp64"):
+        batch = ShotBatch(ps, precision=prec, nsteps_hint=W + 2 * K + 4)
+        batch.run(W)
+        batch.synchronize()
+        l0 = sum(d.kernel_launches() for d in batch.domains)
+        clocks = ClockSampler(local) if prec == "fp32" else None
+        if clocks:
+            clocks.start()
+        ms = max_over_ranks(timed(batch, K))
+        if clocks:
+            clk = clocks.stop()
+        launches = sum(d.kernel_launches() for d in batch.domains) - l0
+        res[prec] = {"ms": ms, "value": world * npts * K / (ms / 1e3) / 1e9, "launches": int(launches),
+                     "seis": batch.seismograms(), "bytes": sum(d.device_bytes() for d in batch.domains)}
+        if prec == "fp32":
+            # end to end: each shot's initial fields from pinned host, run, stations back
+            hosts = [torch.zeros((9,) + tuple(q.blocks[0].nqrs[::-1]), dtype=torch.float64,
+                                 pin_memory=True).numpy() for q in ps]
+            for d in batch.domains:
+                d.t = 0.0
+            barrier()
+            t0 = time.perf_counter()
+            for d, hbuf in zip(batch.domains, hosts):
+                d.set_fields(hbuf, 0)
+            batch.run(K)
+            seis_e2e = batch.seismograms()
+            batch.synchronize()
+            barrier()
+            el = time.perf_counter() - t0
+            e2e = {"value": world * npts * K / el / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": sum(h.nbytes for h in hosts) / K,
+                   "d2h_bytes_per_step": sum(x.nbytes for x in seis_e2e) / K,
+                   "what": "set_fields of every shot from pinned host, run K steps, read every shot's stations"}
+        batch.close()
+        del batch
+        torch.cuda.empty_cache()
+    # per-shot station error of FP32 against FP64, over the shots whose
+    # stations the direct wave has reached within the run
+    norms = [float(np.linalg.norm(b[:, :, 1:])) for b in res["fp64"]["seis"]]
+    big = max(norms) if norms else 0.0
+    errs = [float(np.linalg.norm(a[:, :, 1:] - b[:, :, 1:]) / nb)
+            for a, b, nb in zip(res["fp32"]["seis"], res["fp64"]["seis"], norms) if nb > 1e-6 * big]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, n, el, cores = oracle_steps(ps[0], 2, 0, 30.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{n} RK time step(s) of shot 0 ({'x'.join(map(str, ps[0].blocks[0].nqrs))}) in "
+                         f"{el:.1f} s (CPU restatement of the reference solver, OpenMP over z)"}
+    if rank == 0:
+        r = res["fp32"]
+        achieved = words * 4 * 5 * K / (r["ms"] / 1e3) / 1e9
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": r["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": name, "shots": len(ps), "points": npts, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (%.1f GB on the device)" % (r["bytes"] / 1e9)},
+                "e2e": e2e, "gpu_launches": r["launches"],
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                             "kernel": "whole step of every shot (stage kernels, concurrent streams)",
+                             "alg_bytes_per_step": words * 4 * 5},
+                "cpu_baseline": cpu, "clocks": clk,
+                "fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / K},
+                "seismogram_rel_l2_fp32_vs_fp64": {"max": max(errs) if errs else None,
+                                                   "median": float(np.median(errs)) if errs else None,
+                                                   "shots_with_signal": len(errs)}}
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
