@@ -1920,11 +1920,22 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
   cp_async_commit();
   // this group's rates and material, one step ahead
   const int nd = gS ? 6 : 3, d0 = gS ? 3 : 0;
-  T dfo[6], m0 = 0, m1 = 0;
+  // FP32 (compensated) path: the update's global operands -- the compensation
+  // and sigma_zz of group S, which the staged plane does not hold -- also one
+  // plane ahead (FP64 keeps its registers for the stencil)
+  constexpr bool PRE = sizeof(T) == 4;
+  constexpr int NPRE = PRE ? 6 : 1;
+  const bool upd = (a.flags & F_UPDATE) != 0, kahan = PRE && upd && b.FC != nullptr;
+  T dfo[6], m0 = 0, m1 = 0, fco[NPRE], szo = 0;
   if (active) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) dfo[c] = c < nd ? b.DF[(d0 + c) * V + pc] : (T)0;
     if (gS) { m0 = b.M[pc]; m1 = b.M[V + pc]; } else { m0 = b.M[2 * V + pc]; }
+    if constexpr (PRE) {
+#pragma unroll
+      for (int c = 0; c < NPRE; ++c) fco[c] = (kahan && c < nd) ? b.FC[(d0 + c) * V + pc] : (T)0;
+      if (upd && gS) szo = ld(F + 5 * V + pc);
+    }
   }
   const T mx = active ? ld(b.mq + x) : (T)0, my = active ? ld(b.mr + y) : (T)0;
 
@@ -1936,7 +1947,7 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
     __syncthreads();
     if (z + 1 <= ze) fill(z + 1, buf ^ 1);
     cp_async_commit();
-    T qn0 = 0, qn1 = 0, qn2 = 0, dfn[6], mn0 = 0, mn1 = 0;
+    T qn0 = 0, qn1 = 0, qn2 = 0, dfn[6], mn0 = 0, mn1 = 0, fcn[NPRE], szn = 0;
     if (z + 1 <= ze) {
       const long long pn = p + 4 * b.sz;
       qn0 = ld(F + q0 * V + pn); qn1 = ld(F + q1 * V + pn); qn2 = ld(F + q2 * V + pn);
@@ -1944,6 +1955,11 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
 #pragma unroll
         for (int c = 0; c < 6; ++c) dfn[c] = c < nd ? b.DF[(d0 + c) * V + p + b.sz] : (T)0;
         if (gS) { mn0 = b.M[p + b.sz]; mn1 = b.M[V + p + b.sz]; } else { mn0 = b.M[2 * V + p + b.sz]; }
+        if constexpr (PRE) {
+#pragma unroll
+          for (int c = 0; c < NPRE; ++c) fcn[c] = (kahan && c < nd) ? b.FC[(d0 + c) * V + p + b.sz] : (T)0;
+          if (upd && gS) szn = ld(F + 5 * V + p + b.sz);
+        }
       }
     }
     if (active) {
@@ -1978,7 +1994,7 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
             const T dv[3] = {df0, df1, df2}, fv[3] = {f0, f1, f2};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              T comp = b.FC[c * V + p];
+              T comp = PRE ? fco[c % NPRE] : b.FC[c * V + p];
               T yv = Bdt * dv[c] - comp;
               T tv = fv[c] + yv;
               b.FC[c * V + p] = (tv - fv[c]) - yv;
@@ -2021,12 +2037,12 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
         if (a.flags & F_UPDATE) {
           T fc[9];
           fc[3] = P[3][r0][c0]; fc[4] = P[4][r0][c0];
-          fc[5] = ld(F + 5 * V + p);
+          fc[5] = PRE ? szo : ld(F + 5 * V + p);
           fc[6] = P[5][r0][c0]; fc[7] = P[6][r0][c0]; fc[8] = P[7][r0][c0];
           if (b.FC) {
 #pragma unroll
             for (int c = 3; c < 9; ++c) {
-              T comp = b.FC[c * V + p];
+              T comp = PRE ? fco[(c - 3) % NPRE] : b.FC[c * V + p];
               T yv = Bdt * df[c] - comp;
               T tv = fc[c] + yv;
               b.FC[c * V + p] = (tv - fc[c]) - yv;
@@ -2048,6 +2064,11 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
     q[0][6] = qn0; q[1][6] = qn1; q[2][6] = qn2;
 #pragma unroll
     for (int c = 0; c < 6; ++c) dfo[c] = dfn[c];
+    if constexpr (PRE) {
+#pragma unroll
+      for (int c = 0; c < NPRE; ++c) fco[c] = fcn[c];
+      szo = szn;
+    }
     m0 = mn0; m1 = mn1;
   }
   cp_async_wait_all();
