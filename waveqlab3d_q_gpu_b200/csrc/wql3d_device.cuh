@@ -146,6 +146,12 @@ __device__ __forceinline__ long long pidx(const Blk<T> &b, int x, int y, int z) 
 template <typename T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
 
+// L2 prefetch hint: pulls a line the kernel reads late towards the SM
+// without holding a register for it
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // central (interior) SBP row at 1-based i of n points on axis a: 7 <= i <= n-6,
 // or up to an open face of a slab
 template <typename T>
@@ -739,6 +745,11 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
   const long long V = b.vol;
   const T *F = a.cur ? b.F1 : b.F0;
   T *Fn = a.cur ? b.F0 : b.F1;
+  if (b.FC && (a.flags & F_UPDATE)) {
+    // the compensation is read only by the update at the end
+#pragma unroll
+    for (int c = 0; c < 9; ++c) prefetch_l2(b.FC + c * V + p);
+  }
   const double t0 = a.time ? a.time->t : 0.0;
   const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
 
@@ -1484,6 +1495,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
   const T *__restrict__ F = a.cur ? b.F1 : b.F0;
   T *__restrict__ Fn = a.cur ? b.F0 : b.F1;
   T *__restrict__ DFp = b.DF + p;
+  if (a.flags & F_UPDATE) {
+    // F and the compensation are read only by the update at the end
+#pragma unroll
+    for (int c = 0; c < 9; ++c) prefetch_l2(F + c * V + p);
+    if (b.FC) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) prefetch_l2(b.FC + c * V + p);
+    }
+  }
   T df[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
