@@ -1980,6 +1980,14 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
           for (int c = 0; c < NPRE; ++c) fcn[c] = (kahan && c < nd) ? b.FC[(d0 + c) * V + p + b.sz] : (T)0;
           if (upd && gS) szn = ld(F + 5 * V + p + b.sz);
         }
+        if (PRE && RESP != RESP_EL && gS) {
+          // the next plane's memory variables, read late by anelastic_point
+          const int nmv = 6 * b.nmech;
+          for (int c = 0; c < nmv; ++c) {
+            prefetch_l2(b.eta + (long long)c * V + p + b.sz);
+            prefetch_l2(b.deta + (long long)c * V + p + b.sz);
+          }
+        }
       }
     }
     if (active) {
