@@ -1166,6 +1166,23 @@ __device__ __forceinline__ AxisSlab axis_slab(const Blk<T> &b, int x, int y, int
   return s;
 }
 
+// L2 prefetch of the slab-local Q and DQ of this point on one axis (read
+// late, after the rates, by slab_do)
+template <typename T, int AX>
+__device__ __forceinline__ void slab_prefetch(const Blk<T> &b, int x, int y, int z, AxisSlab s) {
+  if (!s.in()) return;
+  constexpr int FL = 2 * AX, FH = 2 * AX + 1;
+  const long long q = s.hi ? slab_index<T, FH>(b, x, y, z) : slab_index<T, FL>(b, x, y, z);
+  const long long PV = s.hi ? b.pvol[FH] : b.pvol[FL];
+  const T *Qp = (s.hi ? b.Q[FH] : b.Q[FL]) + q;
+  const T *DQp = (s.hi ? b.DQ[FH] : b.DQ[FL]) + q;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    prefetch_l2(Qp + c * PV);
+    prefetch_l2(DQp + c * PV);
+  }
+}
+
 // one slab F of one point: scale DQ (F_SCALE), subtract the PML damping terms
 // from the rates and add the auxiliary-field sources to DQ (rhs;
 // src/RHS_Interior.f90:1913-2265, J form; the source terms are re-read from
@@ -1517,6 +1534,11 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     sz = axis_slab<T, 2>(b, x, y, z);
   }
   const bool in_pml = sx.in() || sy.in() || sz.in();
+  if (in_pml) {
+    slab_prefetch<T, 0>(b, x, y, z, sx);
+    slab_prefetch<T, 1>(b, x, y, z, sy);
+    slab_prefetch<T, 2>(b, x, y, z, sz);
+  }
   const bool face_pt = x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz;
   const bool integrate = (a.flags & F_UPDATE) != 0;
   const bool sat = (a.flags & F_SAT) != 0;
