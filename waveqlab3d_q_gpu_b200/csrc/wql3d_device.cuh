@@ -745,10 +745,14 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
   const long long V = b.vol;
   const T *F = a.cur ? b.F1 : b.F0;
   T *Fn = a.cur ? b.F0 : b.F1;
-  if (b.FC && (a.flags & F_UPDATE)) {
-    // the compensation is read only by the update at the end
+  if (a.flags & F_UPDATE) {
+    // F and the compensation are read by the update at the end
 #pragma unroll
-    for (int c = 0; c < 9; ++c) prefetch_l2(b.FC + c * V + p);
+    for (int c = 0; c < 9; ++c) prefetch_l2(F + c * V + p);
+    if (b.FC) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) prefetch_l2(b.FC + c * V + p);
+    }
   }
   const double t0 = a.time ? a.time->t : 0.0;
   const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
