@@ -1,5 +1,5 @@
 """Manufactured solution on the CUDA path: parity with the oracle and the
-convergence order."""
+convergence order (src/mms.f90:136-235)."""
 import numpy as np
 import pytest
 

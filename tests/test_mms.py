@@ -1,4 +1,4 @@
-"""Convergence of the manufactured solution on the oracle.
+"""Convergence of the manufactured solution (src/mms.f90:136-235) on the oracle.
 
 The reference carries the manufactured solution and its derivatives
 (src/mms.f90:136-235) and the exact boundary data of its SATs
