@@ -272,8 +272,13 @@ const char *wql3d_last_error(void);
    result and nonfinite: device-accessible outputs written on `stream`
    (max |array[i]| and 1 if any element is NaN/Inf).  n may not exceed
    WQL3D_NOALLOC_MAX_ELEMENTS (WQL3D_EINVAL otherwise).  The first call on a
-   device looks up the scratch address for that device, so make it before any
-   stream capture.  Calls whose kernels overlap on the GPU share the scratch
+   device looks up the scratch address for that device and loads the
+   library's kernels onto it (with lazy module loading this is when the
+   driver places the scratch and the kernel code on the device), so make it
+   before any stream capture and before the window in which the caller must
+   not allocate; later calls allocate nothing.  The address is cached per
+   device: after cudaDeviceReset the entry point must not be called again in
+   that process.  Calls whose kernels overlap on the GPU share the scratch
    and race; calls ordered on one stream are safe. */
 #define WQL3D_NOALLOC_MAX_ELEMENTS (65536LL * 8192LL)
 int wql3d_max_abs_noalloc(const double *array, int64_t n, double *result, int32_t *nonfinite, void *stream);

@@ -13,11 +13,41 @@ from waveqlab3d_q_gpu_b200.problem import AnelasticParams, Block, Problem, Sourc
 
 PIN_MAX_FIELD = 1.6623128367649574e02
 
+# inputfile/test_elastic_locked_interface_o6.in: published per-block maxima of
+# the final state, 5 digits (CODEX_PUNAKHA_HANDOFF.md:142-143,
+# PHASE2_SCRATCH_MEMORY_AUDIT.md:222-223 of the reference)
+LOCKED_PIN_BLOCK_MAX = (2.0699e03, 1.6389e03)
+
 
 def pin_case(**kw):
     b = Block(nqrs=(41, 41, 41), aqrs=(-2.0, -2.0, -2.0), bqrs=(2.0, 2.0, 2.0), rho_s_p=(2.7, 3.464, 6.0),
               sources=[Source("Cos-Bell", 0.0, 0.05, 0.0, 0.0, 0.0, 0.0, -10.0, 0.0, 0.0, 0.0, 0.0)])
     return Problem(blocks=[b], t_final=0.02, CFL=0.2, source_order=4, source_alpha=0, **kw)
+
+
+def locked_pin_case(**kw):
+    """inputfile/test_elastic_locked_interface_o6.in of the reference: two 41^3
+    Cartesian traditional-6 blocks on [-2,0] x [-1,1]^2 and [0,2] x [-1,1]^2
+    meeting at x = 0 with a locked interface, absorbing SATs on every outer
+    face, rho_s_p = (2.7, 3.464, 6); the tensor_listU row of block 1,
+    'Cos-Bell' 0 0.05 -0.25 0 0 0 -10 0 0 0 0 0, is a Cos-Bell moment
+    (t_init 0.05, M_xx = -0.25, M_xz = -10) at the origin, a node of block 1's
+    interface face, with the 9-point delta (alpha 0); block 2 has no source.
+    CFL 0.2, t_final 0.15: 103 steps, long enough for the wave to cross the
+    interface and reach the outer y / z faces."""
+    src = [Source("Cos-Bell", 0.0, 0.05, -0.25, 0.0, 0.0, 0.0, -10.0, 0.0, 0.0, 0.0, 0.0)]
+    b1 = Block(nqrs=(41, 41, 41), aqrs=(-2.0, -1.0, -1.0), bqrs=(0.0, 1.0, 1.0), rho_s_p=(2.7, 3.464, 6.0),
+               lqrs=(1, 1, 1), rqrs=(0, 1, 1), sources=src)
+    b2 = Block(nqrs=(41, 41, 41), aqrs=(0.0, -1.0, -1.0), bqrs=(2.0, 1.0, 1.0), rho_s_p=(2.7, 3.464, 6.0),
+               lqrs=(0, 1, 1), rqrs=(1, 1, 1))
+    from waveqlab3d_q_gpu_b200.problem import InterfaceParams
+    return Problem(blocks=[b1, b2], t_final=0.15, CFL=0.2, source_order=4, source_alpha=0,
+                   interface=InterfaceParams(coupling="locked"), **kw)
+
+
+def round_sig(v, digits=5):
+    """v rounded to `digits` significant digits (the reference prints ES11.4 / 5 digits)."""
+    return float("%.*E" % (digits - 1, v))
 
 
 def curvilinear_coords(nq, nr, ns, L=(2.0, 2.4, 2.2), amp=0.04, seed=0):

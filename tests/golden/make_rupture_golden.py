@@ -35,4 +35,6 @@ def main(ref: str) -> str:
 
 
 if __name__ == "__main__":
-    print(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_rupture_golden.py <reference project root>")
+    print(main(sys.argv[1]))

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from cases import PIN_MAX_FIELD, pin_case
+from cases import LOCKED_PIN_BLOCK_MAX, PIN_MAX_FIELD, locked_pin_case, pin_case, round_sig
 
 
 def test_elastic_traditional_o6_final_state(oracle_lib):
@@ -15,6 +15,23 @@ def test_elastic_traditional_o6_final_state(oracle_lib):
         mf, me, _ = d.final_state()
         assert abs(mf - PIN_MAX_FIELD) / PIN_MAX_FIELD < 1e-13, "%.16E" % mf
         assert me == 0.0
+
+
+def test_elastic_locked_interface_o6_block_maxima(oracle_lib):
+    """inputfile/test_elastic_locked_interface_o6.in -> block1 max = 2.0699E+03,
+    block2 max = 1.6389E+03 (the 5 printed digits).  103 steps: the wave crosses
+    the locked interface and reaches the absorbing outer faces, so this pins the
+    interface SAT and the physical-boundary SATs that the 6-step pin above never
+    reaches.  Locked coupling does not feed the slip back, so the one-process
+    double slip accumulation does not change the fields."""
+    p = locked_pin_case()
+    assert p.nt() == 103
+    d = oracle_lib.OracleDomain(p)
+    d.run(p.nt())
+    mf, me, bm = d.final_state()
+    assert me == 0.0
+    assert [round_sig(v) for v in bm[:2]] == list(LOCKED_PIN_BLOCK_MAX), bm
+    assert mf == max(bm[:2])
 
 
 def test_dt_and_nt_follow_block_time_step():

@@ -62,6 +62,31 @@ def test_noalloc_max_matches_final_state_twice(wql3d_lib):
     g2.close()
 
 
+def test_noalloc_second_call_allocates_no_device_memory(wql3d_lib):
+    """After the first call on the device (set-up), a call leaves the device's
+    free memory unchanged: inputs and outputs are the caller's, the scratch is
+    the library's static array."""
+    import torch
+    L = wql3d_lib
+    a = torch.linspace(-3.0, 2.0, 1 << 20, dtype=torch.float64, device="cuda")
+    res = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    flag = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+
+    def call():
+        rc = L.wql3d_max_abs_noalloc(C.c_void_p(a.data_ptr()), a.numel(), C.c_void_p(res.data_ptr()),
+                                     C.c_void_p(flag.data_ptr()), None)
+        assert rc == 0, L.wql3d_last_error()
+        torch.cuda.synchronize()
+
+    call()
+    free0, _ = torch.cuda.mem_get_info()
+    call()
+    call()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert float(res.item()) == 3.0 and int(flag.item()) == 0
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch(wql3d_lib):
     L = wql3d_lib
     limit = 65536 * 8192

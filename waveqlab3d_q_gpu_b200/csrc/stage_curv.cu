@@ -1,0 +1,64 @@
+// Curvilinear stage launcher: derivative pass, memory-variable pass, face-SAT
+// pre-pass and point update (or the generic point update where a block's two
+// PML slabs on one axis overlap), compiled once per precision.
+#include "wql3d_stage.cuh"
+
+namespace wql3d {
+
+template <typename T>
+void launch_curv_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
+  const long long npts = (long long)b.nx * b.ny * b.nz;
+  if (a.flags & F_RHS) {
+    const unsigned fgr = (unsigned)((npts + 255) / 256);
+    k_curv_grad<T, 2, 1><<<fgr, 256, 0, c.stream>>>(b, a.cur);
+    ++*c.launches;
+  }
+  // the lean kernel keeps one PML slab per axis: blocks whose two slabs on
+  // an axis overlap (2 npml > n) take the generic update
+  bool overlap = false;
+  const int nax[3] = {b.nx, b.ny, b.nz};
+  for (int ax = 0; ax < 3; ++ax)
+    if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) overlap = true;
+  if (!tuning().lean || overlap) {
+    dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
+    switch (c.response) {
+      case RESP_EL: k_curv_update<T, RESP_EL><<<gr, th, 0, c.stream>>>(b, a); break;
+      case RESP_Q4: k_curv_update<T, RESP_Q4><<<gr, th, 0, c.stream>>>(b, a); break;
+      case RESP_Q8: k_curv_update<T, RESP_Q8><<<gr, th, 0, c.stream>>>(b, a); break;
+      default: k_curv_update<T, RESP_FQ8><<<gr, th, 0, c.stream>>>(b, a); break;
+    }
+    ++*c.launches;
+    return;
+  }
+  if (c.response != RESP_EL && (a.flags & (F_RHS | F_SCALE | F_UPDATE))) {
+    // memory variables first: k_curv_point subtracts their sums; 3 (FP64) or
+    // 8 (FP32) resident blocks of 128 threads
+    constexpr int AMINB = sizeof(T) == 4 ? 8 : 3;
+    const unsigned agr = (unsigned)((npts + 127) / 128);
+    switch (c.response) {
+      case RESP_Q4: k_curv_anelastic<T, RESP_Q4, AMINB><<<agr, 128, 0, c.stream>>>(b, a); break;
+      case RESP_Q8: k_curv_anelastic<T, RESP_Q8, AMINB><<<agr, 128, 0, c.stream>>>(b, a); break;
+      default: k_curv_anelastic<T, RESP_FQ8, AMINB><<<agr, 128, 0, c.stream>>>(b, a); break;
+    }
+    ++*c.launches;
+  }
+  if ((a.flags & F_SAT) && b.foff[6] > 0) {
+    k_curv_face_sat<T><<<(b.foff[6] + 127) / 128, 128, 0, c.stream>>>(b, a.cur);
+    ++*c.launches;
+  }
+  // point update: 256 threads, 2 (FP64) or 4 (FP32) resident blocks
+  constexpr int PMINB = sizeof(T) == 4 ? 4 : 2;
+  const unsigned gr = (unsigned)((npts + 255) / 256);
+  switch (c.response) {
+    case RESP_EL: k_curv_point<T, RESP_EL, 256, PMINB><<<gr, 256, 0, c.stream>>>(b, a); break;
+    case RESP_Q4: k_curv_point<T, RESP_Q4, 256, PMINB><<<gr, 256, 0, c.stream>>>(b, a); break;
+    case RESP_Q8: k_curv_point<T, RESP_Q8, 256, PMINB><<<gr, 256, 0, c.stream>>>(b, a); break;
+    default: k_curv_point<T, RESP_FQ8, 256, PMINB><<<gr, 256, 0, c.stream>>>(b, a); break;
+  }
+  ++*c.launches;
+}
+
+template void launch_curv_stage<WQL3D_REAL>(Blk<WQL3D_REAL> &, const StageCtx &, const StageArgs &);
+int WQL3D_CAT(upload_tables_curv_, WQL3D_TAG)(const ConstTables &t) { return upload_tables_here(t); }
+
+}  // namespace wql3d

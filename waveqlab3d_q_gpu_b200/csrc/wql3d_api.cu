@@ -8,6 +8,7 @@
 #include "wql3d.h"
 #include "wql3d_device.cuh"
 #include "wql3d_iface.cuh"
+#include "wql3d_stage.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -190,6 +191,21 @@ int upload_constants() {
   CK(cudaMemcpyToSymbol(c_rkA, kRkA, sizeof(kRkA)));
   CK(cudaMemcpyToSymbol(c_rkB, kRkB, sizeof(kRkB)));
   CK(cudaMemcpyToSymbol(c_rkC, kRkC, sizeof(kRkC)));
+  // the same tables into each stage-launcher translation unit's constants
+  ConstTables t;
+  memcpy(t.sbp_cnt, cnt, sizeof(cnt));
+  memcpy(t.sbp_idx, idx, sizeof(idx));
+  memcpy(t.sbp_c, kSbpC, sizeof(kSbpC));
+  memcpy(t.rkA, kRkA, sizeof(kRkA));
+  memcpy(t.rkB, kRkB, sizeof(kRkB));
+  memcpy(t.rkC, kRkC, sizeof(kRkC));
+  int (*const up[])(const ConstTables &) = {upload_tables_cart_f64, upload_tables_cart_f32, upload_tables_curv_f64,
+                                            upload_tables_curv_f32, upload_tables_generic_f64,
+                                            upload_tables_generic_f32};
+  for (auto f : up) {
+    const int e = f(t);
+    if (e != 0) return fail(WQL3D_ECUDA, std::string("stage constants: ") + cudaGetErrorString((cudaError_t)e));
+  }
   return WQL3D_OK;
 }
 
@@ -782,194 +798,18 @@ int setup_block(wql3d_domain *d, int bi) {
   return WQL3D_OK;
 }
 
-// tuning of the Cartesian interior kernel (tile height TY, z-chunk length)
-struct Tuning {
-  int ty = 4;
-  int zchunk = 12;
-  int generic = 0;   // 1: every point through the generic per-point kernel
-  int split = 1;     // interior: two warp groups (velocity / stress rates) with register z-queues
-  int lean = 1;      // curvilinear update: k_curv_point (0: generic point update k_curv_update)
-  int curv_lb = -1;  // k_curv_point threads x min blocks: 0 = 256x2, 1 = 128x3, 2 = 256x1, 3 = 256x3,
-                     // 4 = 256x4; -1: 256x2 (FP64), 256x4 (FP32)
-  int grad_minb = 2; // k_curv_grad resident 256-thread blocks per SM (2, 3; 4 with 3-D tiles)
-  int grad_bx = 32;  // k_curv_grad 3-D tile width along x (32, 64)
-  int grad_flat = 1; // k_curv_grad over a flattened point index (0: 3-D tiles)
-  int an_minb = 0;   // k_curv_anelastic: resident 128-thread blocks per SM (3, 4, 6, 8); 0: 3 (FP64), 8 (FP32)
-};
-
-Tuning tuning() {
-  static Tuning t = [] {
-    Tuning r;
-    if (const char *e = getenv("WQL3D_TY")) r.ty = atoi(e) == 8 ? 8 : 4;
-    if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = std::max(1, atoi(e));
-    if (const char *e = getenv("WQL3D_CURV_LB")) r.curv_lb = std::min(4, std::max(0, atoi(e)));
-    if (const char *e = getenv("WQL3D_GRAD_MINB")) r.grad_minb = atoi(e);
-    if (const char *e = getenv("WQL3D_AN_MINB")) r.an_minb = atoi(e);
-    if (const char *e = getenv("WQL3D_GRAD_BX")) r.grad_bx = atoi(e) == 64 ? 64 : 32;
-    if (const char *e = getenv("WQL3D_GRAD_FLAT")) r.grad_flat = atoi(e) != 0;
-    if (const char *e = getenv("WQL3D_KERNEL")) {
-      r.generic = strcmp(e, "generic") == 0;
-      if (strcmp(e, "ring") == 0) r.split = 0;
-      if (strcmp(e, "curv_generic_update") == 0) r.lean = 0;
-    }
-    return r;
-  }();
-  return t;
-}
-
-template <typename T, int RESP>
-void launch_interior_cart(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
-  Tuning tu = tuning();
-  int nxi = b.hi[0] - b.lo[0] + 1, nyi = b.hi[1] - b.lo[1] + 1, nzi = b.hi[2] - b.lo[2] + 1;
-  if (nxi <= 0 || nyi <= 0 || nzi <= 0) return;
-  if (tu.split) {
-    dim3 gr((nxi + 31) / 32, (nyi + tu.ty - 1) / tu.ty, (nzi + tu.zchunk - 1) / tu.zchunk);
-    if (tu.ty == 8) {
-      size_t sm = SplitSmem<T, 8>::bytes;
-      cudaFuncSetAttribute(k_interior_split<T, RESP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_interior_split<T, RESP, 8><<<gr, 512, sm, d->stream>>>(b, a, tu.zchunk);
-    } else {
-      size_t sm = SplitSmem<T, 4>::bytes;
-      cudaFuncSetAttribute(k_interior_split<T, RESP, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_interior_split<T, RESP, 4><<<gr, 256, sm, d->stream>>>(b, a, tu.zchunk);
-    }
-    d->launches++;
-    return;
-  }
-  dim3 gr((nxi + 31) / 32, (nyi + tu.ty - 1) / tu.ty, (nzi + tu.zchunk - 1) / tu.zchunk);
-  if (tu.ty == 8) {
-    size_t sm = InteriorSmem<T, 8>::bytes;
-    cudaFuncSetAttribute(k_interior_cart<T, RESP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_interior_cart<T, RESP, 8><<<gr, dim3(32, 8), sm, d->stream>>>(b, a, tu.zchunk);
-  } else {
-    size_t sm = InteriorSmem<T, 4>::bytes;
-    cudaFuncSetAttribute(k_interior_cart<T, RESP, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_interior_cart<T, RESP, 4><<<gr, dim3(32, 4), sm, d->stream>>>(b, a, tu.zchunk);
-  }
-  d->launches++;
-}
-
-template <typename T, int MESH, int RESP>
-void launch_shell(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
-  long long n = shell_count(b);
-  if (n <= 0) return;
-  unsigned g = (unsigned)((n + 127) / 128);
-  if (b.sep) k_shell<T, MESH, RESP, true><<<g, 128, 0, d->stream>>>(b, a, (int)n);
-  else k_shell<T, MESH, RESP, false><<<g, 128, 0, d->stream>>>(b, a, (int)n);
-  d->launches++;
-}
-
-template <typename T, int MINB>
-void launch_curv_anelastic(wql3d_domain *d, Blk<T> &b, const StageArgs &a, unsigned gr, unsigned th) {
-  switch (d->response) {
-    case 1: k_curv_anelastic<T, RESP_Q4, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 2: k_curv_anelastic<T, RESP_Q8, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-    default: k_curv_anelastic<T, RESP_FQ8, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-  }
-}
-
-template <typename T, int MAXT, int MINB>
-void launch_curv_point(wql3d_domain *d, Blk<T> &b, const StageArgs &a) {
-  const long long npts = (long long)b.nx * b.ny * b.nz;
-  const unsigned th = MAXT, gr = (unsigned)((npts + MAXT - 1) / MAXT);
-  switch (d->response) {
-    case 0: k_curv_point<T, RESP_EL, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 1: k_curv_point<T, RESP_Q4, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 2: k_curv_point<T, RESP_Q8, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-    default: k_curv_point<T, RESP_FQ8, MAXT, MINB><<<gr, th, 0, d->stream>>>(b, a); break;
-  }
-}
-
 template <typename T>
 void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = false) {
   Blk<T> &b = blk<T>(d, bi);
-  int mesh = d->hb[bi].mesh;
-  if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !tuning().generic && !b.mms) {
-    // strict interior (z-marching kernel) + near-boundary shell
-    switch (d->response) {
-      case 0: launch_interior_cart<T, RESP_EL>(d, b, a); launch_shell<T, MESH_CART, RESP_EL>(d, b, a); break;
-      case 1: launch_interior_cart<T, RESP_Q4>(d, b, a); launch_shell<T, MESH_CART, RESP_Q4>(d, b, a); break;
-      case 2: launch_interior_cart<T, RESP_Q8>(d, b, a); launch_shell<T, MESH_CART, RESP_Q8>(d, b, a); break;
-      default: launch_interior_cart<T, RESP_FQ8>(d, b, a); launch_shell<T, MESH_CART, RESP_FQ8>(d, b, a); break;
-    }
-    return;
-  }
-  dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
-  if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !tuning().generic && !b.mms) {
-    // derivative pass, then the point update of every point
-    if (a.flags & F_RHS) {
-      const int gbx = tuning().grad_bx, gby = 256 / gbx / 2;
-      dim3 gth(gbx, gby, 2), ggr((b.nx + gbx - 1) / gbx, (b.ny + gby - 1) / gby, (b.nz + 1) / 2);
-      if (tuning().grad_flat) {
-        const long long np = (long long)b.nx * b.ny * b.nz;
-        const unsigned fgr = (unsigned)((np + 255) / 256);
-        if (tuning().grad_minb == 3)
-          k_curv_grad<T, 3, 1><<<fgr, 256, 0, d->stream>>>(b, a.cur);
-        else
-          k_curv_grad<T, 2, 1><<<fgr, 256, 0, d->stream>>>(b, a.cur);
-      } else {
-        switch (tuning().grad_minb) {
-          case 3: k_curv_grad<T, 3, 0><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
-          case 4: k_curv_grad<T, 4, 0><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
-          default: k_curv_grad<T, 2, 0><<<ggr, gth, 0, d->stream>>>(b, a.cur); break;
-        }
-      }
-      d->launches++;
-    }
-    // the lean kernel keeps one PML slab per axis: blocks whose two slabs on
-    // an axis overlap (2 npml > n) take the generic update
-    bool overlap = false;
-    const int nax[3] = {b.nx, b.ny, b.nz};
-    for (int ax = 0; ax < 3; ++ax)
-      if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) overlap = true;
-    if (tuning().lean && !overlap) {
-      if (d->response != 0 && (a.flags & (F_RHS | F_SCALE | F_UPDATE))) {
-        // memory variables first: k_curv_point subtracts their sums
-        const long long npts = (long long)b.nx * b.ny * b.nz;
-        const unsigned ath = 128, agr = (unsigned)((npts + 127) / 128);
-        const int am = tuning().an_minb > 0 ? tuning().an_minb : (sizeof(T) == 4 ? 8 : 3);
-        switch (am) {
-          case 8: launch_curv_anelastic<T, 8>(d, b, a, agr, ath); break;
-          case 6: launch_curv_anelastic<T, 6>(d, b, a, agr, ath); break;
-          case 4: launch_curv_anelastic<T, 4>(d, b, a, agr, ath); break;
-          default: launch_curv_anelastic<T, 3>(d, b, a, agr, ath); break;
-        }
-        d->launches++;
-      }
-      if ((a.flags & F_SAT) && b.foff[6] > 0) {
-        k_curv_face_sat<T><<<(b.foff[6] + 127) / 128, 128, 0, d->stream>>>(b, a.cur);
-        d->launches++;
-      }
-      const int lb = tuning().curv_lb >= 0 ? tuning().curv_lb : (sizeof(T) == 4 ? 4 : 0);
-      switch (lb) {
-        case 1: launch_curv_point<T, 128, 3>(d, b, a); break;
-        case 2: launch_curv_point<T, 256, 1>(d, b, a); break;
-        case 3: launch_curv_point<T, 256, 3>(d, b, a); break;
-        case 4: launch_curv_point<T, 256, 4>(d, b, a); break;
-        default: launch_curv_point<T, 256, 2>(d, b, a); break;
-      }
-    } else {
-      switch (d->response) {
-        case 0: k_curv_update<T, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
-        case 1: k_curv_update<T, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
-        case 2: k_curv_update<T, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
-        default: k_curv_update<T, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
-      }
-    }
-    d->launches++;
-    return;
-  }
-  switch (d->response * 2 + mesh) {
-    case 0: k_stage<T, MESH_CART, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 1: k_stage<T, MESH_CURV, RESP_EL><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 2: k_stage<T, MESH_CART, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 3: k_stage<T, MESH_CURV, RESP_Q4><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 4: k_stage<T, MESH_CART, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 5: k_stage<T, MESH_CURV, RESP_Q8><<<gr, th, 0, d->stream>>>(b, a); break;
-    case 6: k_stage<T, MESH_CART, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
-    default: k_stage<T, MESH_CURV, RESP_FQ8><<<gr, th, 0, d->stream>>>(b, a); break;
-  }
-  d->launches++;
+  const int mesh = d->hb[bi].mesh;
+  StageCtx c{d->stream, d->response, &d->launches};
+  const bool special = tuning().generic || b.mms;
+  if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !special)
+    launch_cart_stage<T>(b, c, a);
+  else if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !special)
+    launch_curv_stage<T>(b, c, a);
+  else
+    launch_generic_stage<T>(b, mesh, c, a);
 }
 
 template <typename T>

@@ -46,9 +46,8 @@ __constant__ double c_delta9[4][9] = {
     {-0.00728125, -0.028, 0.014875, 0.224, 0.4265625, 0.336, 0.081375, -0.032, -0.01553125},
     {-0.0095625, -0.02990625, 0.03053125, 0.25284375, 0.42890625, 0.30903125, 0.06384375, -0.03196875, -0.01371875}};
 
-// F components staged in the interior kernel's shared plane / z-ring
+// F components staged in the interior kernel's shared plane
 __constant__ int c_smf[8] = {0, 1, 2, 3, 4, 6, 7, 8};
-__constant__ int c_qf[6] = {0, 1, 2, 5, 7, 8};
 
 struct DevSource {
   int type;
@@ -1697,192 +1696,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // ---------------------------------------------------------------------------
 // Strict interior of a Cartesian block, src/JU_xJU_yJU_z6.f90:16426-16636,
-// fused with scale, sources and the RK update.  2.5-D: a block owns a
-// 32 x TY column tile and marches up a z-chunk.  x- and y-derivatives come
-// from a shared-memory plane with 3-point halos, double-buffered and filled
-// one plane ahead with cp.async; z-derivatives from a per-thread ring of
-// eight planes (six fields) in shared memory, also fed one plane ahead.
-// Every F value leaves HBM once per tile; halo re-reads hit L2.
-// smem plane fields: 0 vx 1 vy 2 vz 3 sxx 4 syy 5 sxy 6 sxz 7 syz
-// ring fields:       0 vx 1 vy 2 vz 3 szz 4 sxz 5 syz
-// ---------------------------------------------------------------------------
-template <typename T, int TY>
-struct InteriorSmem {
-  static constexpr int VEC = 16 / (int)sizeof(T);                  // elements per 16-byte cp.async
-  static constexpr int W = ((38 + VEC - 1 + VEC - 1) / VEC) * VEC;  // haloed row, whole chunks
-  static constexpr int H = TY + 6, NT = 32 * TY, RING = 8;
-  static constexpr int CH = W / VEC;                                // chunks per row
-  static constexpr size_t plane_elems = (size_t)8 * H * W;
-  static constexpr size_t bytes = sizeof(T) * (2 * plane_elems + (size_t)RING * 6 * NT);
-};
-
-template <typename T, int RESP, int TY>
-__global__ void __launch_bounds__(32 * TY, (TY == 4 ? 2 : 1)) k_interior_cart(Blk<T> b, StageArgs a, int zchunk) {
-  using SM = InteriorSmem<T, TY>;
-  constexpr int W = SM::W, H = SM::H, NT = SM::NT, RING = SM::RING, VEC = SM::VEC, CH = SM::CH;
-  constexpr int NPOS = H * CH, PPT = (NPOS + NT - 1) / NT;  // 16-byte chunk positions per plane field
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T (*S)[8][H][W] = reinterpret_cast<T (*)[8][H][W]>(smraw);                       // [2] haloed planes
-  T (*Z)[6][NT] = reinterpret_cast<T (*)[6][NT]>(smraw + sizeof(T) * 2 * SM::plane_elems);  // ring
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * 32 + tx;
-  const int x0 = b.lo[0] + blockIdx.x * 32;
-  const int y0 = b.lo[1] + blockIdx.y * TY;
-  const int zs = b.lo[2] + blockIdx.z * zchunk;
-  if (zs > b.hi[2]) return;
-  const int ze = min(zs + zchunk - 1, b.hi[2]);
-  const int x = x0 + tx, y = y0 + ty;
-  const bool active = x <= b.hi[0] && y <= b.hi[1];
-  const long long V = b.vol;
-  const T *F = a.cur ? b.F1 : b.F0;
-  T *Fn = a.cur ? b.F0 : b.F1;
-  const double t0 = a.time ? a.time->t : 0.0;
-  const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
-  const long long pc = pidx(b, min(x, b.nx), min(y, b.ny), zs);  // this thread's column (clamped)
-  // the haloed row starts at x0-3 rounded down to a 16-byte boundary of the
-  // padded row; sh is the resulting shift of x0-3 inside the shared row
-  const long long row0 = pidx(b, x0 - 3, y0 - 3, zs);             // element offset of (x0-3, y0-3, zs)
-  const int sh = (int)(row0 % VEC);
-  const long long base0 = row0 - sh;                               // 16-byte aligned
-  const long long rowlen = b.sy;                                   // padded row length
-  const long long rowstart0 = base0 - ((base0 % b.sz) % b.sy);     // start of the padded row of base0
-  // per-thread chunk positions of one plane field (identical for every plane and field)
-  int soff[PPT];
-  long long goff[PPT];
-  bool gok[PPT];
-#pragma unroll
-  for (int k = 0; k < PPT; ++k) {
-    int pos = tid + k * NT;
-    int yy = pos / CH, ch = pos - yy * CH;
-    soff[k] = yy * W + ch * VEC;
-    goff[k] = (long long)yy * b.sy + (long long)ch * VEC;
-    long long inrow = base0 - rowstart0 + (long long)ch * VEC;     // element index within the padded row
-    gok[k] = pos < NPOS && (y0 - 3 + yy) <= b.ny + 3 && inrow + VEC <= rowlen;
-  }
-  auto fill = [&](int zz, int buf) {
-    const long long plane0 = base0 + (long long)(zz - zs) * b.sz;
-    T *dst = &S[buf][0][0][0];
-#pragma unroll
-    for (int f = 0; f < 8; ++f) {
-      const T *srcf = F + c_smf[f] * V + plane0;
-#pragma unroll
-      for (int k = 0; k < PPT; ++k)
-        if (tid + k * NT < NPOS) cp_async<16>(dst + f * H * W + soff[k], gok[k] ? srcf + goff[k] : F, gok[k]);
-    }
-  };
-  auto ring = [&](int zz) {  // plane zz of the six ring fields into its slot
-    const long long pz = pc + (long long)(zz - zs) * b.sz;
-    const int slot = (zz - zs + 3 + RING) % RING;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) cp_async<sizeof(T)>(&Z[slot][f][tid], F + c_qf[f] * V + pz, true);
-  };
-
-  // prime: planes zs-3 .. zs+3 of the ring, haloed plane zs
-#pragma unroll 1
-  for (int zz = zs - 3; zz <= zs + 3; ++zz) ring(zz);
-  fill(zs, 0);
-  cp_async_commit();
-  T dfo[9], lam = 0, mu = 0, rho = 1;
-  if (active) {
-#pragma unroll
-    for (int c = 0; c < 9; ++c) dfo[c] = b.DF[c * V + pc];
-    lam = b.M[pc]; mu = b.M[V + pc]; rho = b.M[2 * V + pc];
-  }
-  const T mx = active ? ld(b.mq + x) : (T)0, my = active ? ld(b.mr + y) : (T)0;
-
-  for (int z = zs; z <= ze; ++z) {
-    const int i = z - zs;
-    const int buf = i & 1;
-    const long long p = pc + (long long)i * b.sz;
-    cp_async_wait_all();
-    __syncthreads();  // plane z and ring plane z+3 resident; buffer buf^1 free
-    if (z + 1 <= ze) {
-      fill(z + 1, buf ^ 1);
-      ring(z + 4);
-    }
-    cp_async_commit();
-    // next step's rates and material (plain loads, consumed one step later)
-    T dfn[9], lamn = 0, mun = 0, rhon = 1;
-    if (active && z + 1 <= ze) {
-#pragma unroll
-      for (int c = 0; c < 9; ++c) dfn[c] = b.DF[c * V + p + b.sz];
-      lamn = b.M[p + b.sz]; mun = b.M[V + p + b.sz]; rhon = b.M[2 * V + p + b.sz];
-    }
-    if (active) {
-      const T mz = ld(b.ms + z);
-      const int sp1 = (i + 4) % RING, sp2 = (i + 5) % RING, sp3 = (i + 6) % RING;
-      const int sm1 = (i + 2) % RING, sm2 = (i + 1) % RING, sm3 = i % RING, s0 = (i + 3) % RING;
-      const T(*P)[H][W] = S[buf];
-#define DX(f) (((T)0 + (mx * b.cx[0]) * (P[f][ty + 3][tx + sh + 4] - P[f][ty + 3][tx + sh + 2])) + \
-               (mx * b.cx[1]) * (P[f][ty + 3][tx + sh + 5] - P[f][ty + 3][tx + sh + 1])) + \
-              (mx * b.cx[2]) * (P[f][ty + 3][tx + sh + 6] - P[f][ty + 3][tx + sh + 0])
-#define DY(f) (((T)0 + (my * b.cy[0]) * (P[f][ty + 4][tx + sh + 3] - P[f][ty + 2][tx + sh + 3])) + \
-               (my * b.cy[1]) * (P[f][ty + 5][tx + sh + 3] - P[f][ty + 1][tx + sh + 3])) + \
-              (my * b.cy[2]) * (P[f][ty + 6][tx + sh + 3] - P[f][ty + 0][tx + sh + 3])
-#define DZ(k) (((T)0 + (mz * b.cz[0]) * (Z[sp1][k][tid] - Z[sm1][k][tid])) + \
-               (mz * b.cz[1]) * (Z[sp2][k][tid] - Z[sm2][k][tid])) + \
-              (mz * b.cz[2]) * (Z[sp3][k][tid] - Z[sm3][k][tid])
-      T df[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) df[c] = (a.flags & F_SCALE) ? (T)a.A * dfo[c] : dfo[c];
-      const T a1 = (T)1 / rho, a2 = (T)2 * mu + lam, a3 = lam, a4 = mu;
-      const T vxx = DX(0), vyx = DX(1), vzx = DX(2);
-      const T vxy = DY(0), vyy = DY(1), vzy = DY(2);
-      const T vxz = DZ(0), vyz = DZ(1), vzz = DZ(2);
-      df[0] = df[0] + a1 * (DX(3) + DY(5) + DZ(4));
-      df[1] = df[1] + a1 * (DX(5) + DY(4) + DZ(5));
-      df[2] = df[2] + a1 * (DX(6) + DY(7) + DZ(3));
-      df[3] = df[3] + a2 * vxx + a3 * (vyy + vzz);
-      df[4] = df[4] + a2 * vyy + a3 * (vxx + vzz);
-      df[5] = df[5] + a2 * vzz + a3 * (vxx + vyy);
-      df[6] = df[6] + a4 * (vxy + vyx);
-      df[7] = df[7] + a4 * (vxz + vzx);
-      df[8] = df[8] + a4 * (vyz + vzy);
-#undef DX
-#undef DY
-#undef DZ
-      if (RESP != RESP_EL) {
-        T e[6] = {vxx, vyy, vzz, vxy + vyx, vxz + vzx, vyz + vzy};
-        T tr = vxx + vyy + vzz;
-        anelastic_point<T, RESP>(b, a, x, y, z, p, e, tr, df, true);
-      }
-      if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] &&
-          y <= b.sbox[3] && z >= b.sbox[4] && z <= b.sbox[5])
-        add_sources<T, MESH_CART>(b, tst, x, y, z, p, df);
-#pragma unroll
-      for (int c = 0; c < 9; ++c) b.DF[c * V + p] = df[c];
-      if (a.flags & F_UPDATE) {
-        const T Bdt = (T)a.Bdt;
-        T fc[9];
-        fc[0] = Z[s0][0][tid]; fc[1] = Z[s0][1][tid]; fc[2] = Z[s0][2][tid];
-        fc[3] = P[3][ty + 3][tx + sh + 3]; fc[4] = P[4][ty + 3][tx + sh + 3]; fc[5] = Z[s0][3][tid];
-        fc[6] = P[5][ty + 3][tx + sh + 3]; fc[7] = Z[s0][4][tid]; fc[8] = Z[s0][5][tid];
-        if (b.FC) {
-#pragma unroll
-          for (int c = 0; c < 9; ++c) {
-            T comp = b.FC[c * V + p];
-            T yv = Bdt * df[c] - comp;
-            T tv = fc[c] + yv;
-            b.FC[c * V + p] = (tv - fc[c]) - yv;
-            Fn[c * V + p] = tv;
-          }
-        } else {
-#pragma unroll
-          for (int c = 0; c < 9; ++c) Fn[c * V + p] = fc[c] + Bdt * df[c];
-        }
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 9; ++c) dfo[c] = dfn[c];
-    lam = lamn; mu = mun; rho = rhon;
-  }
-  cp_async_wait_all();
-}
-
-// ---------------------------------------------------------------------------
-// Strict interior of a Cartesian block, two warp groups per tile.
-// Same arithmetic as k_interior_cart (src/JU_xJU_yJU_z6.f90:16426-16636), but
-// the nine outputs of a point are split: warps of group V (velocity rates)
+// fused with scale, sources and the RK update; two warp groups per tile.
+// 2.5-D: a block owns a 32 x TY column tile and marches up a z-chunk.  The
+// nine outputs of a point are split: warps of group V (velocity rates)
 // need z-derivatives of s_xz, s_yz, s_zz, warps of group S (stress rates) of
 // v_x, v_y, v_z, so each thread's seven-plane z-queue is three fields and
 // lives in registers.  Shared memory holds only the double-buffered haloed
@@ -2142,12 +1958,12 @@ __global__ void k_update_inplace(Blk<T> b, int cur, double dt) {
 }
 
 // rk_vector_openacc.f90:22-37 / :58-75 equivalents on flat device arrays
-__global__ void k_scale_array(double *r, long long n, double A) {
+static __global__ void k_scale_array(double *r, long long n, double A) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long s = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += s) r[i] = A * r[i];
 }
-__global__ void k_axpy_array(double *x, const double *r, long long n, double dt) {
+static __global__ void k_axpy_array(double *x, const double *r, long long n, double dt) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long s = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += s) x[i] = x[i] + dt * r[i];
@@ -2192,7 +2008,7 @@ __global__ void k_sample(Blk<T> b, int cur, DevTime *tm, int w_stride, int incre
   if (threadIdx.x == 0 && increment) tm->nsamp = s + 1;
 }
 
-__global__ void k_advance(DevTime *tm, double dt) {
+static __global__ void k_advance(DevTime *tm, double dt) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     tm->t = tm->t + c_rkC[5] * dt;
     tm->n = tm->n + 1;

@@ -106,7 +106,13 @@ __global__ void k_noalloc_final(const NoallocSlot *slots, int nblocks, double *r
 }
 
 // Device address of the scratch for the current device, looked up once per
-// device (with that device current) and cached.
+// device (with that device current) and cached.  The same first call also
+// asks for both kernels' attributes: with lazy module loading (the CUDA 12
+// default) that is what puts the kernels' code on the device, so after the
+// first call on a device no later call makes the driver reserve memory.  The
+// cached address belongs to the device's primary context: after a
+// cudaDeviceReset the cached address is stale and the entry point must not be
+// called again in that process.
 int scratch_for_current_device(NoallocSlot **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -124,6 +130,13 @@ int scratch_for_current_device(NoallocSlot **out) {
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       wql3d::set_last_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+      return WQL3D_ECUDA;
+    }
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, k_noalloc_partial);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_noalloc_final);
+    if (e != cudaSuccess) {
+      wql3d::set_last_error(std::string("cudaFuncGetAttributes(noalloc kernels): ") + cudaGetErrorString(e));
       return WQL3D_ECUDA;
     }
     g_scratch_ptr[dev] = (NoallocSlot *)p;

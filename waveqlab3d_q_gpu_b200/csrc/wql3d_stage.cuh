@@ -1,0 +1,87 @@
+// Host-side launchers of the per-block stage kernels, one family per
+// translation unit (stage_cart.cu, stage_curv.cu, stage_generic.cu), each
+// compiled once per precision (WQL3D_REAL = double / float) so that the
+// heavy kernel templates build in parallel.  wql3d_api.cu calls them through
+// the declarations below.
+//
+// __constant__ tables are per translation unit (no relocatable device code):
+// every family TU exports an uploader that copies the SBP rows and the RK
+// coefficients into its own copy.
+#pragma once
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+
+#include "wql3d_device.cuh"
+
+namespace wql3d {
+
+struct ConstTables {
+  int sbp_cnt[6];
+  int sbp_idx[6][8];
+  double sbp_c[2][6][8];
+  double rkA[5], rkB[5], rkC[6];
+};
+
+// per-stage launch context of one block
+struct StageCtx {
+  cudaStream_t stream;
+  int response;       // RESP_*
+  int64_t *launches;  // kernel-launch counter of the owning domain
+};
+
+// tuning switches read once per translation unit from the environment
+struct Tuning {
+  int zchunk = 12;    // z planes per Cartesian interior tile
+  int generic = 0;    // 1: every point through the generic per-point kernel
+  int lean = 1;       // curvilinear update: k_curv_point (0: generic point update k_curv_update)
+};
+
+inline Tuning tuning() {
+  static Tuning t = [] {
+    Tuning r;
+    if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = atoi(e) > 0 ? atoi(e) : 1;
+    if (const char *e = getenv("WQL3D_KERNEL")) {
+      r.generic = strcmp(e, "generic") == 0;
+      if (strcmp(e, "curv_generic_update") == 0) r.lean = 0;
+    }
+    return r;
+  }();
+  return t;
+}
+
+// copy the tables into this translation unit's __constant__ memory
+inline int upload_tables_here(const ConstTables &t) {
+  cudaError_t e = cudaMemcpyToSymbol(c_sbp_cnt, t.sbp_cnt, sizeof(t.sbp_cnt));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_sbp_idx, t.sbp_idx, sizeof(t.sbp_idx));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_sbp_c, t.sbp_c, sizeof(t.sbp_c));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rkA, t.rkA, sizeof(t.rkA));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rkB, t.rkB, sizeof(t.rkB));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rkC, t.rkC, sizeof(t.rkC));
+  return (int)e;
+}
+
+// Cartesian fused stage (flags == F_ALL): strict interior + near-boundary shell
+template <typename T>
+void launch_cart_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a);
+// curvilinear split stage: derivative pass, memory variables, face SATs, point update
+template <typename T>
+void launch_curv_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a);
+// generic per-point kernel (any flags, MMS, both meshes)
+template <typename T>
+void launch_generic_stage(Blk<T> &b, int mesh, const StageCtx &c, const StageArgs &a);
+
+int upload_tables_cart_f64(const ConstTables &t);
+int upload_tables_cart_f32(const ConstTables &t);
+int upload_tables_curv_f64(const ConstTables &t);
+int upload_tables_curv_f32(const ConstTables &t);
+int upload_tables_generic_f64(const ConstTables &t);
+int upload_tables_generic_f32(const ConstTables &t);
+
+}  // namespace wql3d
+
+// one family TU: WQL3D_REAL (double or float) and WQL3D_TAG (f64 or f32) come
+// from the compile line
+#define WQL3D_CAT2(a, b) a##b
+#define WQL3D_CAT(a, b) WQL3D_CAT2(a, b)
