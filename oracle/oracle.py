@@ -32,7 +32,7 @@ class OrcDesc(C.Structure):
         ("src_type", C.POINTER(C.c_int)), ("src_par", C.POINTER(C.c_double)),
         ("nrec", C.c_int), ("rec_xyz", C.POINTER(C.c_double)),
         ("mms", C.c_int), ("mms_nt", C.c_double), ("mms_nx", C.c_double), ("mms_ny", C.c_double),
-        ("mms_nz", C.c_double),
+        ("mms_nz", C.c_double), ("fd", C.c_int),
     ]
 
 
@@ -162,7 +162,8 @@ class OracleDomain:
             if sstr is not None:
                 for k in range(len(sstr)):
                     d.sstr[k], d.pstr[k] = sstr[k], pstr[k]
-            d.tau0 = problem.tau0
+            d.tau0 = problem.sat_penalty()
+            d.fd = problem.fd_operator()
             if problem.mms is not None:
                 d.mms = 1
                 d.mms_nt, d.mms_nx, d.mms_ny, d.mms_nz = (problem.mms.nt, problem.mms.nx, problem.mms.ny,

@@ -83,6 +83,55 @@ static void sbp_stencil(int i, int n, int *cnt, int *idx, double *c) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* Upwind-4 SBP operator pair, src/JU_xJU_yJU_z6.f90:1439-2033 (near         */
+/* boundary) and :17865-18400 (interior).  Velocities take the forward       */
+/* operator D+, stresses the backward operator D-.  Left closure rows 1..4   */
+/* in the order the reference writes their terms; the right closure of each  */
+/* operator is the negated mirror of the other operator's left rows.  The    */
+/* near-boundary routine writes the interior rows with 15-digit literals,    */
+/* the interior routine with exact fractions.                                */
+/* ------------------------------------------------------------------------ */
+static const sbp_row g_up4_plus[4] = {
+    {4, {4, 3, 2, 1}, {0.030612244897959, -0.591836734693878, 2.091836734693878, -1.530612244897959}},
+    {5, {5, 4, 3, 2, 1}, {0.065573770491803, -0.234972677595628, 0.811475409836066, -0.180327868852459,
+                          -0.461748633879781}},
+    {6, {6, 5, 4, 3, 2, 1}, {0.097560975609756, -0.585365853658537, 1.581300813008130, -0.707317073170732,
+                             -0.475609756097561, 0.089430894308943}},
+    {7, {7, 6, 5, 4, 3, 2, 1}, {0.080536912751678, -0.483221476510067, 1.449664429530201, -0.785234899328859,
+                                -0.218120805369128, -0.073825503355705, 0.030201342281879}}};
+static const sbp_row g_up4_minus[4] = {
+    {4, {4, 3, 2, 1}, {-0.091836734693878, -0.224489795918367, 1.724489795918367, -1.408163265306122}},
+    {4, {4, 3, 2, 1}, {0.060109289617486, 0.319672131147541, 0.180327868852459, -0.560109289617486}},
+    {4, {4, 3, 2, 1}, {0.264227642276423, 0.707317073170732, -1.207317073170732, 0.235772357723577}},
+    {5, {5, 4, 3, 2, 1}, {0.241610738255034, 0.785234899328859, -1.305369127516778, 0.288590604026846,
+                          -0.010067114093960}}};
+
+/* Row of D+ (plus = 1) or D- (plus = 0) at 1-based i of n points. */
+static void up4_stencil(int plus, int i, int n, int *cnt, int *idx, double *c) {
+  static const double cp[5] = {-0.250000000000000, -0.833333333333333, 1.500000000000000, -0.500000000000000,
+                               0.083333333333333};
+  static const double cm[5] = {-0.083333333333333, 0.500000000000000, -1.500000000000000, 0.833333333333333,
+                               0.250000000000000};
+  if (i >= 5 && i <= n - 4) {
+    *cnt = 5;
+    for (int k = 0; k < 5; ++k) {
+      idx[k] = plus ? i - 1 + k : i - 3 + k;
+      c[k] = plus ? cp[k] : cm[k];
+    }
+    return;
+  }
+  if (i >= n - 3) { /* negated mirror of the other operator's left row n+1-i */
+    const sbp_row *r = plus ? &g_up4_minus[n - i] : &g_up4_plus[n - i];
+    *cnt = r->n;
+    for (int k = 0; k < r->n; ++k) { idx[k] = n + 1 - r->idx[k]; c[k] = -r->c[k]; }
+    return;
+  }
+  const sbp_row *r = plus ? &g_up4_plus[i - 1] : &g_up4_minus[i - 1];
+  *cnt = r->n;
+  for (int k = 0; k < r->n; ++k) { idx[k] = r->idx[k]; c[k] = r->c[k]; }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Block storage                                                             */
 /* ------------------------------------------------------------------------ */
 typedef struct {
@@ -465,6 +514,35 @@ static void jju6(const oblk *b, int x, int y, int z, double *const X[3], double 
 }
 
 /* ------------------------------------------------------------------------ */
+/* Near-boundary derivative JJU_x4_upwind, src/JU_xJU_yJU_z6.f90:1439-2033:  */
+/* velocities X(p) * D+ u, stresses D-((X J) F) with the reference's         */
+/* association ((c X) J) F of each term.                                     */
+/* ------------------------------------------------------------------------ */
+static void jju_up4(const oblk *b, int x, int y, int z, double *const X[3], double Ju[9]) {
+  double Jd[3][9];
+  int cnt, idx[8];
+  double c[8];
+  const long p0 = ID(b, x, y, z);
+  const int pos[3] = {x, y, z}, nn[3] = {b->nx, b->ny, b->nz};
+  for (int a = 0; a < 3; ++a) {
+    for (int plus = 1; plus >= 0; --plus) {
+      up4_stencil(plus, pos[a], nn[a], &cnt, idx, c);
+      for (int f = plus ? 0 : 3; f < (plus ? 3 : 9); ++f) {
+        double s = 0.0;
+        for (int k = 0; k < cnt; ++k) {
+          const int q[3] = {a == 0 ? idx[k] : x, a == 1 ? idx[k] : y, a == 2 ? idx[k] : z};
+          const long p = ID(b, q[0], q[1], q[2]);
+          const double term = plus ? c[k] * b->F[f][p] : c[k] * X[a][p] * b->J[p] * b->F[f][p];
+          s = (k == 0) ? term : s + term;
+        }
+        Jd[a][f] = plus ? X[a][p0] * s : s;
+      }
+    }
+  }
+  for (int f = 0; f < 9; ++f) Ju[f] = (1.0 / b->hq) * Jd[0][f] + (1.0 / b->hr) * Jd[1][f] + (1.0 / b->hs) * Jd[2][f];
+}
+
+/* ------------------------------------------------------------------------ */
 /* PML: src/RHS_Interior.f90:1846-2265, src/RHS_Interior.f90:2351-2451       */
 /* ------------------------------------------------------------------------ */
 static double pml_d0(void) { return 6.0 / (2.0 * 1.0) * log(1.0 / 1.0e-3); }
@@ -608,16 +686,18 @@ static void anelastic_point(oblk *b, long p, int x, int y, int z, double exx, do
 /* RHS_near_boundaries (traditional branch), src/RHS_Interior.f90:136-281    */
 /* ------------------------------------------------------------------------ */
 static void interior_bounds(const oblk *b, int lo[3], int hi[3]) {
-  /* src/RHS_Interior.f90:199-214, src/JU_xJU_yJU_z6.f90:16158-16173 */
-  int ix = 6, iy = 6, iz = 6, fx = 6, fy = 6, fz = 6;
+  /* src/RHS_Interior.f90:199-214, src/JU_xJU_yJU_z6.f90:16158-16173; the
+     upwind-4 width is 4 (src/JU_xJU_yJU_z6.f90:17915-17931) */
+  const int w = b->d.fd == ORC_FD_UPWIND4 ? 4 : 6;
+  int ix = w, iy = w, iz = w, fx = w, fy = w, fz = w;
   const int *pm = b->d.pml;
   int np = b->d.npml;
-  if (pm[4]) iz = np > 6 ? np : 6;
-  if (pm[5]) fz = np > 6 ? np : 6;
-  if (pm[2]) iy = np > 6 ? np : 6;
-  if (pm[3]) fy = np > 6 ? np : 6;
-  if (pm[0]) ix = np > 6 ? np : 6;
-  if (pm[1]) fx = np > 6 ? np : 6;
+  if (pm[4]) iz = np > w ? np : w;
+  if (pm[5]) fz = np > w ? np : w;
+  if (pm[2]) iy = np > w ? np : w;
+  if (pm[3]) fy = np > w ? np : w;
+  if (pm[0]) ix = np > w ? np : w;
+  if (pm[1]) fx = np > w ? np : w;
   lo[0] = ix + 1; hi[0] = b->nx - fx;
   lo[1] = iy + 1; hi[1] = b->ny - fy;
   lo[2] = iz + 1; hi[2] = b->nz - fz;
@@ -632,9 +712,15 @@ static void rhs_near_boundaries(oblk *b) {
       for (int x = 1; x <= b->nx; ++x) {
         if ((lo[2] <= z && z <= hi[2]) && (lo[1] <= y && y <= hi[1]) && (lo[0] <= x && x <= hi[0])) continue;
         double Ux[9], Uy[9], Uz[9], DU[9];
-        jju6(b, x, y, z, b->mx, Ux);
-        jju6(b, x, y, z, b->my, Uy);
-        jju6(b, x, y, z, b->mz, Uz);
+        if (b->d.fd == ORC_FD_UPWIND4) { /* src/RHS_Interior.f90:443-470 */
+          jju_up4(b, x, y, z, b->mx, Ux);
+          jju_up4(b, x, y, z, b->my, Uy);
+          jju_up4(b, x, y, z, b->mz, Uz);
+        } else {
+          jju6(b, x, y, z, b->mx, Ux);
+          jju6(b, x, y, z, b->my, Uy);
+          jju6(b, x, y, z, b->mz, Uz);
+        }
         long p = ID(b, x, y, z);
         double rhoJ_inv = 1.0 / (b->M[2][p] * b->J[p]);
         double lambda2mu = b->M[0][p] + 2.0 * b->M[1][p];
@@ -675,7 +761,97 @@ static void rhs_near_boundaries(oblk *b) {
 /* ------------------------------------------------------------------------ */
 /* Strict interior JJU_x6_interior, src/JU_xJU_yJU_z6.f90:16088-16640        */
 /* ------------------------------------------------------------------------ */
+/* Rates of a strict-interior point from its derivative terms, shared by both
+   interior routines (src/JU_xJU_yJU_z6.f90:16426-16636, :17990-18120). */
+static void interior_rates(oblk *b, long p, int x, int y, int z, int curv, const double DFx[9],
+                           const double DFy[9], const double DFz[9]) {
+  double a1 = curv ? 1.0 / (b->M[2][p] * b->J[p]) : 1.0 / b->M[2][p];
+  double a2 = 2.0 * b->M[1][p] + b->M[0][p];
+  double a3 = b->M[0][p];
+  double a4 = b->M[1][p];
+  b->DF[0][p] = b->DF[0][p] + a1 * (DFx[3] + DFy[6] + DFz[7]);
+  b->DF[1][p] = b->DF[1][p] + a1 * (DFx[6] + DFy[4] + DFz[8]);
+  b->DF[2][p] = b->DF[2][p] + a1 * (DFx[7] + DFy[8] + DFz[5]);
+  b->DF[3][p] = b->DF[3][p] + a2 * DFx[0] + a3 * (DFy[1] + DFz[2]);
+  b->DF[4][p] = b->DF[4][p] + a2 * DFy[1] + a3 * (DFx[0] + DFz[2]);
+  b->DF[5][p] = b->DF[5][p] + a2 * DFz[2] + a3 * (DFx[0] + DFy[1]);
+  b->DF[6][p] = b->DF[6][p] + a4 * (DFy[0] + DFx[1]);
+  b->DF[7][p] = b->DF[7][p] + a4 * (DFz[0] + DFx[2]);
+  b->DF[8][p] = b->DF[8][p] + a4 * (DFz[1] + DFy[2]);
+  if (b->d.response != ORC_ELASTIC) {
+    double tr = DFx[0] + DFy[1] + DFz[2];
+    anelastic_point(b, p, x, y, z, DFx[0], DFy[1], DFz[2], DFy[0] + DFx[1], DFz[0] + DFx[2], DFz[1] + DFy[2], tr,
+                    NULL, 1);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Strict interior JJU_x4_interior_upwind, src/JU_xJU_yJU_z6.f90:17865-18400 */
+/* forward differences (-1/4, -5/6, 3/2, -1/2, 1/12 at offsets -1..3) of the */
+/* velocities, backward (-1/12, 1/2, -3/2, 5/6, 1/4 at -3..1) of the         */
+/* stresses; Cartesian: diagonal metric at the point, 1/rho; curvilinear:    */
+/* metric at the point for the velocities, (F X) J at the taps for stresses. */
+/* ------------------------------------------------------------------------ */
+static void rhs_interior_up4(oblk *b) {
+  int lo[3], hi[3];
+  interior_bounds(b, lo, hi);
+  static const double cf[5] = {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0};
+  static const double cb[5] = {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0};
+  double cfx[5], cfy[5], cfz[5], cbx[5], cby[5], cbz[5];
+  for (int k = 0; k < 5; ++k) {
+    cfx[k] = cf[k] / b->hq; cfy[k] = cf[k] / b->hr; cfz[k] = cf[k] / b->hs;
+    cbx[k] = cb[k] / b->hq; cby[k] = cb[k] / b->hr; cbz[k] = cb[k] / b->hs;
+  }
+  const long sx = 1, sy = b->NX, sz = (long)b->NX * b->NY;
+  const int curv = b->d.mesh == 1;
+#pragma omp parallel for schedule(static)
+  for (int z = lo[2]; z <= hi[2]; ++z)
+    for (int y = lo[1]; y <= hi[1]; ++y)
+      for (int x = lo[0]; x <= hi[0]; ++x) {
+        const long p = ID(b, x, y, z);
+        double DFx[9] = {0}, DFy[9] = {0}, DFz[9] = {0};
+        for (int s = -1; s <= 3; ++s) {
+          const int k = s + 1;
+          const long fx = p + s * sx, fy = p + s * sy, fz = p + s * sz;                  /* forward taps */
+          const long bx = p + (s - 2) * sx, by = p + (s - 2) * sy, bz = p + (s - 2) * sz;  /* backward taps */
+          if (curv) {
+            for (int f = 0; f < 3; ++f) {
+              const double *Ff = b->F[f];
+              DFx[f] = DFx[f] + b->mx[0][p] * cfx[k] * Ff[fx] + b->mx[1][p] * cfy[k] * Ff[fy] + b->mx[2][p] * cfz[k] * Ff[fz];
+              DFy[f] = DFy[f] + b->my[0][p] * cfx[k] * Ff[fx] + b->my[1][p] * cfy[k] * Ff[fy] + b->my[2][p] * cfz[k] * Ff[fz];
+              DFz[f] = DFz[f] + b->mz[0][p] * cfx[k] * Ff[fx] + b->mz[1][p] * cfy[k] * Ff[fy] + b->mz[2][p] * cfz[k] * Ff[fz];
+            }
+            for (int f = 3; f < 9; ++f) {
+              const double *Ff = b->F[f];
+              DFx[f] = DFx[f] + cbx[k] * Ff[bx] * b->mx[0][bx] * b->J[bx] + cby[k] * Ff[by] * b->mx[1][by] * b->J[by] +
+                       cbz[k] * Ff[bz] * b->mx[2][bz] * b->J[bz];
+              DFy[f] = DFy[f] + cbx[k] * Ff[bx] * b->my[0][bx] * b->J[bx] + cby[k] * Ff[by] * b->my[1][by] * b->J[by] +
+                       cbz[k] * Ff[bz] * b->my[2][bz] * b->J[bz];
+              DFz[f] = DFz[f] + cbx[k] * Ff[bx] * b->mz[0][bx] * b->J[bx] + cby[k] * Ff[by] * b->mz[1][by] * b->J[by] +
+                       cbz[k] * Ff[bz] * b->mz[2][bz] * b->J[bz];
+            }
+          } else {
+            for (int f = 0; f < 3; ++f) {
+              DFx[f] = DFx[f] + b->mx[0][p] * cfx[k] * b->F[f][fx];
+              DFy[f] = DFy[f] + b->my[1][p] * cfy[k] * b->F[f][fy];
+              DFz[f] = DFz[f] + b->mz[2][p] * cfz[k] * b->F[f][fz];
+            }
+            for (int f = 3; f < 9; ++f) {
+              DFx[f] = DFx[f] + b->mx[0][p] * cbx[k] * b->F[f][bx];
+              DFy[f] = DFy[f] + b->my[1][p] * cby[k] * b->F[f][by];
+              DFz[f] = DFz[f] + b->mz[2][p] * cbz[k] * b->F[f][bz];
+            }
+          }
+        }
+        interior_rates(b, p, x, y, z, curv, DFx, DFy, DFz);
+      }
+}
+
 static void rhs_interior(oblk *b) {
+  if (b->d.fd == ORC_FD_UPWIND4) {
+    rhs_interior_up4(b);
+    return;
+  }
   int lo[3], hi[3];
   interior_bounds(b, lo, hi);
   static const double c[3] = {0.75, -0.15, 1.0 / 60.0};
@@ -720,24 +896,7 @@ static void rhs_interior(oblk *b) {
               DFz[f] = DFz[f] + b->mz[2][p] * cz[s - 1] * (b->F[f][p + s * sz] - b->F[f][p - s * sz]);
             }
         }
-        double a1 = curv ? 1.0 / (b->M[2][p] * b->J[p]) : 1.0 / b->M[2][p];
-        double a2 = 2.0 * b->M[1][p] + b->M[0][p];
-        double a3 = b->M[0][p];
-        double a4 = b->M[1][p];
-        b->DF[0][p] = b->DF[0][p] + a1 * (DFx[3] + DFy[6] + DFz[7]);
-        b->DF[1][p] = b->DF[1][p] + a1 * (DFx[6] + DFy[4] + DFz[8]);
-        b->DF[2][p] = b->DF[2][p] + a1 * (DFx[7] + DFy[8] + DFz[5]);
-        b->DF[3][p] = b->DF[3][p] + a2 * DFx[0] + a3 * (DFy[1] + DFz[2]);
-        b->DF[4][p] = b->DF[4][p] + a2 * DFy[1] + a3 * (DFx[0] + DFz[2]);
-        b->DF[5][p] = b->DF[5][p] + a2 * DFz[2] + a3 * (DFx[0] + DFy[1]);
-        b->DF[6][p] = b->DF[6][p] + a4 * (DFy[0] + DFx[1]);
-        b->DF[7][p] = b->DF[7][p] + a4 * (DFz[0] + DFx[2]);
-        b->DF[8][p] = b->DF[8][p] + a4 * (DFz[1] + DFy[2]);
-        if (b->d.response != ORC_ELASTIC) {
-          double tr = DFx[0] + DFy[1] + DFz[2];
-          anelastic_point(b, p, x, y, z, DFx[0], DFy[1], DFz[2], DFy[0] + DFx[1], DFz[0] + DFx[2],
-                          DFz[1] + DFy[2], tr, NULL, 1);
-        }
+        interior_rates(b, p, x, y, z, curv, DFx, DFy, DFz);
       }
 }
 

@@ -27,6 +27,7 @@ enum {
 };
 
 /* interface coupling laws, src/Interface_Condition.f90 */
+enum { ORC_FD_TRADITIONAL6 = 0, ORC_FD_UPWIND4 = 1 };
 enum { ORC_IFACE_LOCKED = 0, ORC_IFACE_SLIP_WEAKENING = 1, ORC_IFACE_LINEAR = 2, ORC_IFACE_RATE_STATE = 3 };
 enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1, ORC_FAULT_TPV101 = 2, ORC_FAULT_TPV102 = 3 };
 /* fault outputs, src/domain.f90:782-845 and src/fault_output.f90:73-122; layout [comp][ns][nr] */
@@ -58,6 +59,10 @@ typedef struct {
      exact boundary data in the face SATs when mms != 0 */
   int mms;
   double mms_nt, mms_nx, mms_ny, mms_nz;
+  /* derivative operator (fd_type / order of &problem_list): ORC_FD_TRADITIONAL6
+     or ORC_FD_UPWIND4 (velocities by the forward, stresses by the backward
+     upwind SBP operator, src/JU_xJU_yJU_z6.f90:1439-2033, :17865-18400) */
+  int fd;
 } orc_desc;
 
 typedef struct {

@@ -18,6 +18,11 @@ PIN_MAX_FIELD = 1.6623128367649574e02
 # PHASE2_SCRATCH_MEMORY_AUDIT.md:222-223 of the reference)
 LOCKED_PIN_BLOCK_MAX = (2.0699e03, 1.6389e03)
 
+# inputfile/test_anelastic_Q8_dynamic.in / test_anelastic_Q4_dynamic.in
+# (upwind order 4): published final max|field| and max|memory variable|,
+# 5 digits (ACCELERATOR_RUNTIME.md:176-177, NVHPC_shutdown_regression_fix.md:35-41)
+UPWIND4_PIN = {"anelastic-Q8": (1.8221e02, 1.4544e01), "anelastic-Q4": (1.8221e02, 1.1049e01)}
+
 
 def pin_case(**kw):
     b = Block(nqrs=(41, 41, 41), aqrs=(-2.0, -2.0, -2.0), bqrs=(2.0, 2.0, 2.0), rho_s_p=(2.7, 3.464, 6.0),
@@ -43,6 +48,17 @@ def locked_pin_case(**kw):
     from waveqlab3d_q_gpu_b200.problem import InterfaceParams
     return Problem(blocks=[b1, b2], t_final=0.15, CFL=0.2, source_order=4, source_alpha=0,
                    interface=InterfaceParams(coupling="locked"), **kw)
+
+
+def upwind4_pin_case(response="anelastic-Q8", **kw):
+    """inputfile/test_anelastic_Q8_dynamic.in (and its Q4 twin) of the reference:
+    the 41^3 block, absorbing faces and Cos-Bell M_xz source of ``pin_case``
+    with fd_type = 'upwind', order = 4, CFL 0.25, t_final 0.02 (5 steps) and
+    Qs0 = 100, Qp0 = 50, fref = 1 (default band 0.05-20 Hz)."""
+    b = Block(nqrs=(41, 41, 41), aqrs=(-2.0, -2.0, -2.0), bqrs=(2.0, 2.0, 2.0), rho_s_p=(2.7, 3.464, 6.0),
+              sources=[Source("Cos-Bell", 0.0, 0.05, 0.0, 0.0, 0.0, 0.0, -10.0, 0.0, 0.0, 0.0, 0.0)])
+    return Problem(blocks=[b], response=response, t_final=0.02, CFL=0.25, source_order=4, source_alpha=0,
+                   anelastic=AnelasticParams(Qs0=100.0, Qp0=50.0, fref=1.0), fd_type="upwind", order=4, **kw)
 
 
 def round_sig(v, digits=5):

@@ -2,7 +2,8 @@
 import numpy as np
 import pytest
 
-from cases import LOCKED_PIN_BLOCK_MAX, PIN_MAX_FIELD, locked_pin_case, pin_case, round_sig
+from cases import (LOCKED_PIN_BLOCK_MAX, PIN_MAX_FIELD, UPWIND4_PIN, locked_pin_case, pin_case, round_sig,
+                   upwind4_pin_case)
 
 
 def test_elastic_traditional_o6_final_state(oracle_lib):
@@ -32,6 +33,22 @@ def test_elastic_locked_interface_o6_block_maxima(oracle_lib):
     assert me == 0.0
     assert [round_sig(v) for v in bm[:2]] == list(LOCKED_PIN_BLOCK_MAX), bm
     assert mf == max(bm[:2])
+
+
+@pytest.mark.parametrize("response", ["anelastic-Q8", "anelastic-Q4"])
+def test_anelastic_upwind4_dynamic_final_state(oracle_lib, response):
+    """inputfile/test_anelastic_Q8_dynamic.in -> 1.8221E+02 / 1.4544E+01 and
+    test_anelastic_Q4_dynamic.in -> 1.8221E+02 / 1.1049E+01 (max|field|,
+    max|memory variable|, 5 printed digits).  Upwind order 4 with SAT penalty
+    144/49; the published memory-variable maxima pin the Q4 / Q8 updates."""
+    for f32 in (False, True):
+        p = upwind4_pin_case(response, closure_f32_literal=f32)
+        assert p.nt() == 5 and p.fd_operator() == 1
+        assert abs(p.sat_penalty() - 144.0 / 49.0) < 1e-15
+        d = oracle_lib.OracleDomain(p)
+        d.run(p.nt())
+        mf, me, _ = d.final_state()
+        assert (round_sig(mf), round_sig(me)) == UPWIND4_PIN[response], (mf, me)
 
 
 def test_dt_and_nt_follow_block_time_step():

@@ -5,20 +5,56 @@
 
 namespace wql3d {
 
+// fused stage: face-SAT pre-pass, then one pass over every point with the
+// derivative terms and memory-variable sums in registers; MB resident blocks
+// of 128 threads per SM
+template <typename T, int MB>
+static void launch_fused_mb(Blk<T> &b, const StageCtx &c, const StageArgs &a, unsigned gr) {
+  switch (c.response) {
+    case RESP_EL: k_curv_fused<T, RESP_EL, MB><<<gr, 128, 0, c.stream>>>(b, a); break;
+    case RESP_Q4: k_curv_fused<T, RESP_Q4, MB><<<gr, 128, 0, c.stream>>>(b, a); break;
+    case RESP_Q8: k_curv_fused<T, RESP_Q8, MB><<<gr, 128, 0, c.stream>>>(b, a); break;
+    default: k_curv_fused<T, RESP_FQ8, MB><<<gr, 128, 0, c.stream>>>(b, a); break;
+  }
+}
+
+template <typename T>
+static void launch_curv_fused(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
+  const long long npts = (long long)b.nx * b.ny * b.nz;
+  if ((a.flags & F_SAT) && b.foff[6] > 0) {
+    k_curv_face_sat<T><<<(b.foff[6] + 127) / 128, 128, 0, c.stream>>>(b, a.cur);
+    ++*c.launches;
+  }
+  const unsigned gr = (unsigned)((npts + 127) / 128);
+  const int mb = tuning().fused_minb;
+  if (sizeof(T) == 8) {
+    if (mb == 3) launch_fused_mb<T, 3>(b, c, a, gr);
+    else launch_fused_mb<T, 2>(b, c, a, gr);
+  } else {
+    if (mb == 6) launch_fused_mb<T, 6>(b, c, a, gr);
+    else launch_fused_mb<T, 4>(b, c, a, gr);
+  }
+  ++*c.launches;
+}
+
 template <typename T>
 void launch_curv_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
   const long long npts = (long long)b.nx * b.ny * b.nz;
-  if (a.flags & F_RHS) {
-    const unsigned fgr = (unsigned)((npts + 255) / 256);
-    k_curv_grad<T, 2, 1><<<fgr, 256, 0, c.stream>>>(b, a.cur);
-    ++*c.launches;
-  }
-  // the lean kernel keeps one PML slab per axis: blocks whose two slabs on
+  // the lean kernels keep one PML slab per axis: blocks whose two slabs on
   // an axis overlap (2 npml > n) take the generic update
   bool overlap = false;
   const int nax[3] = {b.nx, b.ny, b.nz};
   for (int ax = 0; ax < 3; ++ax)
     if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) overlap = true;
+  if (tuning().curv_fused && tuning().lean && !overlap) {
+    launch_curv_fused<T>(b, c, a);
+    return;
+  }
+  if (a.flags & F_RHS) {
+    const unsigned fgr = (unsigned)((npts + 255) / 256);
+    k_curv_grad<T, 2, 1><<<fgr, 256, 0, c.stream>>>(b, a.cur);
+    ++*c.launches;
+  }
   if (!tuning().lean || overlap) {
     dim3 th(32, 4, 2), gr((b.nx + 31) / 32, (b.ny + 3) / 4, (b.nz + 1) / 2);
     switch (c.response) {

@@ -1014,27 +1014,15 @@ __global__ void __launch_bounds__(256) k_stage(Blk<T> b, StageArgs a) {
 template <typename T>
 __device__ __forceinline__ bool flat_point(const Blk<T> &b, int &x, int &y, int &z);
 
-// FLAT: one thread per point of a flattened (x fastest) 1-D launch, every lane
-// busy; otherwise 3-D tiles of blockDim points.
-template <typename T, int MINB, int FLAT>
-__global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
-  int x, y, z;
-  if (FLAT) {
-    if (!flat_point(b, x, y, z)) return;
-  } else {
-    x = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    y = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    z = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (x > b.nx || y > b.ny || z > b.nz) return;
-  }
-  const long long p = pidx(b, x, y, z);
+// The 18 derivative terms of one point (layout of G above) into registers.
+template <typename T>
+__device__ __forceinline__ void curv_derivs(const Blk<T> &b, const T *__restrict__ F, int x, int y, int z, long long p,
+                                            T U[9], T S[9]) {
   const long long V = b.vol;
-  const T *F = cur ? b.F1 : b.F0;
   const int pos[3] = {x, y, z};
   const int nn[3] = {b.nx, b.ny, b.nz};
   const long long st[3] = {1, b.sy, b.sz};
   const T ih[3] = {b.ihq, b.ihr, b.ihs};
-  T U[9], S[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) { U[k] = 0; S[k] = 0; }
 #pragma unroll 1
@@ -1080,6 +1068,25 @@ __global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
 #pragma unroll
       for (int f = 0; f < 3; ++f) U[r * 3 + f] = U[r * 3 + f] + h * (xp[r] * sv[f]);
   }
+}
+
+// FLAT: one thread per point of a flattened (x fastest) 1-D launch, every lane
+// busy; otherwise 3-D tiles of blockDim points.
+template <typename T, int MINB, int FLAT>
+__global__ void __launch_bounds__(256, MINB) k_curv_grad(Blk<T> b, int cur) {
+  int x, y, z;
+  if (FLAT) {
+    if (!flat_point(b, x, y, z)) return;
+  } else {
+    x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    z = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (x > b.nx || y > b.ny || z > b.nz) return;
+  }
+  const long long p = pidx(b, x, y, z);
+  const long long V = b.vol;
+  T U[9], S[9];
+  curv_derivs<T>(b, cur ? b.F1 : b.F0, x, y, z, p, U, S);
   T *Gp = b.G + p;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
@@ -1190,9 +1197,23 @@ __device__ __forceinline__ void slab_prefetch(const Blk<T> &b, int x, int y, int
 // from the rates and add the auxiliary-field sources to DQ (rhs;
 // src/RHS_Interior.f90:1913-2265, J form; the source terms are re-read from
 // the derivative scratch Gp), store DQ and integrate Q (integrate)
-template <typename T, int F>
+// derivative terms of one point (G slot k): from the scratch G ...
+template <typename T>
+struct GMem {
+  const T *p;
+  long long V;
+  __device__ __forceinline__ T operator()(int k) const { return p[k * V]; }
+};
+// ... or from registers (the fused stage kernel)
+template <typename T>
+struct GReg {
+  const T *U, *S;
+  __device__ __forceinline__ T operator()(int k) const { return k < 9 ? U[k] : S[k - 9]; }
+};
+
+template <typename T, int F, typename GA>
 __device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int x, int y, int z, bool rhs,
-                                        bool integrate, bool sat, const T *Gp, long long V, T rhoJ_inv,
+                                        bool integrate, bool sat, const GA &G, T rhoJ_inv,
                                         T lambda2mu, T lam, T mu, T J, T df[9]) {
   constexpr int AX = F >> 1;
   const long long q = slab_index<T, F>(b, x, y, z);
@@ -1220,14 +1241,14 @@ __device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int
     // G slots: 0-8 velocity gradients (Ux, Uy, Uz 1:3), 9-17 Ux4 Ux7 Ux8 Uy7 Uy5 Uy9 Uz8 Uz9 Uz6
     T src[9];
     if (AX == 2) {
-      src[0] = Gp[15 * V] / J; src[1] = Gp[16 * V] / J; src[2] = Gp[17 * V] / J; src[3] = 0; src[4] = 0;
-      src[5] = Gp[8 * V]; src[6] = 0; src[7] = Gp[6 * V]; src[8] = Gp[7 * V];
+      src[0] = G(15) / J; src[1] = G(16) / J; src[2] = G(17) / J; src[3] = 0; src[4] = 0;
+      src[5] = G(8); src[6] = 0; src[7] = G(6); src[8] = G(7);
     } else if (AX == 1) {
-      src[0] = Gp[12 * V] / J; src[1] = Gp[13 * V] / J; src[2] = Gp[14 * V] / J; src[3] = 0; src[4] = Gp[4 * V];
-      src[5] = 0; src[6] = Gp[3 * V]; src[7] = 0; src[8] = Gp[5 * V];
+      src[0] = G(12) / J; src[1] = G(13) / J; src[2] = G(14) / J; src[3] = 0; src[4] = G(4);
+      src[5] = 0; src[6] = G(3); src[7] = 0; src[8] = G(5);
     } else {
-      src[0] = Gp[9 * V] / J; src[1] = Gp[10 * V] / J; src[2] = Gp[11 * V] / J; src[3] = Gp[0 * V]; src[4] = 0;
-      src[5] = 0; src[6] = Gp[1 * V]; src[7] = Gp[2 * V]; src[8] = 0;
+      src[0] = G(9) / J; src[1] = G(10) / J; src[2] = G(11) / J; src[3] = G(0); src[4] = 0;
+      src[5] = 0; src[6] = G(1); src[7] = G(2); src[8] = 0;
     }
     const T cfs = (T)1;
 #pragma unroll
@@ -1248,12 +1269,12 @@ __device__ __forceinline__ void slab_do(const Blk<T> &b, const StageArgs &a, int
   }
 }
 
-template <typename T, int AX>
+template <typename T, int AX, typename GA>
 __device__ __forceinline__ void slab_pass(const Blk<T> &b, const StageArgs &a, int x, int y, int z, AxisSlab s,
-                                          bool rhs, bool integrate, bool sat, const T *Gp, long long V, T rhoJ_inv,
+                                          bool rhs, bool integrate, bool sat, const GA &G, T rhoJ_inv,
                                           T lambda2mu, T lam, T mu, T J, T df[9]) {
-  if (s.hi) slab_do<T, 2 * AX + 1>(b, a, x, y, z, rhs, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-  else if (s.lo) slab_do<T, 2 * AX>(b, a, x, y, z, rhs, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+  if (s.hi) slab_do<T, 2 * AX + 1>(b, a, x, y, z, rhs, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
+  else if (s.lo) slab_do<T, 2 * AX>(b, a, x, y, z, rhs, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
 }
 
 // PML strain correction term d * Q[c] of the slab of one axis (0 outside)
@@ -1546,6 +1567,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
   const bool integrate = (a.flags & F_UPDATE) != 0;
   const bool sat = (a.flags & F_SAT) != 0;
   const T *Gp = b.G + p;
+  const GMem<T> G{Gp, V};
   if (a.flags & F_RHS) {
     const T lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
     const T J = ld(b.J + p);
@@ -1573,14 +1595,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
     }
     // PML damping and auxiliary fields, reference slab order z, y, x
     if (in_pml) {
-      slab_pass<T, 2>(b, a, x, y, z, sz, true, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-      slab_pass<T, 1>(b, a, x, y, z, sy, true, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
-      slab_pass<T, 0>(b, a, x, y, z, sx, true, integrate, sat, Gp, V, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 2>(b, a, x, y, z, sz, true, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 1>(b, a, x, y, z, sy, true, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 0>(b, a, x, y, z, sx, true, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
     }
   } else if (in_pml && (a.flags & (F_SCALE | F_UPDATE | F_SAT))) {
-    slab_pass<T, 2>(b, a, x, y, z, sz, false, integrate, sat, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
-    slab_pass<T, 1>(b, a, x, y, z, sy, false, integrate, sat, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
-    slab_pass<T, 0>(b, a, x, y, z, sx, false, integrate, sat, Gp, V, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 2>(b, a, x, y, z, sz, false, integrate, sat, G, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 1>(b, a, x, y, z, sy, false, integrate, sat, G, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    slab_pass<T, 0>(b, a, x, y, z, sx, false, integrate, sat, G, (T)0, (T)0, (T)0, (T)0, (T)1, df);
   }
   if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
       z >= b.sbox[4] && z <= b.sbox[5]) {
@@ -1611,6 +1633,159 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
 #pragma unroll
   for (int c = 0; c < 9; ++c) DFp[c * V] = df[c];
   if (a.flags & F_UPDATE) {
+    const T Bdt = (T)a.Bdt;
+    if (b.FC) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        const T f0 = F[c * V + p];
+        const T comp = b.FC[c * V + p];
+        const T yv = Bdt * df[c] - comp;
+        const T tv = f0 + yv;
+        b.FC[c * V + p] = (tv - f0) - yv;
+        Fn[c * V + p] = tv;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Fn[c * V + p] = F[c * V + p] + Bdt * df[c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused curvilinear stage: the derivative terms of k_curv_grad, the memory
+// variables of k_curv_anelastic and the point update of k_curv_point for one
+// point per thread of a flattened launch, with the 18 derivative terms and
+// the memory-variable sums kept in registers (no scratch G / S6 in HBM).
+// Rate terms: A DF + elastic rates, PML damping (slabs z, y, x), minus the
+// memory-variable sums, sources, face SATs (from the k_curv_face_sat
+// buffers, reference face order), interface SAT; the memory-variable strain
+// rates take the PML correction from Q before this stage's Q update, as in
+// the split passes.
+// ---------------------------------------------------------------------------
+template <typename T, int RESP, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a) {
+  int x, y, z;
+  if (!flat_point(b, x, y, z)) return;
+  const long long p = pidx(b, x, y, z);
+  const long long V = b.vol;
+  const T *__restrict__ F = a.cur ? b.F1 : b.F0;
+  T *__restrict__ Fn = a.cur ? b.F0 : b.F1;
+  T *__restrict__ DFp = b.DF + p;
+  const bool rhs = (a.flags & F_RHS) != 0;
+  const bool integrate = (a.flags & F_UPDATE) != 0;
+  const bool sat = (a.flags & F_SAT) != 0;
+  if (integrate && b.FC) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) prefetch_l2(b.FC + c * V + p);
+  }
+  AxisSlab sx = {false, false}, sy = {false, false}, sz = {false, false};
+  if (b.npml > 0) {
+    sx = axis_slab<T, 0>(b, x, y, z);
+    sy = axis_slab<T, 1>(b, x, y, z);
+    sz = axis_slab<T, 2>(b, x, y, z);
+  }
+  const bool in_pml = sx.in() || sy.in() || sz.in();
+  T U[9], S[9];
+  if (rhs) curv_derivs<T>(b, F, x, y, z, p, U, S);
+  T df[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    const T v = DFp[c * V];
+    df[c] = (a.flags & F_SCALE) ? (T)a.A * v : v;
+  }
+  T lam = 0, mu = 0, J = 1, rhoJ_inv = 0, lambda2mu = 0;
+  if (rhs) {
+    const T rho = b.M[2 * V + p];
+    lam = b.M[p];
+    mu = b.M[V + p];
+    J = ld(b.J + p);
+    rhoJ_inv = (T)1 / (rho * J);
+    lambda2mu = lam + (T)2 * mu;
+    // rates of src/RHS_Interior.f90:238-254 from the derivative terms
+    df[0] = df[0] + (S[0] + S[3] + S[6]) * rhoJ_inv;
+    df[1] = df[1] + (S[1] + S[4] + S[7]) * rhoJ_inv;
+    df[2] = df[2] + (S[2] + S[5] + S[8]) * rhoJ_inv;
+    df[3] = df[3] + (lambda2mu * U[0] + lam * (U[4] + U[8]));
+    df[4] = df[4] + (lambda2mu * U[4] + lam * (U[0] + U[8]));
+    df[5] = df[5] + (lambda2mu * U[8] + lam * (U[0] + U[4]));
+    df[6] = df[6] + mu * (U[3] + U[1]);
+    df[7] = df[7] + mu * (U[6] + U[2]);
+    df[8] = df[8] + mu * (U[7] + U[5]);
+  }
+  // memory-variable strain rates (k_curv_anelastic), PML-corrected from the
+  // slabs' Q before this stage's Q update
+  T e[6] = {0, 0, 0, 0, 0, 0}, tr = 0;
+  if (RESP != RESP_EL && rhs) {
+    e[0] = U[0]; e[1] = U[4]; e[2] = U[8];
+    e[3] = U[3] + U[1]; e[4] = U[6] + U[2]; e[5] = U[7] + U[5];
+    if (in_pml) {
+      T dx, qx3, qx6, qx7, dy, qy4, qy6, qy8, dz, qz5, qz7, qz8;
+      slab_strain<T, 0>(b, x, y, z, sx, 3, 6, 7, dx, qx3, qx6, qx7);
+      slab_strain<T, 1>(b, x, y, z, sy, 4, 6, 8, dy, qy4, qy6, qy8);
+      slab_strain<T, 2>(b, x, y, z, sz, 5, 7, 8, dz, qz5, qz7, qz8);
+      e[0] = e[0] - dx * qx3;
+      e[1] = e[1] - dy * qy4;
+      e[2] = e[2] - dz * qz5;
+      e[3] = e[3] - dx * qx6 - dy * qy6;
+      e[4] = e[4] - dx * qx7 - dz * qz7;
+      e[5] = e[5] - dy * qy8 - dz * qz8;
+      tr = e[0] + e[1] + e[2];
+    } else {
+      tr = U[0] + U[4] + U[8];
+    }
+  }
+  // PML damping and auxiliary fields, reference slab order z, y, x (before
+  // the memory-variable sums here, so the derivative terms die before the
+  // memory-variable stream: a rounding-level reordering of the rate sum)
+  if (in_pml) {
+    const GReg<T> G{U, S};
+    if (rhs) {
+      slab_pass<T, 2>(b, a, x, y, z, sz, true, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 1>(b, a, x, y, z, sy, true, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
+      slab_pass<T, 0>(b, a, x, y, z, sx, true, integrate, sat, G, rhoJ_inv, lambda2mu, lam, mu, J, df);
+    } else if (a.flags & (F_SCALE | F_UPDATE | F_SAT)) {
+      slab_pass<T, 2>(b, a, x, y, z, sz, false, integrate, sat, G, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+      slab_pass<T, 1>(b, a, x, y, z, sy, false, integrate, sat, G, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+      slab_pass<T, 0>(b, a, x, y, z, sx, false, integrate, sat, G, (T)0, (T)0, (T)0, (T)0, (T)1, df);
+    }
+  }
+  if (RESP != RESP_EL) {
+    const T lm = rhs ? lam : b.M[p], mm = rhs ? mu : b.M[V + p];
+    T s6[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    anelastic_lean<T, RESP>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs);
+    if (rhs) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) df[3 + c] = df[3 + c] + s6[3 + c];
+    }
+  }
+  if ((a.flags & F_SOURCE) && b.nsrc > 0 && x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] &&
+      z >= b.sbox[4] && z <= b.sbox[5]) {
+    const double t0 = a.time ? a.time->t : 0.0;
+    const double tst = a.stage <= 1 ? t0 : t0 + c_rkC[a.stage - 1] * a.dt;
+    add_sources<T, MESH_CURV>(b, tst, x, y, z, p, df);
+  }
+  if (sat && (x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz)) {
+    face_sat_add<T, 0>(b, x, y, z, df);
+    face_sat_add<T, 1>(b, x, y, z, df);
+    face_sat_add<T, 2>(b, x, y, z, df);
+    face_sat_add<T, 3>(b, x, y, z, df);
+    face_sat_add<T, 4>(b, x, y, z, df);
+    face_sat_add<T, 5>(b, x, y, z, df);
+  }
+  if (a.flags & F_ISAT) {
+    // interface SAT, src/RHS_Interior.f90:1813-1837: DF(face) -= tau0/hx * (F_x | G_x)
+    const int side = x == 1 ? 0 : (x == b.nx ? 1 : -1);
+    if (side >= 0 && b.isat[side]) {
+      const T pen = b.tau0 / b.hq;
+      const long long fp = (long long)(y - 1) + (long long)b.ny * (z - 1);
+      const long long fn = (long long)b.ny * b.nz;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) df[c] = df[c] - pen * b.isat[side][c * fn + fp];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) DFp[c * V] = df[c];
+  if (integrate) {
     const T Bdt = (T)a.Bdt;
     if (b.FC) {
 #pragma unroll

@@ -197,6 +197,24 @@ class Problem:
     interface: InterfaceParams = field(default_factory=InterfaceParams)
     tau0: float = TAU0_TRADITIONAL6
     mms: Optional[MMSParams] = None
+    # derivative operator of &problem_list: fd_type 'traditional' (order 6)
+    # or 'upwind' (order 4: forward operator on the velocities, backward on
+    # the stresses, src/JU_xJU_yJU_z6.f90:1439-2033)
+    fd_type: str = "traditional"
+    order: int = 6
+
+    def fd_operator(self) -> int:
+        """Operator code of the C descriptors: 0 traditional-6, 1 upwind-4."""
+        if self.fd_type == "traditional" and self.order == 6:
+            return 0
+        if self.fd_type == "upwind" and self.order == 4:
+            return 1
+        raise ValueError("unsupported operator fd_type=%r order=%r" % (self.fd_type, self.order))
+
+    def sat_penalty(self) -> float:
+        """SAT penalty tau0 of the operator, src/block.f90:242-258: 1/0.315949074074074
+        for traditional-6, 144/49 for upwind-4."""
+        return 144.0 / 49.0 if self.fd_operator() == 1 else self.tau0
 
     def dt(self) -> float:
         """Global time step, src/domain.f90:150-171 and src/block.f90:495-510.
