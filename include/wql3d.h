@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define WQL3D_ABI_VERSION 2
+#define WQL3D_ABI_VERSION 3
 
 /* status codes */
 #define WQL3D_OK 0
@@ -54,6 +54,11 @@ extern "C" {
 /* mesh kinds (type_of_mesh) */
 #define WQL3D_MESH_CARTESIAN 0
 #define WQL3D_MESH_CURVILINEAR 1
+
+/* derivative operator (fd_type / order of &problem_list) */
+#define WQL3D_FD_TRADITIONAL6 0       /* traditional 6th-order SBP, src/JU_xJU_yJU_z6.f90:12-809, :16088-16640 */
+#define WQL3D_FD_UPWIND4 1            /* upwind 4th order: forward operator on velocities, backward on stresses,
+                                         src/JU_xJU_yJU_z6.f90:1439-2033, :17865-18400 (SAT tau0 = 144/49) */
 
 /* arithmetic */
 #define WQL3D_FP64 0
@@ -119,6 +124,8 @@ typedef struct wql3d_block_desc {
   /* receivers (stations), src/seismogram.f90:11-492 */
   int32_t nrec;
   const double *rec_xyz;       /* per receiver x y z; nearest node as Find_Coordinates */
+  int32_t fd_operator;         /* WQL3D_FD_*; upwind blocks run the per-point stage kernel and
+                                  are not split into s-slabs */
 } wql3d_block_desc;
 
 /* Whole-run description (the &problem_list subset the hot path needs). */

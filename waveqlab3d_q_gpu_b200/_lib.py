@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libwql3d.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 OK = 0
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENONFINITE", -5: "ESTATE"}
 
@@ -31,6 +31,7 @@ class BlockDesc(C.Structure):
         ("nsrc", C.c_int32), ("src_order", C.c_int32), ("src_alpha", C.c_int32),
         ("src_type", ip), ("src_par", dp),
         ("nrec", C.c_int32), ("rec_xyz", dp),
+        ("fd_operator", C.c_int32),
     ]
 
 

@@ -52,6 +52,24 @@ const int kSbpIdx[6][8] = {{6, 5, 4, 3, 2, 1, 0, 0}, {6, 5, 4, 3, 1, 0, 0, 0}, {
                            {7, 6, 5, 3, 2, 1, 0, 0}, {8, 7, 6, 4, 3, 2, 1, 0}, {9, 8, 7, 5, 4, 3, 2, 1}};
 double kSbpC[2][6][8];
 
+// upwind-4 left closure rows 1..4 of D+ ([0], velocities) and D- ([1],
+// stresses), absolute 1-based tap indices and coefficients in the order of
+// src/JU_xJU_yJU_z6.f90:1488-1570
+const int kUp4Cnt[2][4] = {{4, 5, 6, 7}, {4, 4, 4, 5}};
+const int kUp4Idx[2][4][8] = {{{4, 3, 2, 1}, {5, 4, 3, 2, 1}, {6, 5, 4, 3, 2, 1}, {7, 6, 5, 4, 3, 2, 1}},
+                              {{4, 3, 2, 1}, {4, 3, 2, 1}, {4, 3, 2, 1}, {5, 4, 3, 2, 1}}};
+const double kUp4C[2][4][8] = {
+    {{0.030612244897959, -0.591836734693878, 2.091836734693878, -1.530612244897959},
+     {0.065573770491803, -0.234972677595628, 0.811475409836066, -0.180327868852459, -0.461748633879781},
+     {0.097560975609756, -0.585365853658537, 1.581300813008130, -0.707317073170732, -0.475609756097561,
+      0.089430894308943},
+     {0.080536912751678, -0.483221476510067, 1.449664429530201, -0.785234899328859, -0.218120805369128,
+      -0.073825503355705, 0.030201342281879}},
+    {{-0.091836734693878, -0.224489795918367, 1.724489795918367, -1.408163265306122},
+     {0.060109289617486, 0.319672131147541, 0.180327868852459, -0.560109289617486},
+     {0.264227642276423, 0.707317073170732, -1.207317073170732, 0.235772357723577},
+     {0.241610738255034, 0.785234899328859, -1.305369127516778, 0.288590604026846, -0.010067114093960}}};
+
 void sbp_tables() {
   static bool done = false;
   if (done) return;
@@ -461,11 +479,53 @@ int setup_block(wql3d_domain *d, int bi) {
     b.rowc = drc;
     b.rowo = dro;
   }
-  // strict interior bounds, src/JU_xJU_yJU_z6.f90:16158-16173
+  b.fd = bd.fd_operator;
+  {
+    // upwind-4 closure rows (src/JU_xJU_yJU_z6.f90:1488-1660): D+ left rows
+    // 1..4 and D- left rows 1..4 in the reference's summation order; the right
+    // rows of each operator are the negated mirror of the other's left rows
+    std::vector<double> rc(16 * 8, 0.0);
+    std::vector<int> ro(16 * 8, 0);
+    for (int r = 0; r < 4; ++r)
+      for (int k = 0; k < kUp4Cnt[0][r]; ++k) {
+        rc[r * 8 + k] = kUp4C[0][r][k];                       // D+ left
+        ro[r * 8 + k] = kUp4Idx[0][r][k] - (r + 1);
+        rc[(12 + r) * 8 + k] = -kUp4C[0][r][k];               // D- right (mirror of D+ left)
+        ro[(12 + r) * 8 + k] = (r + 1) - kUp4Idx[0][r][k];
+      }
+    for (int r = 0; r < 4; ++r)
+      for (int k = 0; k < kUp4Cnt[1][r]; ++k) {
+        rc[(8 + r) * 8 + k] = kUp4C[1][r][k];                 // D- left
+        ro[(8 + r) * 8 + k] = kUp4Idx[1][r][k] - (r + 1);
+        rc[(4 + r) * 8 + k] = -kUp4C[1][r][k];                // D+ right (mirror of D- left)
+        ro[(4 + r) * 8 + k] = (r + 1) - kUp4Idx[1][r][k];
+      }
+    double *drc;
+    int *dro;
+    CK(d->mem.get(&drc, rc.size()));
+    CK(d->mem.get(&dro, ro.size()));
+    CK(cudaMemcpyAsync(drc, rc.data(), sizeof(double) * rc.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(dro, ro.data(), sizeof(int) * ro.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    b.urowc = drc;
+    b.urowo = dro;
+    // interior forward / backward coefficients over h (src/JU_xJU_yJU_z6.f90:17885-17889, 17910-17911)
+    const double cf[5] = {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0};
+    const double cb[5] = {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0};
+    const double hh[3] = {1.0 / (double)(h.nq - 1), 1.0 / (double)(h.nr - 1), 1.0 / (double)(nsg - 1)};
+    for (int a = 0; a < 3; ++a)
+      for (int k = 0; k < 5; ++k) {
+        b.ufw[a][k] = (T)(cf[k] / hh[a]);
+        b.ubw[a][k] = (T)(cb[k] / hh[a]);
+      }
+  }
+  // strict interior bounds, src/JU_xJU_yJU_z6.f90:16158-16173 (traditional-6,
+  // width 6) and :17915-17931 (upwind-4, width 4)
   int np = bd.npml;
-  int ix = bd.pml[0] ? std::max(np, 6) : 6, fx = bd.pml[1] ? std::max(np, 6) : 6;
-  int iy = bd.pml[2] ? std::max(np, 6) : 6, fy = bd.pml[3] ? std::max(np, 6) : 6;
-  int iz = bd.pml[4] ? std::max(np, 6) : 6, fz = bd.pml[5] ? std::max(np, 6) : 6;
+  const int w = b.fd == WQL3D_FD_UPWIND4 ? 4 : 6;
+  int ix = bd.pml[0] ? std::max(np, w) : w, fx = bd.pml[1] ? std::max(np, w) : w;
+  int iy = bd.pml[2] ? std::max(np, w) : w, fy = bd.pml[3] ? std::max(np, w) : w;
+  int iz = bd.pml[4] ? std::max(np, w) : w, fz = bd.pml[5] ? std::max(np, w) : w;
   if (b.open_lo[2]) iz = 0;   // open faces: the central row reaches the face
   if (b.open_hi[2]) fz = 0;
   b.lo[0] = ix + 1; b.hi[0] = h.nq - fx;
@@ -684,7 +744,7 @@ int setup_block(wql3d_domain *d, int bi) {
                 else omax = std::max(omax, v);
               }
           }
-      b.sep = omax <= 1e-12 * dmin ? 1 : 0;
+      b.sep = (omax <= 1e-12 * dmin && b.fd == WQL3D_FD_TRADITIONAL6) ? 1 : 0;
     }
   }
 
@@ -803,7 +863,7 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
   Blk<T> &b = blk<T>(d, bi);
   const int mesh = d->hb[bi].mesh;
   StageCtx c{d->stream, d->response, &d->launches};
-  const bool special = tuning().generic || b.mms;
+  const bool special = tuning().generic || b.mms || b.fd != WQL3D_FD_TRADITIONAL6;
   if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !special)
     launch_cart_stage<T>(b, c, a);
   else if (mesh == WQL3D_MESH_CURVILINEAR && b.G && !special)
@@ -1002,6 +1062,13 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     return cleanup(fail(WQL3D_ECUDA, "time init"));
   if (d->mem.get(&d->red, 592) != cudaSuccess || d->mem.get(&d->flag, 1) != cudaSuccess)
     return cleanup(fail(WQL3D_ENOMEM, "reduction scratch"));
+  for (int i = 0; i < desc->nblocks; ++i) {
+    const int fd = desc->block[i].fd_operator;
+    if (fd != WQL3D_FD_TRADITIONAL6 && fd != WQL3D_FD_UPWIND4)
+      return cleanup(fail(WQL3D_EINVAL, "unknown fd_operator"));
+    if (fd != WQL3D_FD_TRADITIONAL6 && desc->slab_ns_global > 0)
+      return cleanup(fail(WQL3D_EINVAL, "upwind blocks are not split into s-slabs"));
+  }
   if (desc->slab_ns_global > 0) {
     // one s-slab of a larger block: open faces carry no boundary condition or PML
     const wql3d_block_desc &b0 = desc->block[0];

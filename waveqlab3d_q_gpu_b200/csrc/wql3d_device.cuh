@@ -90,6 +90,13 @@ struct Blk {
   int sep;              // Cartesian block whose metric is diagonal to roundoff (separable shell)
   const double *rowc;   // closure rows 0..11 (left 1..6, right n..n-5): 8 signed coefficients each
   const int *rowo;      // matching tap offsets relative to the point
+  // derivative operator: 0 traditional-6, 1 upwind-4 (forward D+ on the
+  // velocities, backward D- on the stresses); upwind closure rows 0..15:
+  // D+ left 1..4, D+ right n..n-3, D- left 1..4, D- right n..n-3
+  int fd;
+  const double *urowc;
+  const int *urowo;
+  T ufw[3][5], ubw[3][5];  // upwind-4 interior forward / backward coefficients over h per axis
   // open faces of an s-slab of a larger block (ghost planes hold the
   // neighbour's data): the central row applies up to the face on that axis
   int open_lo[3], open_hi[3];
@@ -698,6 +705,156 @@ __device__ void jju6_all(const Blk<T> &b, const T *F, int x, int y, int z, long 
   }
 }
 
+// Row of the upwind-4 operator D+ (plus) or D- at 1-based i of n points:
+// interior rows with the near-boundary routine's 15-digit literals
+// (src/JU_xJU_yJU_z6.f90:1488-1505), closures from the block's tables.
+template <typename T>
+__device__ __forceinline__ void up4_row(const Blk<T> &b, bool plus, int i, int n, Row &r) {
+  if (i >= 5 && i <= n - 4) {
+    r.cnt = 5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) r.off[k] = plus ? k - 1 : k - 3;
+    if (plus) {
+      r.c[0] = -0.250000000000000; r.c[1] = -0.833333333333333; r.c[2] = 1.500000000000000;
+      r.c[3] = -0.500000000000000; r.c[4] = 0.083333333333333;
+    } else {
+      r.c[0] = -0.083333333333333; r.c[1] = 0.500000000000000; r.c[2] = -1.500000000000000;
+      r.c[3] = 0.833333333333333; r.c[4] = 0.250000000000000;
+    }
+    return;
+  }
+  const int row = (plus ? 0 : 8) + (i <= 4 ? i - 1 : 4 + (n - i));
+  r.cnt = 8;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    r.off[k] = __ldg(b.urowo + row * 8 + k);
+    r.c[k] = __ldg(b.urowc + row * 8 + k);
+  }
+}
+
+// Near-boundary upwind-4 derivatives of all nine fields for the three metric
+// rows, JJU_x4_upwind (src/JU_xJU_yJU_z6.f90:1439-2033): velocities
+// X_r,a(p) * D+_a(u), stresses D-_a(X_r,a J s) with each term associated as
+// ((c X) J) s.
+template <typename T>
+__device__ void jju_up4_all(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T U[3][9]) {
+  const int pos[3] = {x, y, z};
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  const long long st[3] = {1, b.sy, b.sz};
+  const T ih[3] = {b.ihq, b.ihr, b.ihs};
+  const long long V = b.vol;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int f = 0; f < 9; ++f) U[r][f] = 0;
+#pragma unroll 1
+  for (int a = 0; a < 3; ++a) {
+    Row rp, rm;
+    up4_row(b, true, pos[a], nn[a], rp);
+    up4_row(b, false, pos[a], nn[a], rm);
+    T sv[3] = {0, 0, 0};
+    for (int k = 0; k < rp.cnt; ++k) {
+      const T c = (T)rp.c[k];
+      if (c == (T)0) continue;
+      const long long q = p + (long long)rp.off[k] * st[a];
+#pragma unroll
+      for (int f = 0; f < 3; ++f) sv[f] = sv[f] + c * ld(F + f * V + q);
+    }
+    T acc[3][6];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int f = 0; f < 6; ++f) acc[r][f] = 0;
+    for (int k = 0; k < rm.cnt; ++k) {
+      const T c = (T)rm.c[k];
+      if (c == (T)0) continue;
+      const long long q = p + (long long)rm.off[k] * st[a];
+      const T Jq = ld(b.J + q);
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const T cXJ = (c * ld(b.met + (long long)(r * 3 + a) * V + q)) * Jq;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) acc[r][f] = acc[r][f] + cXJ * ld(F + (3 + f) * V + q);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const T Xp = ld(b.met + (long long)(r * 3 + a) * V + p);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) U[r][f] = U[r][f] + ih[a] * (Xp * sv[f]);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) U[r][3 + f] = U[r][3 + f] + ih[a] * acc[r][f];
+    }
+  }
+}
+
+// Strict-interior upwind-4 derivative terms, JJU_x4_interior_upwind
+// (src/JU_xJU_yJU_z6.f90:17865-18400): forward differences of the
+// velocities at offsets -1..3, backward of the stresses at -3..1; Cartesian
+// with the diagonal metric at the point, curvilinear with the metric at the
+// point for the velocities and (s X) J at the taps for the stresses.
+template <typename T, int MESH>
+__device__ __forceinline__ void up4_interior(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T DFx[9],
+                                             T DFy[9], T DFz[9]) {
+  const long long V = b.vol;
+  const long long st[3] = {1, b.sy, b.sz};
+  if (MESH == MESH_CART) {
+    const T mx = ld(b.mq + x), my = ld(b.mr + y), mz = ld(b.ms + z);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const int s = k - 1;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T *Fc = F + c * V;
+        DFx[c] = DFx[c] + mx * b.ufw[0][k] * ld(Fc + p + s * st[0]);
+        DFy[c] = DFy[c] + my * b.ufw[1][k] * ld(Fc + p + s * st[1]);
+        DFz[c] = DFz[c] + mz * b.ufw[2][k] * ld(Fc + p + s * st[2]);
+      }
+#pragma unroll
+      for (int c = 3; c < 9; ++c) {
+        const T *Fc = F + c * V;
+        DFx[c] = DFx[c] + mx * b.ubw[0][k] * ld(Fc + p + (s - 2) * st[0]);
+        DFy[c] = DFy[c] + my * b.ubw[1][k] * ld(Fc + p + (s - 2) * st[1]);
+        DFz[c] = DFz[c] + mz * b.ubw[2][k] * ld(Fc + p + (s - 2) * st[2]);
+      }
+    }
+  } else {
+    T mp[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) mp[k] = ld(b.met + k * V + p);
+#pragma unroll 1
+    for (int k = 0; k < 5; ++k) {
+      const int s = k - 1;
+      const long long q0 = p + s * st[0], q1 = p + s * st[1], q2 = p + s * st[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T *Fc = F + c * V;
+        const T f0 = ld(Fc + q0), f1 = ld(Fc + q1), f2 = ld(Fc + q2);
+        DFx[c] = DFx[c] + mp[0] * b.ufw[0][k] * f0 + mp[1] * b.ufw[1][k] * f1 + mp[2] * b.ufw[2][k] * f2;
+        DFy[c] = DFy[c] + mp[3] * b.ufw[0][k] * f0 + mp[4] * b.ufw[1][k] * f1 + mp[5] * b.ufw[2][k] * f2;
+        DFz[c] = DFz[c] + mp[6] * b.ufw[0][k] * f0 + mp[7] * b.ufw[1][k] * f1 + mp[8] * b.ufw[2][k] * f2;
+      }
+      const long long r0 = p + (s - 2) * st[0], r1 = p + (s - 2) * st[1], r2 = p + (s - 2) * st[2];
+      const T J0 = ld(b.J + r0), J1 = ld(b.J + r1), J2 = ld(b.J + r2);
+      T m0[3], m1[3], m2[3];  // metric row r, q- / r- / s-entry at the backward taps
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        m0[r] = ld(b.met + (r * 3 + 0) * V + r0);
+        m1[r] = ld(b.met + (r * 3 + 1) * V + r1);
+        m2[r] = ld(b.met + (r * 3 + 2) * V + r2);
+      }
+#pragma unroll
+      for (int c = 3; c < 9; ++c) {
+        const T *Fc = F + c * V;
+        const T g0 = b.ubw[0][k] * ld(Fc + r0), g1 = b.ubw[1][k] * ld(Fc + r1), g2 = b.ubw[2][k] * ld(Fc + r2);
+        DFx[c] = DFx[c] + g0 * m0[0] * J0 + g1 * m1[0] * J1 + g2 * m2[0] * J2;
+        DFy[c] = DFy[c] + g0 * m0[1] * J0 + g1 * m1[1] * J1 + g2 * m2[1] * J2;
+        DFz[c] = DFz[c] + g0 * m0[2] * J0 + g1 * m1[2] * J1 + g2 * m2[2] * J2;
+      }
+    }
+  }
+}
+
 // Separable Cartesian near-boundary derivative of all nine fields along one
 // axis: m_a(i) * (1/h_a) * sum_k c_k F(k).  On a Cartesian grid whose metric
 // is diagonal to roundoff, J*X_a is constant along the axis, so this equals
@@ -779,7 +936,9 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
     T DFx[9], DFy[9], DFz[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) { DFx[c] = 0; DFy[c] = 0; DFz[c] = 0; }
-    if (MESH == MESH_CART) {
+    if (b.fd == 1) {
+      up4_interior<T, MESH>(b, F, x, y, z, p, DFx, DFy, DFz);
+    } else if (MESH == MESH_CART) {
       const T mx = ld(b.mq + x), my = ld(b.mr + y), mz = ld(b.ms + z);
 #pragma unroll
       for (int s = 1; s <= 3; ++s) {
@@ -885,7 +1044,8 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
       rhoJ_inv = (T)1 / rho;
     } else {
       T U[3][9];
-      jju6_all<T>(b, F, x, y, z, p, U);
+      if (b.fd == 1) jju_up4_all<T>(b, F, x, y, z, p, U);
+      else jju6_all<T>(b, F, x, y, z, p, U);
 #pragma unroll
       for (int f = 0; f < 9; ++f) { Ux[f] = U[0][f]; Uy[f] = U[1][f]; Uz[f] = U[2][f]; }
       J = ld(b.J + p);

@@ -145,7 +145,8 @@ class Domain:
             bd.npml = int(b.npml)
             for k in range(3):
                 bd.aqrs[k], bd.bqrs[k] = b.aqrs[k], b.bqrs[k]
-            bd.tau0 = problem.tau0
+            bd.tau0 = problem.sat_penalty()
+            bd.fd_operator = problem.fd_operator()
             bd.host_nb = 0
             if problem.type_of_mesh == "curvilinear":
                 if b.coords is None:
