@@ -257,6 +257,8 @@ int wql3d_update_state_array(double *state, const double *rate, int64_t n, doubl
 /* receivers: samples taken at stage 1 before the update (time_step.f90:137),
    out[(sample*nrec + r)*4 + {t, vx, vy, vz}] */
 int wql3d_get_seismograms(wql3d_domain *d, int block, double *out, int32_t *nsamples);
+/* start the station sample ring again at sample 0 (a new run of the same domain) */
+int wql3d_reset_samples(wql3d_domain *d);
 int wql3d_receiver_index(wql3d_domain *d, int block, int32_t *idx);
 
 /* final diagnostics (close_domain): max|F| over all blocks, max|eta|,
@@ -268,6 +270,45 @@ int wql3d_get_stream(wql3d_domain *d, void **stream);                    /* the 
 int wql3d_device_bytes(wql3d_domain *d, int64_t *bytes);
 int wql3d_kernel_launches(wql3d_domain *d, int64_t *launches);
 const char *wql3d_last_error(void);
+
+/* Parameter updates between runs (the inversion loop of an adjoint driver):
+   material lambda, mu, rho of one block (3 components, host_nb 0) and the
+   moment tensors of its sources (nsrc x 6: mxx myy mzz mxy mxz myz). */
+int wql3d_set_material(wql3d_domain *d, int block, const double *M);
+int wql3d_set_moment(wql3d_domain *d, int block, const double *m6);
+
+/* Device-resident field checkpoints (FP64): the current field buffer of a
+   block copied to / from a caller device array of wql3d_field_volume
+   elements (the library's padded layout) on the domain stream. */
+int wql3d_field_volume(wql3d_domain *d, int block, int64_t *elements);
+int wql3d_store_fields(wql3d_domain *d, int block, double *dev_dst);
+int wql3d_load_fields(wql3d_domain *d, int block, const double *dev_src);
+
+/* Discrete adjoint of the elastic RK step.  No counterpart in the reference,
+   which has no adjoint: it serves waveform-misfit gradients with respect to
+   lambda, mu, rho and the sources' moment tensors.  It is the transpose of the
+   stage operator with every point in the conservative near-boundary form of
+   src/JU_xJU_yJU_z6.f90:12-809 (the curvilinear stage itself; rounding-level
+   different from the Cartesian interior form), the face SATs of
+   src/RHS_Interior.f90:1584-1768 and the sources of src/moment_tensor.f90:875-1125,
+   for one FP64 elastic traditional-6 block without PML (WQL3D_EINVAL otherwise).
+   Usage: enable once; reset; then for n = N..1 with the domain's fields set
+   to F_n (the state at the start of step n) and its time to t_n:
+   wql3d_adjoint_step (adjoint of step n: recomputes the five stage inputs
+   and reverses the stages, accumulating the gradients), then
+   wql3d_adjoint_add_receivers with the misfit derivative with respect to
+   sample n (the stage-1 station velocities v(t_n), nrec x 3).  The field
+   adjoint after n = 1 is the misfit derivative with respect to F_1. */
+int wql3d_adjoint_enable(wql3d_domain *d);
+int wql3d_adjoint_reset(wql3d_domain *d);
+int wql3d_adjoint_step(wql3d_domain *d, int n, double dt);
+int wql3d_adjoint_add_receivers(wql3d_domain *d, int block, const double *res);
+/* L^T R and (dL/d(lambda, mu, rho) F)^T R at the current fields, host arrays
+   (R, Fbar: 9 x n; g: 3 x n; host_nb 0) */
+int wql3d_adjoint_rhs(wql3d_domain *d, int block, const double *R, double *Fbar, double *g);
+int wql3d_get_adjoint_fields(wql3d_domain *d, int block, double *Fbar);
+/* accumulated gradients: g_material 3 x n (lambda, mu, rho), g_moment nsrc x 6 */
+int wql3d_get_adjoint_gradient(wql3d_domain *d, int block, double *g_material, double *g_moment);
 
 /* Allocation-free max|v| reduction over a device array.
    No counterpart in the reference: it serves callers that cannot allocate GPU

@@ -77,6 +77,9 @@ def lib() -> C.CDLL:
         L.orc_q4_coefficients.argtypes = [C.c_double, C.c_double, dp, dp]
         L.orc_q8_coefficients.argtypes = [C.c_double, C.c_double, dp, dp]
         L.orc_modulus_correction.argtypes = [C.c_int, dp, dp, C.c_double, C.c_long, dp, dp, dp, dp, dp]
+        L.orc_adjoint_rhs.restype = C.c_int
+        L.orc_adjoint_rhs.argtypes = [vp, C.c_int, dp, dp, dp]
+        L.orc_adjoint_moment.argtypes = [vp, C.c_int, C.c_double, dp, dp]
         _LIB = L
     return _LIB
 
@@ -239,6 +242,74 @@ class OracleDomain:
 
     def stage(self, stage: int, dt: float):
         lib().orc_stage(self.handle, int(stage), float(dt))
+
+    def adjoint_rhs(self, R: np.ndarray, b: int = 0):
+        """Transpose of the elastic right-hand side at the current fields:
+        (L^T R, (dL/d(lambda, mu, rho) F)^T R) as arrays (9, ns, nr, nq) and
+        (3, ns, nr, nq)."""
+        Rr = np.ascontiguousarray(R, dtype=np.float64)
+        Fb = np.zeros(self._shape(b, 9))
+        g = np.zeros(self._shape(b, 3))
+        rc = lib().orc_adjoint_rhs(self.handle, b, _dptr(Rr), _dptr(Fb), _dptr(g))
+        if rc != 0:
+            raise ValueError("the oracle adjoint covers single elastic blocks without PML or interface")
+        return Fb, g
+
+    def misfit_gradient(self, observed: np.ndarray, nsteps: int):
+        """FP64 discrete adjoint of the waveform misfit chi = 1/2 sum_n sum_r
+        |v_r(t_n) - observed[n, r]|^2 over the stage-1 station samples of
+        nsteps steps from rest (one elastic block).  Stores every step's state,
+        recomputes each step's stage inputs, and reverses the stages with
+        adjoint_rhs / adjoint_moment.  Returns (chi, seismograms,
+        d chi / d(lambda, mu, rho) as (3, ns, nr, nq), d chi / dM as (nsrc, 6))."""
+        from waveqlab3d_q_gpu_b200.problem import RK_A, RK_B, RK_C
+        dt = self.problem.dt()
+        shape9 = self._shape(0, 9)
+        t_start = self.t
+        states, seis = [], []
+        ridx = self.receiver_index()
+        for n in range(nsteps):
+            states.append(self.fields())
+            F = states[-1]
+            seis.append(np.stack([F[c][ridx[:, 2] - 1, ridx[:, 1] - 1, ridx[:, 0] - 1] for c in range(3)], axis=1))
+            self.run(1)
+        seis = np.array(seis)
+        res = seis - observed
+        chi = 0.5 * float(np.sum(res * res))
+        Fb = np.zeros(shape9)
+        gmat = np.zeros(self._shape(0, 3))
+        gM = np.zeros((len(self.problem.blocks[0].sources), 6))
+        for n in range(nsteps - 1, -1, -1):
+            tn = t_start + n * dt
+            # stage inputs F^(0..4) of step n
+            self.set_fields(states[n])
+            self.set_rates(np.zeros(shape9))
+            inputs = [states[n]]
+            for st in range(1, 5):
+                self.t = tn + RK_C[st - 1] * dt
+                self.stage(st, dt)
+                inputs.append(self.fields())
+            DFb = np.zeros(shape9)
+            for st in range(5, 0, -1):
+                R = DFb + RK_B[st - 1] * dt * Fb
+                self.set_fields(inputs[st - 1])
+                fb, g = self.adjoint_rhs(R)
+                Fb = Fb + fb
+                gmat += g
+                if len(gM):
+                    gM += self.adjoint_moment(tn + RK_C[st - 1] * dt, R)
+                DFb = RK_A[st - 1] * R
+            for c in range(3):
+                np.add.at(Fb[c], (ridx[:, 2] - 1, ridx[:, 1] - 1, ridx[:, 0] - 1), res[n][:, c])
+        return chi, seis, gmat, gM
+
+    def adjoint_moment(self, t: float, R: np.ndarray, b: int = 0) -> np.ndarray:
+        """Moment-tensor adjoint of the sources at time t for rate adjoint R: (nsrc, 6)."""
+        nsrc = len(self.problem.blocks[b].sources)
+        g = np.zeros((max(nsrc, 1), 6))
+        Rr = np.ascontiguousarray(R, dtype=np.float64)
+        lib().orc_adjoint_moment(self.handle, b, float(t), _dptr(Rr), _dptr(g))
+        return g[:nsrc]
 
     def _shape(self, b: int, ncomp: int):
         nq, nr, ns = self.problem.blocks[b].nqrs

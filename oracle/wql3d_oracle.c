@@ -1992,3 +1992,286 @@ int orc_get_fault(void *dv, int kind, double *out) {
   return nc;
 }
 
+
+/* ======================================================================== */
+/* Discrete adjoint of the elastic right-hand side (test infrastructure).   */
+/*                                                                          */
+/* For the rates R-bar of one stage, orc_adjoint_rhs adds L^T R-bar to the  */
+/* field adjoint and (dL/dp F)^T R-bar to the material gradient, where L is */
+/* this file's set_rates + impose_boundary_condition for one elastic block  */
+/* (rhs_interior, rhs_near_boundaries with jju6 / jju_up4, face SATs; no    */
+/* PML, memory variables, interface or sources) and F the block's current   */
+/* fields.  Written as the scatter transpose of those loops: every          */
+/* accumulation DF[f][p] += c * F[g][q] there becomes Fbar[g][q] +=         */
+/* c * Rbar[f][p] here.  SAT material derivatives by complex step.          */
+/* ======================================================================== */
+#include <complex.h>
+
+/* adjoint of the rate assembly shared by the interior and near-boundary
+   paths: DU = [a1 (Ux3 + Uy6 + Uz7), ...; a2 Ux0 + a3 (Uy1 + Uz2), ...;
+   a4 (Uy0 + Ux1), ...]; returns the adjoints of Ux, Uy, Uz and adds the
+   material gradient (a1 = 1 / (rho J) or 1 / rho) */
+static void rates_adjoint(const double R[9], double a1, double lam, double mu, double rho, const double Ux[9],
+                          const double Uy[9], const double Uz[9], double Ubx[9], double Uby[9], double Ubz[9],
+                          double *glam, double *gmu, double *grho) {
+  const double a2 = 2.0 * mu + lam, a3 = lam, a4 = mu;
+  for (int f = 0; f < 9; ++f) { Ubx[f] = 0.0; Uby[f] = 0.0; Ubz[f] = 0.0; }
+  Ubx[3] += a1 * R[0]; Uby[6] += a1 * R[0]; Ubz[7] += a1 * R[0];
+  Ubx[6] += a1 * R[1]; Uby[4] += a1 * R[1]; Ubz[8] += a1 * R[1];
+  Ubx[7] += a1 * R[2]; Uby[8] += a1 * R[2]; Ubz[5] += a1 * R[2];
+  Ubx[0] += a2 * R[3] + a3 * R[4] + a3 * R[5];
+  Uby[1] += a3 * R[3] + a2 * R[4] + a3 * R[5];
+  Ubz[2] += a3 * R[3] + a3 * R[4] + a2 * R[5];
+  Uby[0] += a4 * R[6]; Ubx[1] += a4 * R[6];
+  Ubz[0] += a4 * R[7]; Ubx[2] += a4 * R[7];
+  Ubz[1] += a4 * R[8]; Uby[2] += a4 * R[8];
+  const double vs = R[0] * (Ux[3] + Uy[6] + Uz[7]) + R[1] * (Ux[6] + Uy[4] + Uz[8]) + R[2] * (Ux[7] + Uy[8] + Uz[5]);
+  const double tr = Ux[0] + Uy[1] + Uz[2];
+  *grho += -a1 / rho * vs;
+  *glam += (R[3] + R[4] + R[5]) * tr;
+  *gmu += 2.0 * (R[3] * Ux[0] + R[4] * Uy[1] + R[5] * Uz[2]) + R[6] * (Uy[0] + Ux[1]) + R[7] * (Uz[0] + Ux[2]) +
+          R[8] * (Uz[1] + Uy[2]);
+}
+
+/* scatter transpose of one near-boundary derivative (jju6 or jju_up4) for
+   metric row X: Ub = adjoint of Ju; adds to Fbar */
+static void jju_adjoint(const oblk *b, int x, int y, int z, double *const X[3], const double Ub[9], double **Fbar) {
+  const long p0 = ID(b, x, y, z);
+  const int pos[3] = {x, y, z}, nn[3] = {b->nx, b->ny, b->nz};
+  const double ih[3] = {1.0 / b->hq, 1.0 / b->hr, 1.0 / b->hs};
+  int cnt, idx[8];
+  double c[8];
+  for (int a = 0; a < 3; ++a)
+    for (int grp = 0; grp < 2; ++grp) { /* 0: velocities, 1: stresses */
+      if (b->d.fd == ORC_FD_UPWIND4) up4_stencil(grp == 0, pos[a], nn[a], &cnt, idx, c);
+      else sbp_stencil(pos[a], nn[a], &cnt, idx, c);
+      for (int k = 0; k < cnt; ++k) {
+        const int q3[3] = {a == 0 ? idx[k] : x, a == 1 ? idx[k] : y, a == 2 ? idx[k] : z};
+        const long q = ID(b, q3[0], q3[1], q3[2]);
+        if (grp == 0)
+          for (int f = 0; f < 3; ++f) Fbar[f][q] += ih[a] * X[a][p0] * c[k] * Ub[f];
+        else
+          for (int f = 3; f < 9; ++f) Fbar[f][q] += ih[a] * c[k] * b->J[q] * X[a][q] * Ub[f];
+      }
+    }
+}
+
+/* the SAT term pen * structure(bc_point(u)) of one face point in complex
+   arithmetic (material perturbed by a complex step) */
+static void sat_point_c(int plus, const double u[9], double complex rho, double complex mu, double complex lam,
+                        const double l[3], const double m[3], const double n[3], double norm, double r, double pen,
+                        double complex out[9]) {
+  const double complex c_p = csqrt((2.0 * mu + lam) / rho), c_s = csqrt(mu / rho);
+  const double complex Zp = rho * c_p, Zs = rho * c_s;
+  double T[3];
+  T[0] = n[0] * u[3] + n[1] * u[6] + n[2] * u[7];
+  T[1] = n[0] * u[6] + n[1] * u[4] + n[2] * u[8];
+  T[2] = n[0] * u[7] + n[1] * u[8] + n[2] * u[5];
+  const double vl = l[0] * u[0] + l[1] * u[1] + l[2] * u[2];
+  const double vm = m[0] * u[0] + m[1] * u[1] + m[2] * u[2];
+  const double vn = n[0] * u[0] + n[1] * u[1] + n[2] * u[2];
+  const double Tl = l[0] * T[0] + l[1] * T[1] + l[2] * T[2];
+  const double Tm = m[0] * T[0] + m[1] * T[1] + m[2] * T[2];
+  const double Tn = n[0] * T[0] + n[1] * T[1] + n[2] * T[2];
+  const double s = plus ? 1.0 : -1.0;
+  const double complex pl = 0.5 * ((1.0 - r) * Zs * vl + s * (1.0 + r) * Tl);
+  const double complex pm = 0.5 * ((1.0 - r) * Zs * vm + s * (1.0 + r) * Tm);
+  const double complex pn = 0.5 * ((1.0 - r) * Zp * vn + s * (1.0 + r) * Tn);
+  const double complex ql = 0.5 * ((1.0 - r) * vl + s * (1.0 + r) / Zs * Tl);
+  const double complex qm = 0.5 * ((1.0 - r) * vm + s * (1.0 + r) / Zs * Tm);
+  const double complex qn = 0.5 * ((1.0 - r) * vn + s * (1.0 + r) / Zp * Tn);
+  double complex ub[9];
+  for (int c = 0; c < 3; ++c) ub[c] = norm * (l[c] * pl + m[c] * pm + n[c] * pn);
+  const double complex Fx = l[0] * ql + m[0] * qm + n[0] * qn;
+  const double complex Fy = l[1] * ql + m[1] * qm + n[1] * qn;
+  const double complex Fz = l[2] * ql + m[2] * qm + n[2] * qn;
+  ub[3] = s * (norm * n[0] * Fx);
+  ub[4] = s * (norm * n[1] * Fy);
+  ub[5] = s * (norm * n[2] * Fz);
+  ub[6] = s * (norm * (n[1] * Fx + n[0] * Fy));
+  ub[7] = s * (norm * (n[2] * Fx + n[0] * Fz));
+  ub[8] = s * (norm * (n[2] * Fy + n[1] * Fz));
+  out[0] = pen / rho * ub[0];
+  out[1] = pen / rho * ub[1];
+  out[2] = pen / rho * ub[2];
+  out[3] = pen * ((2.0 * mu + lam) * ub[3] + lam * (ub[4] + ub[5]));
+  out[4] = pen * ((2.0 * mu + lam) * ub[4] + lam * (ub[3] + ub[5]));
+  out[5] = pen * ((2.0 * mu + lam) * ub[5] + lam * (ub[3] + ub[4]));
+  out[6] = pen * (mu * ub[6]);
+  out[7] = pen * (mu * ub[7]);
+  out[8] = pen * (mu * ub[8]);
+}
+
+int orc_adjoint_rhs(void *dv, int bi, const double *Rin, double *Fbout, double *gout) {
+  odom *D = (odom *)dv;
+  oblk *b = D->B[bi];
+  if (b->d.response != ORC_ELASTIC || b->d.mms) return -1;
+  for (int f = 0; f < 6; ++f)
+    if (b->d.pml[f] || b->d.bc[f] == 0) return -1;
+  const long np = b->np;
+  double *R[9], *Fb[9], *g[3];
+  for (int f = 0; f < 9; ++f) { R[f] = zalloc(np, 0.0); Fb[f] = zalloc(np, 0.0); }
+  for (int f = 0; f < 3; ++f) g[f] = zalloc(np, 0.0);
+  set3(b, R, 9, Rin);
+  int lo[3], hi[3];
+  interior_bounds(b, lo, hi);
+  const int curv = b->d.mesh == 1;
+  const long st[3] = {1, b->NX, (long)b->NX * b->NY};
+  for (int z = 1; z <= b->nz; ++z)
+    for (int y = 1; y <= b->ny; ++y)
+      for (int x = 1; x <= b->nx; ++x) {
+        const long p = ID(b, x, y, z);
+        double Rp[9];
+        for (int f = 0; f < 9; ++f) Rp[f] = R[f][p];
+        const double lam = b->M[0][p], mu = b->M[1][p], rho = b->M[2][p];
+        const int interior = lo[2] <= z && z <= hi[2] && lo[1] <= y && y <= hi[1] && lo[0] <= x && x <= hi[0];
+        double Ux[9] = {0}, Uy[9] = {0}, Uz[9] = {0}, Ubx[9], Uby[9], Ubz[9];
+        if (!interior) {
+          if (b->d.fd == ORC_FD_UPWIND4) {
+            jju_up4(b, x, y, z, b->mx, Ux); jju_up4(b, x, y, z, b->my, Uy); jju_up4(b, x, y, z, b->mz, Uz);
+          } else {
+            jju6(b, x, y, z, b->mx, Ux); jju6(b, x, y, z, b->my, Uy); jju6(b, x, y, z, b->mz, Uz);
+          }
+          rates_adjoint(Rp, 1.0 / (rho * b->J[p]), lam, mu, rho, Ux, Uy, Uz, Ubx, Uby, Ubz, &g[0][p], &g[1][p],
+                        &g[2][p]);
+          jju_adjoint(b, x, y, z, b->mx, Ubx, Fb);
+          jju_adjoint(b, x, y, z, b->my, Uby, Fb);
+          jju_adjoint(b, x, y, z, b->mz, Ubz, Fb);
+          continue;
+        }
+        /* strict interior: the forward's DFx / DFy / DFz as plain sums of tap terms */
+        double ws[2][8];  /* per tap: coefficient / h */
+        int offs[2][8], ntap[2];
+        if (b->d.fd == ORC_FD_UPWIND4) {
+          static const double cf[5] = {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0};
+          static const double cb[5] = {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0};
+          ntap[0] = ntap[1] = 5;
+          for (int k = 0; k < 5; ++k) { ws[0][k] = cf[k]; offs[0][k] = k - 1; ws[1][k] = cb[k]; offs[1][k] = k - 3; }
+        } else {
+          static const double cc[6] = {-1.0 / 60.0, 0.15, -0.75, 0.75, -0.15, 1.0 / 60.0};
+          static const int oo[6] = {-3, -2, -1, 1, 2, 3};
+          ntap[0] = ntap[1] = 6;
+          for (int k = 0; k < 6; ++k) { ws[0][k] = ws[1][k] = cc[k]; offs[0][k] = offs[1][k] = oo[k]; }
+        }
+        const double ih[3] = {1.0 / b->hq, 1.0 / b->hr, 1.0 / b->hs};
+        double *const *Xr[3] = {b->mx, b->my, b->mz};
+        double DF3[3][9];  /* [row r] derivative terms DFx, DFy, DFz */
+        for (int r = 0; r < 3; ++r)
+          for (int f = 0; f < 9; ++f) DF3[r][f] = 0.0;
+        for (int r = 0; r < 3; ++r)
+          for (int a = 0; a < 3; ++a) {
+            if (!curv && a != r) continue;
+            for (int grp = 0; grp < 2; ++grp)
+              for (int k = 0; k < ntap[grp]; ++k) {
+                const long q = p + offs[grp][k] * st[a];
+                for (int f = grp ? 3 : 0; f < (grp ? 9 : 3); ++f) {
+                  const double w = ws[grp][k] * ih[a];
+                  DF3[r][f] += (curv && grp) ? w * b->F[f][q] * b->J[q] * Xr[r][a][q] : Xr[r][a][p] * w * b->F[f][q];
+                }
+              }
+          }
+        const double a1 = curv ? 1.0 / (rho * b->J[p]) : 1.0 / rho;
+        rates_adjoint(Rp, a1, lam, mu, rho, DF3[0], DF3[1], DF3[2], Ubx, Uby, Ubz, &g[0][p], &g[1][p], &g[2][p]);
+        const double *Ub[3] = {Ubx, Uby, Ubz};
+        for (int r = 0; r < 3; ++r)
+          for (int a = 0; a < 3; ++a) {
+            if (!curv && a != r) continue;
+            for (int grp = 0; grp < 2; ++grp)
+              for (int k = 0; k < ntap[grp]; ++k) {
+                const long q = p + offs[grp][k] * st[a];
+                const double w = ws[grp][k] * ih[a];
+                for (int f = grp ? 3 : 0; f < (grp ? 9 : 3); ++f)
+                  Fb[f][q] += ((curv && grp) ? w * b->J[q] * Xr[r][a][q] : Xr[r][a][p] * w) * Ub[r][f];
+              }
+          }
+      }
+  /* face SATs: DF(p) -= pen * structure(bc_point(u(p))), linear in u(p) */
+  const double hs_[3] = {b->hq, b->hr, b->hs};
+  for (int f = 0; f < 6; ++f) {
+    const int type = b->d.bc[f];
+    if (type <= 0) continue;
+    const int axis = f / 2, plus = f % 2;
+    const double r = type == 1 ? 0.0 : type == 2 ? 1.0 : -1.0;
+    const int fixed = plus ? (axis == 0 ? b->nx : axis == 1 ? b->ny : b->nz) : 1;
+    const double pen = b->d.tau0 / hs_[axis];
+    for (int c2 = 1; c2 <= b->fdim[f][1]; ++c2)
+      for (int c1 = 1; c1 <= b->fdim[f][0]; ++c1) {
+        int x, y, z;
+        if (axis == 0) { x = fixed; y = c1; z = c2; }
+        else if (axis == 1) { x = c1; y = fixed; z = c2; }
+        else { x = c1; y = c2; z = fixed; }
+        const long p = ID(b, x, y, z);
+        const long fp = FID(b, f, c1, c2);
+        double l3[3], m3[3], n3[3], u[9];
+        for (int c = 0; c < 3; ++c) { l3[c] = b->nl[f][c][fp]; m3[c] = b->nm[f][c][fp]; n3[c] = b->nn[f][c][fp]; }
+        const double qx = b->mx[axis][p], qy = b->my[axis][p], qz = b->mz[axis][p];
+        const double norm = sqrt(qx * qx + qy * qy + qz * qz);
+        const double lam = b->M[0][p], mu = b->M[1][p], rho = b->M[2][p];
+        double complex out[9];
+        for (int j = 0; j < 9; ++j) { /* Jacobian column j (the term is linear in u) */
+          for (int c = 0; c < 9; ++c) u[c] = c == j ? 1.0 : 0.0;
+          sat_point_c(plus, u, rho, mu, lam, l3, m3, n3, norm, r, pen, out);
+          double acc = 0.0;
+          for (int c = 0; c < 9; ++c) acc += creal(out[c]) * R[c][p];
+          Fb[j][p] -= acc;
+        }
+        const double hstep = 1e-30;
+        for (int c = 0; c < 9; ++c) u[c] = b->F[c][p];
+        for (int prm = 0; prm < 3; ++prm) { /* lambda, mu, rho */
+          double complex cl = lam, cm = mu, cr = rho;
+          if (prm == 0) cl += I * hstep;
+          if (prm == 1) cm += I * hstep;
+          if (prm == 2) cr += I * hstep;
+          sat_point_c(plus, u, cr, cm, cl, l3, m3, n3, norm, r, pen, out);
+          double acc = 0.0;
+          for (int c = 0; c < 9; ++c) acc += cimag(out[c]) / hstep * R[c][p];
+          g[prm][p] -= acc;
+        }
+      }
+  }
+  double *outF = Fbout, *outG = gout;
+  double *tmp9 = (double *)malloc(sizeof(double) * 9 * (size_t)b->nx * b->ny * b->nz);
+  get3(b, Fb, 9, tmp9);
+  const long n = (long)b->nx * b->ny * b->nz;
+  for (long i = 0; i < 9 * n; ++i) outF[i] += tmp9[i];
+  get3(b, g, 3, tmp9);
+  for (long i = 0; i < 3 * n; ++i) outG[i] += tmp9[i];
+  free(tmp9);
+  for (int f = 0; f < 9; ++f) { free(R[f]); free(Fb[f]); }
+  for (int f = 0; f < 3; ++f) free(g[f]);
+  return 0;
+}
+
+/* moment-tensor adjoint of the sources at time t: gM[6 * i + c] +=
+   -A_i(t) sum_p delta_i(p) Rbar_(3+c)(p) (set_moment_tensor above) */
+void orc_adjoint_moment(void *dv, int bi, double t, const double *Rin, double *gM) {
+  odom *D = (odom *)dv;
+  oblk *b = D->B[bi];
+  const orc_desc *d = &b->d;
+  const int half = d->src_order == 4 ? 4 : 2;
+  const long n = (long)b->nx * b->ny * b->nz;
+  for (int i = 0; i < b->nsrc; ++i) {
+    const double *sp = &b->spar[i * 11];
+    const int nx0 = b->snear[3 * i], ny0 = b->snear[3 * i + 1], nz0 = b->snear[3 * i + 2];
+    if (nx0 < 1) continue;
+    const double A = source_time(b->stype[i], t, sp[1], sp[0]);
+    for (int k = nz0 - half; k <= nz0 + half; ++k) {
+      if (k < 1 || k > b->nz) continue;
+      for (int m = ny0 - half; m <= ny0 + half; ++m) {
+        if (m < 1 || m > b->ny) continue;
+        for (int l = nx0 - half; l <= nx0 + half; ++l) {
+          if (l < 1 || l > b->nx) continue;
+          const long p = ID(b, l, m, k);
+          const double hx = b->hq / b->mx[0][p], hy = b->hr / b->my[1][p], hz = b->hs / b->mz[2][p];
+          const double ax = (sp[8] - b->sphys[3 * i]) / hx, ay = (sp[9] - b->sphys[3 * i + 1]) / hy;
+          const double az = (sp[10] - b->sphys[3 * i + 2]) / hz;
+          const double delta = singular_source(l, nx0, hx, ax, d->src_order, d->src_alpha) *
+                               singular_source(m, ny0, hy, ay, d->src_order, d->src_alpha) *
+                               singular_source(k, nz0, hz, az, d->src_order, d->src_alpha);
+          const long li = (long)(l - 1) + (long)b->nx * ((long)(m - 1) + (long)b->ny * (long)(k - 1));
+          for (int c = 0; c < 6; ++c) gM[6 * i + c] -= A * delta * Rin[(3 + c) * n + li];
+        }
+      }
+    }
+  }
+}

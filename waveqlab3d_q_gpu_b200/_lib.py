@@ -97,6 +97,19 @@ SIGNATURES = {
     "wql3d_kernel_launches": [C.c_void_p, C.POINTER(C.c_int64)],
     "wql3d_last_error": [],
     "wql3d_max_abs_noalloc": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
+    "wql3d_reset_samples": [C.c_void_p],
+    "wql3d_set_material": [C.c_void_p, C.c_int, dp],
+    "wql3d_set_moment": [C.c_void_p, C.c_int, dp],
+    "wql3d_field_volume": [C.c_void_p, C.c_int, C.POINTER(C.c_int64)],
+    "wql3d_store_fields": [C.c_void_p, C.c_int, C.c_void_p],
+    "wql3d_load_fields": [C.c_void_p, C.c_int, C.c_void_p],
+    "wql3d_adjoint_enable": [C.c_void_p],
+    "wql3d_adjoint_reset": [C.c_void_p],
+    "wql3d_adjoint_step": [C.c_void_p, C.c_int, C.c_double],
+    "wql3d_adjoint_add_receivers": [C.c_void_p, C.c_int, dp],
+    "wql3d_adjoint_rhs": [C.c_void_p, C.c_int, dp, dp, dp],
+    "wql3d_get_adjoint_fields": [C.c_void_p, C.c_int, dp],
+    "wql3d_get_adjoint_gradient": [C.c_void_p, C.c_int, dp, dp],
 }
 
 _LIB = None

@@ -1,0 +1,152 @@
+"""Waveform-misfit gradients through the discrete adjoint of the CUDA stage.
+
+The reference has no adjoint.  This module differentiates the misfit
+
+    chi = 1/2 sum_n sum_r |v_r(t_n) - d_r(t_n)|^2
+
+of the stage-1 station samples (src/time_step.f90:137) of an N-step run
+from rest with respect to the material lambda, mu, rho of every point and
+the moment tensors of the sources, for one FP64 elastic block without PML
+(traditional-6 operator, face SATs, moment-tensor sources).  The adjoint
+kernels are the transposes of the stage operator, the sources and the
+Kennedy-Carpenter (5,4) low-storage update (``wql3d_adjoint_*`` in
+include/wql3d.h).
+
+Memory: sqrt(N)-step checkpointing with recomputation.  The forward run
+stores the fields every K = ceil(sqrt(N)) steps on the device; the reverse
+sweep restores each checkpoint, recomputes its K states into a device
+segment buffer, and reverses those steps.  Device storage is
+(ceil(N/K) + K) field states instead of N; the forward work is done twice.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from .domain import Domain, _ptr
+from .problem import Problem
+
+
+class AdjointSolver:
+    """Forward runs and adjoint sweeps of one elastic block on the current CUDA device."""
+
+    def __init__(self, problem: Problem, nsteps: int, checkpoint_every: Optional[int] = None):
+        if len(problem.blocks) != 1 or problem.response != "elastic":
+            raise ValueError("the adjoint covers one elastic block")
+        self.problem = problem
+        self.nsteps = int(nsteps)
+        self.K = int(checkpoint_every) if checkpoint_every else max(1, math.ceil(math.sqrt(self.nsteps)))
+        self.dt = problem.dt()
+        self.domain = Domain(problem, precision="fp64", max_samples=self.nsteps + 2)
+        L = _lib.load()
+        self.L = L
+        self.h = self.domain.handle
+        _lib.check(L.wql3d_adjoint_enable(self.h), "wql3d_adjoint_enable")
+        ne = C.c_int64()
+        _lib.check(L.wql3d_field_volume(self.h, 0, C.byref(ne)), "wql3d_field_volume")
+        self.nchk = math.ceil(self.nsteps / self.K)
+        self.ckpt = torch.empty((self.nchk, ne.value), dtype=torch.float64, device="cuda")
+        self.seg = torch.empty((self.K, ne.value), dtype=torch.float64, device="cuda")
+        blk = problem.blocks[0]
+        self.nrec = 0 if blk.receivers is None else len(blk.receivers)
+        self.nsrc = len(blk.sources)
+        self.shape = tuple(reversed(blk.nqrs))
+
+    # ------------------------------------------------------------ parameters
+    def set_parameters(self, material: Optional[np.ndarray] = None, moment: Optional[np.ndarray] = None):
+        """material (3, ns, nr, nq) lambda, mu, rho; moment (nsrc, 6) mxx myy mzz mxy mxz myz."""
+        if material is not None:
+            m = np.ascontiguousarray(material, dtype=np.float64)
+            _lib.check(self.L.wql3d_set_material(self.h, 0, _ptr(m)), "wql3d_set_material")
+        if moment is not None and self.nsrc:
+            m6 = np.ascontiguousarray(moment, dtype=np.float64).reshape(self.nsrc, 6)
+            _lib.check(self.L.wql3d_set_moment(self.h, 0, _ptr(m6)), "wql3d_set_moment")
+
+    def _ptr(self, t: torch.Tensor):
+        return C.c_void_p(t.data_ptr())
+
+    # ---------------------------------------------------------------- forward
+    def forward(self) -> np.ndarray:
+        """N steps from rest with checkpoints; returns the station velocities (N, nrec, 3)."""
+        d = self.domain
+        d.set_fields(np.zeros((9,) + self.shape))
+        d.t = 0.0
+        d.n = 1
+        _lib.check(self.L.wql3d_reset_samples(self.h), "wql3d_reset_samples")
+        for k in range(self.nchk):
+            _lib.check(self.L.wql3d_store_fields(self.h, 0, self._ptr(self.ckpt[k])), "wql3d_store_fields")
+            steps = min(self.K, self.nsteps - k * self.K)
+            d.run(steps)
+        seis = d.seismograms()[:self.nsteps, :, 1:4]
+        return np.ascontiguousarray(seis)
+
+    # --------------------------------------------------------------- backward
+    def backward(self, residual: np.ndarray):
+        """Reverse sweep for the misfit derivative residual (N, nrec, 3) with
+        respect to the station samples; returns (d/d(lambda, mu, rho) as
+        (3, ns, nr, nq), d/dM as (nsrc, 6))."""
+        d, L, h = self.domain, self.L, self.h
+        res = np.ascontiguousarray(residual, dtype=np.float64)
+        _lib.check(L.wql3d_adjoint_reset(h), "wql3d_adjoint_reset")
+        for k in range(self.nchk - 1, -1, -1):
+            first = k * self.K
+            steps = min(self.K, self.nsteps - first)
+            # recompute the segment's states F_n, n = first .. first + steps - 1 (0-based)
+            _lib.check(L.wql3d_load_fields(h, 0, self._ptr(self.ckpt[k])), "wql3d_load_fields")
+            d.t = first * self.dt
+            for j in range(steps):
+                _lib.check(L.wql3d_store_fields(h, 0, self._ptr(self.seg[j])), "wql3d_store_fields")
+                if j + 1 < steps:
+                    d.time_step_RK(first + j + 1)
+            for j in range(steps - 1, -1, -1):
+                n = first + j
+                _lib.check(L.wql3d_load_fields(h, 0, self._ptr(self.seg[j])), "wql3d_load_fields")
+                d.t = n * self.dt
+                _lib.check(L.wql3d_adjoint_step(h, n + 1, float(self.dt)), "wql3d_adjoint_step")
+                if self.nrec:
+                    r = np.ascontiguousarray(res[n])
+                    _lib.check(L.wql3d_adjoint_add_receivers(h, 0, _ptr(r)), "wql3d_adjoint_add_receivers")
+        gmat = np.zeros((3,) + self.shape)
+        gM = np.zeros((max(self.nsrc, 1), 6))
+        _lib.check(L.wql3d_get_adjoint_gradient(h, 0, _ptr(gmat), _ptr(gM)), "wql3d_get_adjoint_gradient")
+        return gmat, gM[:self.nsrc]
+
+    def adjoint_fields(self) -> np.ndarray:
+        a = np.zeros((9,) + self.shape)
+        _lib.check(self.L.wql3d_get_adjoint_fields(self.h, 0, _ptr(a)), "wql3d_get_adjoint_fields")
+        return a
+
+    def close(self):
+        self.domain.close()
+
+
+class WaveformMisfit(torch.autograd.Function):
+    """chi(material, moment) = 1/2 ||v(material, moment) - observed||^2 with the
+    gradient from the discrete adjoint (one forward run with checkpoints in
+    forward(), the recomputing reverse sweep in backward())."""
+
+    @staticmethod
+    def forward(ctx, material: torch.Tensor, moment: torch.Tensor, solver: AdjointSolver, observed: np.ndarray):
+        solver.set_parameters(material.detach().cpu().numpy(), moment.detach().cpu().numpy())
+        seis = solver.forward()
+        res = seis - observed
+        ctx.solver = solver
+        ctx.res = res
+        ctx.dev = material.device
+        return torch.tensor(0.5 * float(np.sum(res * res)), dtype=torch.float64, device=material.device)
+
+    @staticmethod
+    def backward(ctx, gout):
+        gmat, gM = ctx.solver.backward(ctx.res)
+        g = float(gout)
+        return (torch.from_numpy(g * gmat).to(ctx.dev), torch.from_numpy(g * gM).to(ctx.dev), None, None)
+
+
+def waveform_misfit(material: torch.Tensor, moment: torch.Tensor, solver: AdjointSolver,
+                    observed: np.ndarray) -> torch.Tensor:
+    return WaveformMisfit.apply(material, moment, solver, observed)

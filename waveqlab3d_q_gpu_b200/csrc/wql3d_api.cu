@@ -9,6 +9,7 @@
 #include "wql3d_device.cuh"
 #include "wql3d_iface.cuh"
 #include "wql3d_stage.cuh"
+#include "wql3d_adjoint.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -184,6 +185,10 @@ struct wql3d_domain {
   // s-slab ghost-plane exchange buffers (2 faces x up to 10 x 3 x nr x nq)
   bool slab = false;
   void *halo_send = nullptr, *halo_recv = nullptr;
+  // discrete adjoint (wql3d_adjoint_enable)
+  bool adj_on = false;
+  AdjBlk adj;
+  double *adj_res = nullptr;   // receiver residuals of one sample (device)
 };
 
 namespace {
@@ -224,6 +229,8 @@ int upload_constants() {
     const int e = f(t);
     if (e != 0) return fail(WQL3D_ECUDA, std::string("stage constants: ") + cudaGetErrorString((cudaError_t)e));
   }
+  if (const int e = upload_tables_adjoint(&t))
+    return fail(WQL3D_ECUDA, std::string("adjoint constants: ") + cudaGetErrorString((cudaError_t)e));
   return WQL3D_OK;
 }
 
@@ -1544,6 +1551,246 @@ int wql3d_final_state(wql3d_domain *d, double *max_field, double *max_memory, do
   return d->fp32 ? final_state<float>(d, max_field, max_memory, block_max)
                  : final_state<double>(d, max_field, max_memory, block_max);
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+namespace {
+
+// transposed derivative rows of the traditional-6 operator for an axis of n
+// points: row q lists (p - q, D[p][q]) over the rows p that read point q,
+// with the forward's row choice (left closure for p <= 6, right closure for
+// p >= n - 5, central row otherwise)
+void transposed_rows(int n, int lit, std::vector<int> &off, std::vector<double> &c) {
+  std::vector<double> D((size_t)n * n, 0.0);
+  for (int p = 1; p <= n; ++p) {
+    if (p <= 6) {
+      const int r = p - 1;
+      for (int k = 0; k < kSbpCnt[r]; ++k) D[(size_t)(p - 1) * n + (kSbpIdx[r][k] - 1)] += kSbpC[lit][r][k];
+    } else if (p >= n - 5) {
+      const int r = n - p;
+      for (int k = 0; k < kSbpCnt[r]; ++k) D[(size_t)(p - 1) * n + (n - kSbpIdx[r][k])] += -kSbpC[lit][r][k];
+    } else {
+      const double cc[6] = {-1.0 / 60.0, 0.15, -0.75, 0.75, -0.15, 1.0 / 60.0};
+      const int oo[6] = {-3, -2, -1, 1, 2, 3};
+      for (int k = 0; k < 6; ++k) D[(size_t)(p - 1) * n + (p - 1 + oo[k])] += cc[k];
+    }
+  }
+  off.assign((size_t)n * ADJ_TW, 0);
+  c.assign((size_t)n * ADJ_TW, 0.0);
+  for (int q = 1; q <= n; ++q) {
+    int k = 0;
+    for (int p = 1; p <= n; ++p) {
+      const double v = D[(size_t)(p - 1) * n + (q - 1)];
+      if (v == 0.0) continue;
+      off[(size_t)(q - 1) * ADJ_TW + k] = p - q;
+      c[(size_t)(q - 1) * ADJ_TW + k] = v;
+      ++k;
+    }
+  }
+}
+
+int adjoint_supported(wql3d_domain *d) {
+  if (d->fp32 || d->nblocks != 1 || d->response != WQL3D_ELASTIC || d->slab || d->desc.remote_side || d->desc.mms)
+    return fail(WQL3D_EINVAL, "the adjoint covers one FP64 elastic block (no interface, slab or MMS)");
+  const wql3d_block_desc &bd = d->desc.block[0];
+  for (int f = 0; f < 6; ++f)
+    if (bd.pml[f] && bd.npml > 0) return fail(WQL3D_EINVAL, "the adjoint covers blocks without PML");
+  if (bd.fd_operator != WQL3D_FD_TRADITIONAL6) return fail(WQL3D_EINVAL, "the adjoint covers traditional-6");
+  if (bd.nq < 13 || bd.nr < 13 || bd.ns < 13) return fail(WQL3D_EINVAL, "the adjoint needs 13 points per axis");
+  return WQL3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wql3d_adjoint_enable(wql3d_domain *d) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  if (d->adj_on) return WQL3D_OK;
+  if (int rc = adjoint_supported(d)) return rc;
+  Blk<double> &b = d->bd[0];
+  const size_t V = (size_t)b.vol;
+  AdjBlk &A = d->adj;
+  Alloc &M = d->mem;
+  CK(M.get(&A.Fb, 9 * V));
+  CK(M.get(&A.DFb, 9 * V));
+  CK(M.get(&A.R, 9 * V));
+  CK(M.get(&A.ZY, 12 * V));
+  CK(M.get(&A.g, 3 * V));
+  CK(M.get(&A.gM, (size_t)6 * std::max(1, b.nsrc)));
+  for (int s = 0; s < 5; ++s) CK(M.get(&A.S[s], 9 * V, false));
+  CK(M.get(&d->adj_res, (size_t)3 * std::max(1, b.nrec)));
+  const int nn[3] = {b.nx, b.ny, b.nz};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<int> off;
+    std::vector<double> c;
+    transposed_rows(nn[a], b.lit, off, c);
+    int *doff;
+    double *dc;
+    CK(M.get(&doff, off.size()));
+    CK(M.get(&dc, c.size()));
+    CK(cudaMemcpyAsync(doff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(dc, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice, d->stream));
+    A.toff[a] = doff;
+    A.tc[a] = dc;
+  }
+  A.res = d->adj_res;
+  CK(cudaStreamSynchronize(d->stream));
+  d->adj_on = true;
+  return WQL3D_OK;
+}
+
+int wql3d_adjoint_reset(wql3d_domain *d) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  const size_t V = (size_t)d->bd[0].vol;
+  AdjBlk &A = d->adj;
+  CK(cudaMemsetAsync(A.Fb, 0, sizeof(double) * 9 * V, d->stream));
+  CK(cudaMemsetAsync(A.DFb, 0, sizeof(double) * 9 * V, d->stream));
+  CK(cudaMemsetAsync(A.g, 0, sizeof(double) * 3 * V, d->stream));
+  CK(cudaMemsetAsync(A.gM, 0, sizeof(double) * 6 * std::max(1, d->bd[0].nsrc), d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_adjoint_step(wql3d_domain *d, int n, double dt) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  Blk<double> &b = d->bd[0];
+  AdjBlk &A = d->adj;
+  const size_t bytes = sizeof(double) * 9 * (size_t)b.vol;
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  const double t0 = h.t;
+  (void)n;
+  // stage inputs F^(0..4) of this step, recomputed from the current fields
+  const int cur0 = d->cur;
+  CK(cudaMemcpyAsync(A.S[0], d->cur ? b.F1 : b.F0, bytes, cudaMemcpyDeviceToDevice, d->stream));
+  for (int s = 1; s <= 4; ++s) {
+    if (int rc = enqueue_stage<double>(d, s, dt, F_ALL)) return rc;
+    CK(cudaMemcpyAsync(A.S[s], d->cur ? b.F1 : b.F0, bytes, cudaMemcpyDeviceToDevice, d->stream));
+  }
+  // leave the domain's fields at F^(0) = F_n
+  d->cur = cur0;
+  CK(cudaMemcpyAsync(d->cur ? b.F1 : b.F0, A.S[0], bytes, cudaMemcpyDeviceToDevice, d->stream));
+  // reversed stages 5..1
+  for (int s = 5; s >= 1; --s) {
+    adj_launch_stage(b, A, s, kRkB[s - 1] * dt, kRkA[s - 1], d->stream, &d->launches);
+    adj_launch_moment(b, A, t0 + kRkC[s - 1] * dt, d->stream, &d->launches);
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_adjoint_add_receivers(wql3d_domain *d, int bi, const double *res) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  if (bi != 0 || !res) return fail(WQL3D_EINVAL, "block / residuals");
+  const int nrec = d->bd[0].nrec;
+  if (nrec <= 0) return WQL3D_OK;
+  CK(cudaMemcpyAsync(d->adj_res, res, sizeof(double) * 3 * nrec, cudaMemcpyHostToDevice, d->stream));
+  adj_launch_receivers(d->bd[0], d->adj, d->stream, &d->launches);
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_adjoint_rhs(wql3d_domain *d, int bi, const double *R, double *Fbar, double *g) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  if (bi != 0 || !R || !Fbar || !g) return fail(WQL3D_EINVAL, "arguments");
+  Blk<double> &b = d->bd[0];
+  AdjBlk &A = d->adj;
+  const size_t V = (size_t)b.vol;
+  CK(cudaMemsetAsync(A.Fb, 0, sizeof(double) * 9 * V, d->stream));
+  CK(cudaMemsetAsync(A.g, 0, sizeof(double) * 3 * V, d->stream));
+  if (int rc = put_array<double>(d, d->hb[0], A.DFb, 9, R, 0)) return rc;
+  CK(cudaMemcpyAsync(A.S[0], d->cur ? b.F1 : b.F0, sizeof(double) * 9 * V, cudaMemcpyDeviceToDevice, d->stream));
+  adj_launch_stage(b, A, 1, 0.0, 0.0, d->stream, &d->launches);
+  CK(cudaGetLastError());
+  if (int rc = get_array<double>(d, d->hb[0], A.Fb, 9, Fbar, 0)) return rc;
+  return get_array<double>(d, d->hb[0], A.g, 3, g, 0);
+}
+
+int wql3d_get_adjoint_fields(wql3d_domain *d, int bi, double *Fbar) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  if (bi != 0 || !Fbar) return fail(WQL3D_EINVAL, "arguments");
+  return get_array<double>(d, d->hb[0], d->adj.Fb, 9, Fbar, 0);
+}
+
+int wql3d_get_adjoint_gradient(wql3d_domain *d, int bi, double *g_material, double *g_moment) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  if (bi != 0) return fail(WQL3D_EINVAL, "block");
+  if (g_material)
+    if (int rc = get_array<double>(d, d->hb[0], d->adj.g, 3, g_material, 0)) return rc;
+  if (g_moment && d->bd[0].nsrc > 0) {
+    CK(cudaMemcpyAsync(g_moment, d->adj.gM, sizeof(double) * 6 * d->bd[0].nsrc, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  return WQL3D_OK;
+}
+
+int wql3d_store_fields(wql3d_domain *d, int bi, double *dev_dst) {
+  DOM_CHECK(d, bi);
+  if (d->fp32 || !dev_dst) return fail(WQL3D_EINVAL, "FP64 domain and a device array");
+  const Blk<double> &b = d->bd[bi];
+  CK(cudaMemcpyAsync(dev_dst, d->cur ? b.F1 : b.F0, sizeof(double) * 9 * (size_t)b.vol, cudaMemcpyDeviceToDevice,
+                     d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_load_fields(wql3d_domain *d, int bi, const double *dev_src) {
+  DOM_CHECK(d, bi);
+  if (d->fp32 || !dev_src) return fail(WQL3D_EINVAL, "FP64 domain and a device array");
+  const Blk<double> &b = d->bd[bi];
+  CK(cudaMemcpyAsync(d->cur ? b.F1 : b.F0, dev_src, sizeof(double) * 9 * (size_t)b.vol, cudaMemcpyDeviceToDevice,
+                     d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_field_volume(wql3d_domain *d, int bi, int64_t *elements) {
+  DOM_CHECK(d, bi);
+  if (!elements) return fail(WQL3D_EINVAL, "null argument");
+  *elements = (int64_t)9 * (d->fp32 ? d->bf[bi].vol : d->bd[bi].vol);
+  return WQL3D_OK;
+}
+
+int wql3d_reset_samples(wql3d_domain *d) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  h.nsamp = 0;
+  CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+int wql3d_set_material(wql3d_domain *d, int bi, const double *M) {
+  DOM_CHECK(d, bi);
+  if (!M) return fail(WQL3D_EINVAL, "null material");
+  return d->fp32 ? put_array<float>(d, d->hb[bi], d->bf[bi].M, 3, M, 0)
+                 : put_array<double>(d, d->hb[bi], d->bd[bi].M, 3, M, 0);
+}
+
+int wql3d_set_moment(wql3d_domain *d, int bi, const double *m6) {
+  DOM_CHECK(d, bi);
+  const int ns = d->fp32 ? d->bf[bi].nsrc : d->bd[bi].nsrc;
+  if (ns <= 0) return WQL3D_OK;
+  if (!m6) return fail(WQL3D_EINVAL, "null moment");
+  DevSource *ds = const_cast<DevSource *>(d->fp32 ? d->bf[bi].src : d->bd[bi].src);
+  std::vector<DevSource> hs((size_t)ns);
+  CK(cudaMemcpyAsync(hs.data(), ds, sizeof(DevSource) * ns, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  for (int i = 0; i < ns; ++i)
+    for (int c = 0; c < 6; ++c) hs[(size_t)i].par[2 + c] = m6[6 * i + c];
+  CK(cudaMemcpyAsync(ds, hs.data(), sizeof(DevSource) * ns, cudaMemcpyHostToDevice, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return WQL3D_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
 
 int wql3d_synchronize(wql3d_domain *d) {
   if (!d) return fail(WQL3D_EINVAL, "null domain");
