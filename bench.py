@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--only-fp32", action="store_true", help="time the FP32 path alone (profiling)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint / forward ratio leg")
+    ap.add_argument("--adjoint-steps", type=int, default=64, help="steps of the adjoint ratio leg")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the full-duration FP32 accuracy leg")
+    ap.add_argument("--accuracy-steps", type=int, default=750, help="steps of the FP32 accuracy leg")
     return ap.parse_args()
 
 
@@ -358,6 +362,9 @@ def main():
     g2.close()
     del g2
 
+    adj = adjoint_leg(args, barrier) if (args.workload == "hill" and not args.no_adjoint) else None
+    acc = fp32_accuracy_leg(args) if (args.workload == "hill" and "fp32" in results and not args.no_accuracy) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         pc, cname = (p, name) if args.workload != "planar" else make_problem(args, 4, cpu_sample=True)
@@ -385,6 +392,10 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
         }
+        if adj is not None:
+            line["adjoint"] = adj
+        if acc is not None:
+            line["fp32_accuracy"] = acc
         if "fp32" in results:
             r32 = results["fp32"]
             s64, s32 = r64["seis"][:, :, 1:], r32["seis"][:, :, 1:]
@@ -405,6 +416,71 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp32_accuracy_leg(args):
+    """Seismogram error of the FP32 compensated path against FP64 over the whole
+    duration of the curvilinear two-block Q8 + PML workload: the same 10 km
+    domain, hill, media, source and stations at h = 0.1 km (101^3 points), run
+    for the configuration's 1500 steps of h = 0.05 km (750 steps at the
+    doubled time step), so the direct wave and the surface waves reach every
+    station.  Relative L2 over all stations and samples, and the worst station."""
+    import numpy as np
+    from waveqlab3d_q_gpu_b200.configs import hill_two_block_q8
+    from waveqlab3d_q_gpu_b200.domain import Domain
+    steps = args.accuracy_steps
+    p = hill_two_block_q8(101, h=0.1, steps=steps)
+    seis = {}
+    for prec in ("fp64", "fp32"):
+        g = Domain(p, precision=prec, nsteps_hint=steps + 2)
+        g.run(steps)
+        seis[prec] = g.seismograms(0)[:, :, 1:]
+        g.close()
+    a, b = seis["fp32"], seis["fp64"]
+    err = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    per = [float(np.linalg.norm(a[:, r] - b[:, r]) / max(np.linalg.norm(b[:, r]), 1e-300)) for r in range(b.shape[1])]
+    return {"workload": "curvilinear-2block-101^3-h0.1-hill-q8-pml20-locked-ricker3hz-10x10rec (same domain and "
+                        "physics as the timed workload at half the resolution)",
+            "steps": steps, "seismogram_rel_l2_vs_fp64": err, "worst_station_rel_l2": max(per),
+            "median_station_rel_l2": float(np.median(per)), "peak_velocity": float(np.abs(b).max())}
+
+
+def adjoint_leg(args, barrier):
+    """Adjoint / forward time ratio on the gradient configuration's grid
+    (configs.adjoint_block: curvilinear 201 x 201 x 101 at h = 0.1 km, elastic,
+    one source, 20 x 20 surface stations) over a sample of the run: one
+    forward solve with sqrt(N) checkpoints versus the reverse sweep that
+    recomputes the segments and applies the adjoint steps, both timed on the
+    device stream with a synchronize on both sides.  The misfit compares with
+    data of the true model (3 % Vs anomaly)."""
+    import numpy as np
+    import torch
+    from waveqlab3d_q_gpu_b200.adjoint import AdjointSolver
+    from waveqlab3d_q_gpu_b200.configs import adjoint_block
+    N = args.adjoint_steps
+    true = adjoint_block(anomaly=True, steps=N)
+    sol = AdjointSolver(true, N)
+    observed = sol.forward()
+    sol.set_parameters(material=adjoint_block(anomaly=False, steps=N).blocks[0].material)
+    sol.forward()
+    sol.backward(np.zeros_like(observed))           # warm-up (graphs, first launches)
+    barrier()
+    t0 = time.perf_counter()
+    seis = sol.forward()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    gmat, gM = sol.backward(seis - observed)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    fwd, bwd = t1 - t0, t2 - t1
+    npts = true.blocks[0].npoints
+    sol.close()
+    return {"workload": "curvilinear-201x201x101-h0.1-elastic-1src-20x20rec (gradient configuration grid; "
+                        "discrete adjoint covers elastic blocks without PML)",
+            "steps": N, "checkpoint_every": sol.K, "forward_s": fwd, "backward_s": bwd,
+            "adjoint_forward_ratio": (fwd + bwd) / fwd, "backward_forward_ratio": bwd / fwd,
+            "forward_gpt_s": npts * N / fwd / 1e9,
+            "gradient_norms": {"material": float(np.linalg.norm(gmat)), "moment": float(np.linalg.norm(gM))}}
 
 
 def shots_main(args, rank, world, local, barrier, max_over_ranks):

@@ -244,3 +244,51 @@ def planar_fault_fq8(nq: int = 512, nr: int = 512, ns: int = 384, h: float = 0.1
                 anelastic=an, interface=ip, w_stride=1)
     p.t_final = steps * p.dt() * (1.0 + 1e-9)
     return p
+
+
+def adjoint_block(nq: int = 201, nr: int = 201, ns: int = 101, h: float = 0.1, seed: int = 5, nrec: int = 20,
+                  anomaly: bool = False, steps: int = 1200) -> Problem:
+    """Curvilinear block of the adjoint / gradient configuration: nq x nr x ns
+    points at spacing h with the depth axis q (x = depth below a smooth
+    seeded topography), smooth layered background Vs 2.0 -> 3.5 km/s with
+    depth, Vp = sqrt(3) Vs, rho = 1.7 + 0.2 Vp, optionally a 3 % Gaussian Vs
+    anomaly of radius 1.5 km centred 4 km below the surface; one seeded
+    double-couple Ricker source (3 Hz) at 2 km depth and nrec x nrec surface
+    stations.  Elastic with absorbing SATs on every face except the free
+    surface: the discrete adjoint covers elastic blocks without PML."""
+    rng = np.random.default_rng(seed)
+    Ly, Lz, Lx = h * (nr - 1), h * (ns - 1), h * (nq - 1)
+    y = np.linspace(0.0, Ly, nr)
+    z = np.linspace(0.0, Lz, ns)
+    Y, Z = np.meshgrid(y, z, indexing="xy")
+    topo = 0.3 * np.exp(-((Y - 0.5 * Ly) ** 2 + (Z - 0.5 * Lz) ** 2) / (2.0 * (0.25 * Ly) ** 2))
+    q = np.linspace(0.0, 1.0, nq)
+    X = np.empty((3, ns, nr, nq))
+    top = -topo[:, :, None]
+    X[0] = top + (Lx - top) * q[None, None, :]
+    X[1] = Y[:, :, None]
+    X[2] = Z[:, :, None]
+    depth = X[0] - X[0][:, :, :1]
+    vs = 2.0 + 1.5 * np.clip(depth / Lx, 0.0, 1.0)
+    if anomaly:
+        r2 = (depth - 4.0) ** 2 + (X[1] - 0.5 * Ly) ** 2 + (X[2] - 0.5 * Lz) ** 2
+        vs = vs * (1.0 + 0.03 * np.exp(-r2 / (1.5 ** 2)))
+    vp = math.sqrt(3.0) * vs
+    rho = 1.7 + 0.2 * vp
+    mat = np.stack([rho * (vp ** 2 - 2 * vs ** 2), rho * vs ** 2, rho])
+    strike, dip, rake = rng.uniform(0, 2 * math.pi), rng.uniform(0.2, 1.4), rng.uniform(-math.pi, math.pi)
+    ns_ = np.array([-math.sin(dip) * math.sin(strike), math.sin(dip) * math.cos(strike), -math.cos(dip)])
+    ds_ = np.array([math.cos(rake) * math.cos(strike) + math.sin(rake) * math.cos(dip) * math.sin(strike),
+                    math.cos(rake) * math.sin(strike) - math.sin(rake) * math.cos(dip) * math.cos(strike),
+                    -math.sin(rake) * math.sin(dip)])
+    M = np.outer(ns_, ds_) + np.outer(ds_, ns_)
+    src = Source("ricker", duration=3.0, t_init=1.2 / 3.0, mxx=M[0, 0], myy=M[1, 1], mzz=M[2, 2], mxy=M[0, 1],
+                 mxz=M[0, 2], myz=M[1, 2], x=2.0, y=0.4 * Ly, z=0.6 * Lz)
+    ys = np.linspace(0.05 * Ly, 0.95 * Ly, nrec)
+    zs = np.linspace(0.05 * Lz, 0.95 * Lz, nrec)
+    rec = np.array([[0.0, yy, zz] for zz in zs for yy in ys])
+    b = Block(nqrs=(nq, nr, ns), aqrs=(0.0, 0.0, 0.0), bqrs=(Lx, Ly, Lz), rho_s_p=(2.7, 3.5, 6.06),
+              lqrs=(2, 1, 1), rqrs=(1, 1, 1), coords=X, material=mat, sources=[src], receivers=rec)
+    p = Problem(blocks=[b], response="elastic", type_of_mesh="curvilinear", CFL=0.5, source_order=4, w_stride=1)
+    p.t_final = steps * p.dt() * (1.0 + 1e-9)
+    return p
