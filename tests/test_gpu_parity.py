@@ -138,3 +138,23 @@ def test_metrics_match_oracle(wql3d_lib, oracle_lib):
     g = _domain(p)
     o = oracle_lib.OracleDomain(p)
     assert rel_l2(g.metrics(), o.metrics()) < 1e-15
+
+
+def test_nonfinite_station_sample_is_reported(wql3d_lib):
+    """A NaN planted in the initial state at a station's node reaches that
+    station's stage-1 sample; wql3d_check_status reports WQL3D_ENONFINITE with
+    the first such step (the reference's RUN-STATION-001 check,
+    src/seismogram.f90:516-524), while a clean run reports 0."""
+    from waveqlab3d_q_gpu_b200._lib import Wql3dError
+    p = small_case(mesh="curvilinear", response="elastic")
+    g = _domain(p, nsteps_hint=8)
+    g.run(3)
+    assert g.check_status() == 0
+    idx = g.receiver_index()[0]
+    F = g.fields()
+    F[0, idx[2] - 1, idx[1] - 1, idx[0] - 1] = float("nan")
+    g.set_fields(F)
+    g.run(2)
+    with pytest.raises(Wql3dError, match="ENONFINITE"):
+        g.check_status()
+    g.close()

@@ -98,6 +98,7 @@ SIGNATURES = {
     "wql3d_last_error": [],
     "wql3d_max_abs_noalloc": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
     "wql3d_reset_samples": [C.c_void_p],
+    "wql3d_check_status": [C.c_void_p, ip],
     "wql3d_set_material": [C.c_void_p, C.c_int, dp],
     "wql3d_set_moment": [C.c_void_p, C.c_int, dp],
     "wql3d_field_volume": [C.c_void_p, C.c_int, C.POINTER(C.c_int64)],

@@ -1063,7 +1063,7 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     return code;
   };
   if (d->mem.get(&d->time, 1) != cudaSuccess) return cleanup(fail(WQL3D_ENOMEM, "time"));
-  DevTime t0 = {0.0, 1, 0};
+  DevTime t0 = {0.0, 1, 0, 0, 0};
   if (cudaMemcpyAsync(d->time, &t0, sizeof(t0), cudaMemcpyHostToDevice, d->stream) != cudaSuccess ||
       cudaStreamSynchronize(d->stream) != cudaSuccess)
     return cleanup(fail(WQL3D_ECUDA, "time init"));
@@ -1751,6 +1751,18 @@ int wql3d_field_volume(wql3d_domain *d, int bi, int64_t *elements) {
   DOM_CHECK(d, bi);
   if (!elements) return fail(WQL3D_EINVAL, "null argument");
   *elements = (int64_t)9 * (d->fp32 ? d->bf[bi].vol : d->bd[bi].vol);
+  return WQL3D_OK;
+}
+
+int wql3d_check_status(wql3d_domain *d, int32_t *bad_step) {
+  if (!d) return fail(WQL3D_EINVAL, "null domain");
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  CK(cudaGetLastError());
+  if (bad_step) *bad_step = h.bad;
+  if (h.bad) return fail(WQL3D_ENONFINITE, "non-finite station value at step " + std::to_string(h.bad) +
+                                                " (RUN-STATION-001)");
   return WQL3D_OK;
 }
 

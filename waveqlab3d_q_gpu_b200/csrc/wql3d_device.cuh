@@ -60,6 +60,8 @@ struct DevTime {
   double t;        // domain time at the start of the current step (D%t)
   int n;           // current step number (1-based)
   int nsamp;       // receiver samples taken
+  int bad;         // first step whose station sample held a non-finite value (0: none)
+  int pad;
 };
 
 template <typename T>
@@ -2334,6 +2336,11 @@ __global__ void k_sample(Blk<T> b, int cur, DevTime *tm, int w_stride, int incre
         o[1] = (double)F[p];
         o[2] = (double)F[b.vol + p];
         o[3] = (double)F[2 * b.vol + p];
+        // the reference stops a run whose station values are not finite
+        // (src/seismogram.f90:516-524, RUN-STATION-001): flag the first such step
+        if (!(fabs(o[1]) <= 1.7976931348623157e308 && fabs(o[2]) <= 1.7976931348623157e308 &&
+              fabs(o[3]) <= 1.7976931348623157e308))
+          atomicCAS(&tm->bad, 0, n);
       } else {
         o[1] = o[2] = o[3] = 0.0;
       }

@@ -249,6 +249,13 @@ class Domain:
     def update_fields(self, dt: float):
         _lib.check(_lib.load().wql3d_update_fields(self.handle, float(dt)), "wql3d_update_fields")
 
+    def check_status(self) -> int:
+        """Waits for the queued work; raises Wql3dError (ENONFINITE) when a station
+        sample so far was not finite (src/seismogram.f90:516-524)."""
+        bad = C.c_int32()
+        _lib.check(_lib.load().wql3d_check_status(self.handle, C.byref(bad)), "wql3d_check_status")
+        return bad.value
+
     def synchronize(self):
         _lib.check(_lib.load().wql3d_synchronize(self.handle), "wql3d_synchronize")
 
