@@ -315,6 +315,27 @@ int wql3d_get_adjoint_fields(wql3d_domain *d, int block, double *Fbar);
 /* accumulated gradients: g_material 3 x n (lambda, mu, rho), g_moment nsrc x 6 */
 int wql3d_get_adjoint_gradient(wql3d_domain *d, int block, double *g_material, double *g_moment);
 
+/* Batched independent shots.  No counterpart in the reference, which runs
+   one problem per process: the batched-shot configuration advances many
+   one-block Cartesian traditional-6 domains (same precision and time step,
+   no PML; responses may differ) with one launch per kernel kind and RK stage
+   for all of them, captured two steps at a time in one CUDA graph.  Work
+   lists assign every CTA to one shot (interior tiles, 128-point chunks of the
+   near-boundary shell).  The first run tunes the interior tiles' z-chunk
+   length over its first steps (each candidate times one step; the arithmetic
+   of a point does not depend on it) and keeps the fastest.  The batch orders
+   its work after the shots' own queued work and theirs after the batch; the
+   shots' domains stay usable for set/get calls.  Domains must outlive the
+   batch. */
+typedef struct wql3d_batch wql3d_batch;
+int wql3d_batch_create(wql3d_domain *const *domains, int32_t n, wql3d_batch **out);
+int wql3d_batch_run(wql3d_batch *bt, double dt, int32_t nsteps, int32_t w_stride);
+/* chosen z-chunk and the tuning record: ntried candidates zs[i] with their step times ms[i] */
+int wql3d_batch_tuning(wql3d_batch *bt, int32_t *zchunk, int32_t *ntried, int32_t *zs, float *ms);
+int wql3d_batch_launches(wql3d_batch *bt, int64_t *launches);
+int wql3d_batch_synchronize(wql3d_batch *bt);
+int wql3d_batch_destroy(wql3d_batch *bt);
+
 /* Allocation-free max|v| reduction over a device array.
    No counterpart in the reference: it serves callers that cannot allocate GPU
    memory when they need the diagnostic (for example a Fortran driver whose

@@ -10,6 +10,7 @@
 #include "wql3d_iface.cuh"
 #include "wql3d_stage.cuh"
 #include "wql3d_adjoint.cuh"
+#include "wql3d_batch.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -222,9 +223,10 @@ int upload_constants() {
   memcpy(t.rkA, kRkA, sizeof(kRkA));
   memcpy(t.rkB, kRkB, sizeof(kRkB));
   memcpy(t.rkC, kRkC, sizeof(kRkC));
-  int (*const up[])(const ConstTables &) = {upload_tables_cart_f64, upload_tables_cart_f32, upload_tables_curv_f64,
-                                            upload_tables_curv_f32, upload_tables_generic_f64,
-                                            upload_tables_generic_f32};
+  int (*const up[])(const ConstTables &) = {upload_tables_cart_f64,    upload_tables_cart_f32,
+                                            upload_tables_curv_f64,    upload_tables_curv_f32,
+                                            upload_tables_generic_f64, upload_tables_generic_f32,
+                                            upload_tables_batch_f64,   upload_tables_batch_f32};
   for (auto f : up) {
     const int e = f(t);
     if (e != 0) return fail(WQL3D_ECUDA, std::string("stage constants: ") + cudaGetErrorString((cudaError_t)e));
@@ -1803,6 +1805,292 @@ int wql3d_set_moment(wql3d_domain *d, int bi, const double *m6) {
 }  // extern "C"
 
 extern "C" {
+
+// ---------------------------------------------------------------------------
+// Batched independent shots (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct wql3d_batch {
+  int n = 0;
+  int fp32 = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<wql3d_domain *> doms;
+  Alloc mem;
+  void *blks = nullptr;           // device array of Blk<T>
+  DevTime **times = nullptr;      // device array of the shots' DevTime pointers
+  struct Cls {
+    int resp = 0, sep = 0;
+    std::vector<int> shots;
+    int *d_shots = nullptr, *d_tile = nullptr, *d_shell = nullptr;
+    int tiles = 0, shell_ctas = 0;
+  } cls[8];
+  int zchunk = 12;
+  int tuned = 0;
+  int cur = 0;
+  cudaGraphExec_t graph = nullptr;
+  double g_dt = 0.0;
+  int g_w = -1, g_cur = -1, g_z = -1;
+  int64_t g_launches = 0, launches = 0;
+  std::vector<std::pair<int, float>> tune_log;   // (zchunk, ms per step) of the tuning steps
+};
+
+namespace {
+
+// the classes' interior tile prefix sums for the current zchunk
+int batch_tiles(wql3d_batch *bt) {
+  for (auto &c : bt->cls) {
+    if (c.shots.empty()) continue;
+    std::vector<int> pre(c.shots.size() + 1, 0);
+    for (size_t i = 0; i < c.shots.size(); ++i) {
+      const wql3d_domain *d = bt->doms[(size_t)c.shots[i]];
+      const int *lo = bt->fp32 ? d->bf[0].lo : d->bd[0].lo, *hi = bt->fp32 ? d->bf[0].hi : d->bd[0].hi;
+      const int nxi = hi[0] - lo[0] + 1, nyi = hi[1] - lo[1] + 1, nzi = hi[2] - lo[2] + 1;
+      const int t = (nxi > 0 && nyi > 0 && nzi > 0)
+                        ? ((nxi + 31) / 32) * ((nyi + 3) / 4) * ((nzi + bt->zchunk - 1) / bt->zchunk) : 0;
+      pre[i + 1] = pre[i] + t;
+    }
+    c.tiles = pre.back();
+    CK(cudaMemcpyAsync(c.d_tile, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, bt->stream));
+    CK(cudaStreamSynchronize(bt->stream));
+  }
+  return WQL3D_OK;
+}
+
+template <typename T>
+void batch_enqueue_step(wql3d_batch *bt, double dt, int w_stride) {
+  launch_batch_sample<T>((const Blk<T> *)bt->blks, bt->times, bt->n, bt->cur, w_stride, bt->stream, &bt->launches);
+  BatchClass<T> cl[8];
+  int ncl = 0;
+  for (auto &c : bt->cls) {
+    if (c.shots.empty()) continue;
+    BatchClass<T> &b = cl[ncl++];
+    b.resp = c.resp;
+    b.sep = c.sep;
+    b.nshots = (int)c.shots.size();
+    b.shots = c.d_shots;
+    b.tile_prefix = c.d_tile;
+    b.shell_prefix = c.d_shell;
+    b.tiles = c.tiles;
+    b.shell_ctas = c.shell_ctas;
+    b.blks = (const Blk<T> *)bt->blks;
+    b.times = bt->times;
+  }
+  for (int st = 1; st <= 5; ++st) {
+    StageArgs a;
+    a.cur = bt->cur;
+    a.flags = F_ALL;
+    a.stage = st;
+    a.A = kRkA[st - 1];
+    a.Bdt = kRkB[st - 1] * dt;
+    a.dt = dt;
+    a.time = nullptr;
+    launch_batch_stage<T>(cl, ncl, a, bt->zchunk, bt->stream, &bt->launches);
+    bt->cur ^= 1;
+  }
+  launch_batch_advance<T>(bt->times, bt->n, dt, bt->stream, &bt->launches);
+}
+
+template <typename T>
+int batch_run(wql3d_batch *bt, double dt, int nsteps, int w_stride) {
+  // project-written tile autotuner: the first steps of the first run each try
+  // one z-chunk length of the interior tiles (the arithmetic of a point does
+  // not depend on it), timed with events; the fastest is kept
+  if (!bt->tuned) {
+    const int cand[6] = {4, 8, 12, 16, 24, 32};
+    float best = 1e30f;
+    int bestz = bt->zchunk;
+    for (int i = 0; i < 6 && nsteps > 0; ++i) {
+      bt->zchunk = cand[i];
+      if (int rc = batch_tiles(bt)) return rc;
+      cudaEvent_t e0, e1;
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      CK(cudaEventRecord(e0, bt->stream));
+      batch_enqueue_step<T>(bt, dt, w_stride);
+      CK(cudaEventRecord(e1, bt->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      bt->tune_log.push_back({cand[i], ms});
+      if (ms < best) { best = ms; bestz = cand[i]; }
+      --nsteps;
+    }
+    bt->zchunk = bestz;
+    if (int rc = batch_tiles(bt)) return rc;
+    bt->tuned = 1;
+  }
+  // CUDA graph of two steps of the whole batch, replayed
+  const int pairs = nsteps / 2;
+  if (pairs > 0) {
+    if (!bt->graph || bt->g_dt != dt || bt->g_w != w_stride || bt->g_cur != bt->cur || bt->g_z != bt->zchunk) {
+      if (bt->graph) { cudaGraphExecDestroy(bt->graph); bt->graph = nullptr; }
+      const int cur0 = bt->cur;
+      const int64_t l0 = bt->launches;
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
+      batch_enqueue_step<T>(bt, dt, w_stride);
+      batch_enqueue_step<T>(bt, dt, w_stride);
+      CK(cudaStreamEndCapture(bt->stream, &g));
+      CK(cudaGraphInstantiate(&bt->graph, g, 0));
+      cudaGraphDestroy(g);
+      bt->cur = cur0;
+      bt->g_dt = dt;
+      bt->g_w = w_stride;
+      bt->g_cur = cur0;
+      bt->g_z = bt->zchunk;
+      bt->g_launches = bt->launches - l0;
+      bt->launches = l0;
+    }
+    for (int k = 0; k < pairs; ++k) {
+      CK(cudaGraphLaunch(bt->graph, bt->stream));
+      bt->launches += bt->g_launches;
+    }
+  }
+  if (nsteps % 2) batch_enqueue_step<T>(bt, dt, w_stride);
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wql3d_batch_create(wql3d_domain *const *domains, int32_t n, wql3d_batch **out) {
+  if (!domains || n <= 0 || !out) return fail(WQL3D_EINVAL, "null argument");
+  if (!domains[0]) return fail(WQL3D_EINVAL, "null domain");
+  const int fp32 = domains[0]->fp32;
+  for (int i = 0; i < n; ++i) {
+    const wql3d_domain *d = domains[i];
+    if (!d) return fail(WQL3D_EINVAL, "null domain");
+    if (d->nblocks != 1 || d->slab || d->desc.remote_side || d->desc.mms || d->hb[0].mesh != WQL3D_MESH_CARTESIAN ||
+        d->desc.block[0].fd_operator != WQL3D_FD_TRADITIONAL6 || d->fp32 != fp32 || d->cur != domains[0]->cur)
+      return fail(WQL3D_EINVAL, "a batch holds one-block Cartesian traditional-6 domains of one precision");
+    for (int f = 0; f < 6; ++f)
+      if (d->desc.block[0].pml[f] && d->desc.block[0].npml > 0)
+        return fail(WQL3D_EINVAL, "batched shots carry no PML");
+  }
+  wql3d_batch *bt = new wql3d_batch();
+  bt->n = n;
+  bt->fp32 = fp32;
+  bt->doms.assign(domains, domains + n);
+  bt->cur = domains[0]->cur;
+  if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&bt->ev, cudaEventDisableTiming) != cudaSuccess) {
+    delete bt;
+    return fail(WQL3D_ECUDA, "batch stream");
+  }
+  bt->mem.stream = bt->stream;
+  auto bad = [&](int code) {
+    cudaStreamSynchronize(bt->stream);
+    bt->mem.release();
+    cudaEventDestroy(bt->ev);
+    cudaStreamDestroy(bt->stream);
+    delete bt;
+    return code;
+  };
+  const size_t bsz = fp32 ? sizeof(Blk<float>) : sizeof(Blk<double>);
+  std::vector<unsigned char> hb(bsz * (size_t)n);
+  std::vector<DevTime *> ht((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    if (fp32) memcpy(hb.data() + bsz * i, &domains[i]->bf[0], bsz);
+    else memcpy(hb.data() + bsz * i, &domains[i]->bd[0], bsz);
+    ht[(size_t)i] = domains[i]->time;
+  }
+  unsigned char *dblk = nullptr;
+  if (bt->mem.get(&dblk, hb.size(), false) != cudaSuccess || bt->mem.get(&bt->times, (size_t)n, false) != cudaSuccess)
+    return bad(fail(WQL3D_ENOMEM, "batch descriptors"));
+  bt->blks = dblk;
+  if (cudaMemcpyAsync(bt->blks, hb.data(), hb.size(), cudaMemcpyHostToDevice, bt->stream) != cudaSuccess ||
+      cudaMemcpyAsync(bt->times, ht.data(), sizeof(DevTime *) * n, cudaMemcpyHostToDevice, bt->stream) != cudaSuccess)
+    return bad(fail(WQL3D_ECUDA, "batch descriptor upload"));
+  // classes: response x separable shell
+  for (int i = 0; i < n; ++i) {
+    const int sep = fp32 ? domains[i]->bf[0].sep : domains[i]->bd[0].sep;
+    auto &c = bt->cls[domains[i]->response * 2 + (sep ? 1 : 0)];
+    c.resp = domains[i]->response;
+    c.sep = sep ? 1 : 0;
+    c.shots.push_back(i);
+  }
+  for (auto &c : bt->cls) {
+    if (c.shots.empty()) continue;
+    const size_t m = c.shots.size();
+    std::vector<int> shell(m + 1, 0);
+    for (size_t i = 0; i < m; ++i) {
+      const wql3d_domain *d = domains[c.shots[i]];
+      const long long sc = fp32 ? shell_count(d->bf[0]) : shell_count(d->bd[0]);
+      shell[i + 1] = shell[i] + (int)((sc + 127) / 128);
+    }
+    c.shell_ctas = shell.back();
+    if (bt->mem.get(&c.d_shots, m, false) != cudaSuccess || bt->mem.get(&c.d_tile, m + 1, false) != cudaSuccess ||
+        bt->mem.get(&c.d_shell, m + 1, false) != cudaSuccess)
+      return bad(fail(WQL3D_ENOMEM, "batch work lists"));
+    if (cudaMemcpyAsync(c.d_shots, c.shots.data(), sizeof(int) * m, cudaMemcpyHostToDevice, bt->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(c.d_shell, shell.data(), sizeof(int) * (m + 1), cudaMemcpyHostToDevice, bt->stream) !=
+            cudaSuccess)
+      return bad(fail(WQL3D_ECUDA, "batch work-list upload"));
+  }
+  if (const int rc = batch_tiles(bt)) return bad(rc);
+  *out = bt;
+  return WQL3D_OK;
+}
+
+int wql3d_batch_run(wql3d_batch *bt, double dt, int32_t nsteps, int32_t w_stride) {
+  if (!bt) return fail(WQL3D_EINVAL, "null batch");
+  if (nsteps <= 0) return WQL3D_OK;
+  // order after the shots' own queued work, and theirs after the batch
+  for (wql3d_domain *d : bt->doms) {
+    CK(cudaEventRecord(bt->ev, d->stream));
+    CK(cudaStreamWaitEvent(bt->stream, bt->ev, 0));
+  }
+  const int rc = bt->fp32 ? batch_run<float>(bt, dt, nsteps, w_stride) : batch_run<double>(bt, dt, nsteps, w_stride);
+  if (rc) return rc;
+  CK(cudaEventRecord(bt->ev, bt->stream));
+  for (wql3d_domain *d : bt->doms) {
+    CK(cudaStreamWaitEvent(d->stream, bt->ev, 0));
+    d->cur = bt->cur;
+  }
+  return WQL3D_OK;
+}
+
+int wql3d_batch_tuning(wql3d_batch *bt, int32_t *zchunk, int32_t *ntried, int32_t *zs, float *ms) {
+  if (!bt) return fail(WQL3D_EINVAL, "null batch");
+  if (zchunk) *zchunk = bt->zchunk;
+  if (ntried) *ntried = (int32_t)bt->tune_log.size();
+  for (size_t i = 0; i < bt->tune_log.size(); ++i) {
+    if (zs) zs[i] = bt->tune_log[i].first;
+    if (ms) ms[i] = bt->tune_log[i].second;
+  }
+  return WQL3D_OK;
+}
+
+int wql3d_batch_launches(wql3d_batch *bt, int64_t *launches) {
+  if (!bt || !launches) return fail(WQL3D_EINVAL, "null argument");
+  *launches = bt->launches;
+  return WQL3D_OK;
+}
+
+int wql3d_batch_synchronize(wql3d_batch *bt) {
+  if (!bt) return fail(WQL3D_EINVAL, "null batch");
+  CK(cudaStreamSynchronize(bt->stream));
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_batch_destroy(wql3d_batch *bt) {
+  if (!bt) return WQL3D_OK;
+  cudaStreamSynchronize(bt->stream);
+  if (bt->graph) cudaGraphExecDestroy(bt->graph);
+  bt->mem.release();
+  cudaEventDestroy(bt->ev);
+  cudaStreamDestroy(bt->stream);
+  delete bt;
+  return WQL3D_OK;
+}
 
 int wql3d_synchronize(wql3d_domain *d) {
   if (!d) return fail(WQL3D_EINVAL, "null domain");

@@ -2050,21 +2050,23 @@ struct SplitSmem {
   static constexpr size_t bytes = sizeof(T) * 2 * plane_elems;
 };
 
+// one 32 x TY column tile (tile indices bx, by, bz) of the strict interior;
+// smraw is the planes' dynamic shared memory
 template <typename T, int RESP, int TY>
-__global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(Blk<T> b, StageArgs a, int zchunk) {
+__device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const StageArgs &a, int zchunk, int bx, int by,
+                                                    int bz, unsigned char *smraw) {
   using SM = SplitSmem<T, TY>;
   constexpr int W = SM::W, H = SM::H, NP = SM::NP, VEC = SM::VEC, CH = SM::CH;
   constexpr int NT = 2 * NP;                                 // threads per block
   constexpr int NPOS = H * CH, PPT = (NPOS + NT - 1) / NT;
-  extern __shared__ __align__(16) unsigned char smraw[];
   T (*S)[8][H][W] = reinterpret_cast<T (*)[8][H][W]>(smraw);
   const int tid = threadIdx.x;
   const bool gS = tid >= NP;                                 // stress-rate group
   const int lt = gS ? tid - NP : tid;
   const int tx = lt & 31, ty = lt >> 5;
-  const int x0 = b.lo[0] + blockIdx.x * 32;
-  const int y0 = b.lo[1] + blockIdx.y * TY;
-  const int zs = b.lo[2] + blockIdx.z * zchunk;
+  const int x0 = b.lo[0] + bx * 32;
+  const int y0 = b.lo[1] + by * TY;
+  const int zs = b.lo[2] + bz * zchunk;
   if (zs > b.hi[2]) return;
   const int ze = min(zs + zchunk - 1, b.hi[2]);
   const int x = x0 + tx, y = y0 + ty;
@@ -2281,6 +2283,12 @@ __global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(B
   cp_async_wait_all();
 }
 
+template <typename T, int RESP, int TY>
+__global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(Blk<T> b, StageArgs a, int zchunk) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  interior_split_tile<T, RESP, TY>(b, a, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
+}
+
 // F <- F + dt*DF over every interior point (update_fields, split path): in place
 template <typename T>
 __global__ void k_update_inplace(Blk<T> b, int cur, double dt) {
@@ -2321,7 +2329,7 @@ __global__ void k_axpy_T(T *x, const T *r, long long n, double dt) {
 // Receiver gather at the start of step n (stage 1, before the update) and
 // time advance at the end of a step.
 template <typename T>
-__global__ void k_sample(Blk<T> b, int cur, DevTime *tm, int w_stride, int increment) {
+__device__ __forceinline__ void sample_block(const Blk<T> &b, int cur, DevTime *tm, int w_stride, int increment) {
   const T *F = cur ? b.F1 : b.F0;
   int n = tm->n;
   if (w_stride <= 0 || ((n - 1) % w_stride) != 0) return;
@@ -2348,6 +2356,11 @@ __global__ void k_sample(Blk<T> b, int cur, DevTime *tm, int w_stride, int incre
   }
   __syncthreads();
   if (threadIdx.x == 0 && increment) tm->nsamp = s + 1;
+}
+
+template <typename T>
+__global__ void k_sample(Blk<T> b, int cur, DevTime *tm, int w_stride, int increment) {
+  sample_block<T>(b, cur, tm, w_stride, increment);
 }
 
 static __global__ void k_advance(DevTime *tm, double dt) {

@@ -72,20 +72,48 @@ def random_shots(n: int = 48, seed: int = 7, nmin: int = 64, nmax: int = 192, h:
 
 
 class ShotBatch:
-    """Independent shots on one device, each a domain on its own stream."""
+    """Independent shots on one device.
 
-    def __init__(self, problems: Sequence[Problem], precision: str = "fp64", nsteps_hint: Optional[int] = None):
+    mode 'batched' (default): one launch per kernel kind and RK stage for
+    every shot (``wql3d_batch_*``: shot x tile work lists, the step pair in one
+    CUDA graph, interior tiles autotuned over the first steps).  mode
+    'streams': each shot a domain on its own stream, its step graph replayed
+    round-robin.  The shots share one time step (same spacing and rho_s_p, as
+    :func:`random_shots` builds them)."""
+
+    def __init__(self, problems: Sequence[Problem], precision: str = "fp64", nsteps_hint: Optional[int] = None,
+                 mode: str = "batched"):
+        import ctypes as C
+        from . import _lib
         from .domain import Domain
         self.domains = [Domain(p, precision=precision, nsteps_hint=nsteps_hint) for p in problems]
+        self.mode = mode
+        self.batch = None
+        self.dt = problems[0].dt()
+        self.w_stride = problems[0].w_stride
+        if any(abs(p.dt() - self.dt) > 1e-15 * self.dt for p in problems):
+            raise ValueError("the shots of a batch share one time step")
+        if mode == "batched":
+            arr = (C.c_void_p * len(self.domains))(*[d.handle.value for d in self.domains])
+            h = C.c_void_p()
+            _lib.check(_lib.load().wql3d_batch_create(arr, len(self.domains), C.byref(h)), "wql3d_batch_create")
+            self.batch = h
 
     @property
     def npoints(self) -> int:
         return sum(b.npoints for d in self.domains for b in d.blocks)
 
     def run(self, nsteps: int, chunk: int = 2):
-        """nsteps on every shot: each shot's step graph replayed ``chunk``
-        steps at a time, round-robin over the shots, so that all streams have
-        work queued at once."""
+        """nsteps on every shot.  Batched: one call; streams: each shot's step
+        graph replayed ``chunk`` steps at a time, round-robin over the shots,
+        so that all streams have work queued at once."""
+        from . import _lib
+        if self.batch is not None:
+            _lib.check(_lib.load().wql3d_batch_run(self.batch, float(self.dt), int(nsteps), int(self.w_stride)),
+                       "wql3d_batch_run")
+            for d in self.domains:
+                d.n += nsteps
+            return
         done = 0
         while done < nsteps:
             k = min(chunk, nsteps - done)
@@ -93,7 +121,29 @@ class ShotBatch:
                 d.run(k)
             done += k
 
+    def tuning(self):
+        """(chosen z-chunk, [(candidate, ms per step), ...]) of the batch's tile autotuner."""
+        import ctypes as C
+        from . import _lib
+        z, n = C.c_int32(), C.c_int32()
+        zs = (C.c_int32 * 16)()
+        ms = (C.c_float * 16)()
+        _lib.check(_lib.load().wql3d_batch_tuning(self.batch, C.byref(z), C.byref(n), zs, ms), "wql3d_batch_tuning")
+        return z.value, [(zs[i], ms[i]) for i in range(n.value)]
+
+    def kernel_launches(self) -> int:
+        import ctypes as C
+        from . import _lib
+        if self.batch is None:
+            return sum(d.kernel_launches() for d in self.domains)
+        v = C.c_int64()
+        _lib.check(_lib.load().wql3d_batch_launches(self.batch, C.byref(v)), "wql3d_batch_launches")
+        return v.value
+
     def synchronize(self):
+        from . import _lib
+        if self.batch is not None:
+            _lib.check(_lib.load().wql3d_batch_synchronize(self.batch), "wql3d_batch_synchronize")
         for d in self.domains:
             d.synchronize()
 
@@ -101,6 +151,10 @@ class ShotBatch:
         return [d.seismograms(0) for d in self.domains]
 
     def close(self):
+        from . import _lib
+        if self.batch is not None:
+            _lib.load().wql3d_batch_destroy(self.batch)
+            self.batch = None
         for d in self.domains:
             d.close()
         self.domains = []
