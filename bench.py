@@ -517,20 +517,27 @@ def shots_main(args, rank, world, local, barrier, max_over_ranks):
 
     res = {}
     clk = None
-    for prec in ("fp32", "fp64"):
-        batch = ShotBatch(ps, precision=prec, nsteps_hint=W + 2 * K + 4)
-        batch.run(W)
+    for prec in ("fp32", "fp64", "fp32-streams"):
+        mode = "streams" if prec.endswith("streams") else "batched"
+        batch = ShotBatch(ps, precision=prec[:4], nsteps_hint=W + 2 * K + 10, mode=mode)
+        batch.run(max(W, 8))           # warm-up; the batched mode's tile autotuner uses its first 6 steps
         batch.synchronize()
-        l0 = sum(d.kernel_launches() for d in batch.domains)
+        l0 = batch.kernel_launches()
         clocks = ClockSampler(local) if prec == "fp32" else None
         if clocks:
             clocks.start()
         ms = max_over_ranks(timed(batch, K))
         if clocks:
             clk = clocks.stop()
-        launches = sum(d.kernel_launches() for d in batch.domains) - l0
+        launches = batch.kernel_launches() - l0
         res[prec] = {"ms": ms, "value": world * npts * K / (ms / 1e3) / 1e9, "launches": int(launches),
-                     "seis": batch.seismograms(), "bytes": sum(d.device_bytes() for d in batch.domains)}
+                     "seis": batch.seismograms(), "bytes": sum(d.device_bytes() for d in batch.domains),
+                     "tuning": batch.tuning() if mode == "batched" else None}
+        if prec == "fp32-streams":
+            batch.close()
+            del batch
+            torch.cuda.empty_cache()
+            continue
         if prec == "fp32":
             # end to end: each shot's initial fields from pinned host, run, stations back
             hosts = [torch.zeros((9,) + tuple(q.blocks[0].nqrs[::-1]), dtype=torch.float64,
@@ -580,6 +587,12 @@ def shots_main(args, rank, world, local, barrier, max_over_ranks):
                              "alg_bytes_per_step": words * 4 * 5},
                 "cpu_baseline": cpu, "clocks": clk,
                 "fp64": {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms"] / K},
+                "batched": {"launches_per_step": r["launches"] / K, "zchunk": r["tuning"][0],
+                            "tuning_ms_per_step": {str(z): m for z, m in r["tuning"][1]},
+                            "what": "one launch per kernel kind and RK stage for all shots, two-step CUDA graph"},
+                "streams": {"value": res["fp32-streams"]["value"], "ms_per_step": res["fp32-streams"]["ms"] / K,
+                            "launches_per_step": res["fp32-streams"]["launches"] / K,
+                            "what": "each shot its own stream and step graph, replayed round-robin"},
                 "seismogram_rel_l2_fp32_vs_fp64": {"max": max(errs) if errs else None,
                                                    "median": float(np.median(errs)) if errs else None,
                                                    "shots_with_signal": len(errs)}}
