@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--only-fp32", action="store_true", help="time the FP32 path alone (profiling)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend of N > 1 runs (gloo: host-side swaps, e.g. two ranks on one GPU)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint / forward ratio leg")
     ap.add_argument("--adjoint-steps", type=int, default=64, help="steps of the adjoint ratio leg")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the full-duration FP32 accuracy leg")
@@ -260,12 +262,12 @@ def main():
         return
     import numpy as np
     import torch
-    torch.cuda.set_device(local)
+    torch.cuda.set_device(local % max(1, torch.cuda.device_count()))
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120))
     from waveqlab3d_q_gpu_b200 import build
     build.build()
     from waveqlab3d_q_gpu_b200.domain import Domain
@@ -284,9 +286,15 @@ def main():
     def max_over_ranks(x):
         if dist is None:
             return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        t = torch.tensor([x], device="cuda" if args.dist_backend == "nccl" else "cpu", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if world > 1 and world % 2 == 0 and args.workload == "hill":
+        pairs_main(args, rank, world, local, barrier, max_over_ranks, p, name)
+        dist.barrier()
+        dist.destroy_process_group()
+        return
 
     if args.workload == "shots":
         shots_main(args, rank, world, local, barrier, max_over_ranks)
@@ -416,6 +424,69 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def pairs_main(args, rank, world, local, barrier, max_over_ranks, p, name):
+    """N = 2, 4, 6, 8 GPUs: the two-block workload with one block per GPU, as
+    the reference runs it (one MPI rank per block): ranks 2k and 2k + 1 hold
+    blocks 1 and 2 of one copy of the problem and swap the interface face
+    trace every RK stage over NCCL into the library's receive buffer
+    (distributed.BlockRank).  N / 2 copies run side by side (weak scaling over
+    copies, each copy split over two GPUs).  Timed with CUDA events on each
+    rank's domain stream between barriers, max over ranks."""
+    import numpy as np
+    import torch
+    from waveqlab3d_q_gpu_b200.distributed import BlockRank
+    K, W = args.steps, max(args.warmup, 3)
+    block, peer = rank % 2, rank ^ 1
+    npts = sum(b.npoints for b in p.blocks)
+    br = BlockRank(p, block, backend=args.dist_backend, nsteps_hint=K + W + 4, peer=peer)
+    g = br.domain
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    br.run(W)
+    g.synchronize()
+    l0 = g.kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    br.run(K)
+    e1.record(stream)
+    g.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    launches = g.kernel_launches() - l0
+    # end to end: this rank's block from pinned host, K steps, stations and fields back
+    nq, nr, ns = p.blocks[block].nqrs
+    host = torch.zeros((9, ns, nr, nq), dtype=torch.float64, pin_memory=True).numpy()
+    barrier()
+    t0 = time.perf_counter()
+    g.set_fields(host, 0)
+    br.run(K)
+    seis = g.seismograms(0)
+    g.fields(0, out=host)
+    g.synchronize()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    br.close()
+    copies = world // 2
+    if rank == 0:
+        line = {"metric": METRIC, "value": copies * npts * K / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
+                "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": name, "points_per_copy": npts, "copies": copies,
+                           "parallelism": f"blocks2x{copies}", "backend": args.dist_backend,
+                           "exchange": "interface face trace every RK stage, NCCL send/recv into the library's "
+                                       "receive buffer"},
+                "e2e": {"value": copies * npts * K / e2e_s / 1e9, "unit": UNIT,
+                        "h2d_bytes_per_step": world * host.nbytes / K,
+                        "d2h_bytes_per_step": world * (host.nbytes + seis.nbytes) / K,
+                        "what": "every rank's block from pinned host, K steps, stations + final fields back"},
+                "gpu_launches": int(launches) * world, "roofline": None, "cpu_baseline": None, "clocks": clk}
+        print(json.dumps(line), flush=True)
 
 
 def fp32_accuracy_leg(args):

@@ -94,13 +94,15 @@ def remote_step(domain, xch, n: int, dt: float):
 
 
 class BlockRank:
-    """Block ``rank`` (0 or 1) of a two-block problem on this process."""
+    """Block ``rank`` (0 or 1) of a two-block problem on this process; its peer
+    holds the other block (process 1 - rank, or ``peer`` when several pairs
+    share the process group)."""
 
     def __init__(self, problem, rank: int, backend: str = "nccl", precision: str = "fp64",
-                 nsteps_hint: Optional[int] = None, exchange=None):
+                 nsteps_hint: Optional[int] = None, exchange=None, peer: Optional[int] = None):
         from .domain import Domain
         self.rank = rank
-        self.peer = 1 - rank
+        self.peer = 1 - rank if peer is None else peer
         self.domain = Domain(problem, precision=precision, nsteps_hint=nsteps_hint, remote_block=rank)
         dev = "cuda" if backend == "nccl" else None
         Mpeer = exchange_array(self.domain.interface_material(), self.peer, device=dev)
