@@ -28,8 +28,8 @@ static void launch_curv_fused(Blk<T> &b, const StageCtx &c, const StageArgs &a) 
   const unsigned gr = (unsigned)((npts + 127) / 128);
   const int mb = tuning().fused_minb;
   if (sizeof(T) == 8) {
-    if (mb == 3) launch_fused_mb<T, 3>(b, c, a, gr);
-    else launch_fused_mb<T, 2>(b, c, a, gr);
+    if (mb == 2) launch_fused_mb<T, 2>(b, c, a, gr);
+    else launch_fused_mb<T, 3>(b, c, a, gr);
   } else {
     if (mb == 6) launch_fused_mb<T, 6>(b, c, a, gr);
     else launch_fused_mb<T, 4>(b, c, a, gr);

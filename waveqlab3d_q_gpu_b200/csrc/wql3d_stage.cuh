@@ -37,7 +37,7 @@ struct Tuning {
   int generic = 0;    // 1: every point through the generic per-point kernel
   int lean = 1;       // curvilinear update: k_curv_point (0: generic point update k_curv_update)
   int curv_fused = 1; // curvilinear stage in one pass, k_curv_fused (0: derivative / memory-variable / point passes)
-  int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 2 (default) or 3 in FP64, 4 (default) or 6 in FP32
+  int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default) or 2 in FP64, 4 (default) or 6 in FP32
 };
 
 inline Tuning tuning() {
