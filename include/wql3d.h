@@ -308,6 +308,14 @@ int wql3d_adjoint_enable(wql3d_domain *d);
 int wql3d_adjoint_reset(wql3d_domain *d);
 int wql3d_adjoint_step(wql3d_domain *d, int n, double dt);
 int wql3d_adjoint_add_receivers(wql3d_domain *d, int block, const double *res);
+/* The same reversal without recomputing the stage inputs: wql3d_record_step
+   runs time step n like wql3d_time_step (one-block FP64 domain) and copies its
+   five stage inputs F^(0..4) into dev_out (5 x wql3d_field_volume doubles on
+   the device); wql3d_adjoint_step_recorded reverses step n from such a record
+   (t_n: the time at the start of step n).  A driver records a checkpoint
+   segment once and reverses it from the records. */
+int wql3d_record_step(wql3d_domain *d, double dt, int n, int w_stride, double *dev_out);
+int wql3d_adjoint_step_recorded(wql3d_domain *d, int n, double dt, double t_n, const double *dev_in);
 /* L^T R and (dL/d(lambda, mu, rho) F)^T R at the current fields, host arrays
    (R, Fbar: 9 x n; g: 3 x n; host_nb 0) */
 int wql3d_adjoint_rhs(wql3d_domain *d, int block, const double *R, double *Fbar, double *g);

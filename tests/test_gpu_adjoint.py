@@ -102,7 +102,8 @@ def test_misfit_gradient_matches_oracle_and_fd(wql3d_lib, oracle_lib, mesh):
 
 def test_autograd_function_and_checkpoint_interval(wql3d_lib):
     """torch.autograd through WaveformMisfit: the gradient is independent of the
-    checkpoint interval (K = 1, sqrt(N), N) and equals the solver's backward."""
+    checkpoint interval (K = 1, sqrt(N), N) and of recording the stage inputs
+    versus recomputing them, and equals the solver's backward."""
     import torch
     from waveqlab3d_q_gpu_b200.adjoint import AdjointSolver, waveform_misfit
     p = _problem("curvilinear")
@@ -112,15 +113,15 @@ def test_autograd_function_and_checkpoint_interval(wql3d_lib):
     rng = np.random.default_rng(2)
     observed = 0.8 * seis0 + 1e-3 * np.abs(seis0).max() * rng.standard_normal(seis0.shape)
     grads = []
-    for K in (1, None, N):
-        sol = AdjointSolver(p, N, checkpoint_every=K)
+    for K, rec in ((1, True), (None, True), (N, True), (None, False)):
+        sol = AdjointSolver(p, N, checkpoint_every=K, record_stages=rec)
         mat = torch.tensor(p.blocks[0].material, dtype=torch.float64, device="cuda", requires_grad=True)
         s0 = p.blocks[0].sources[0]
         mom = torch.tensor([[s0.mxx, s0.myy, s0.mzz, s0.mxy, s0.mxz, s0.myz]], dtype=torch.float64, device="cuda",
                            requires_grad=True)
         chi = waveform_misfit(mat, mom, sol, observed)
         chi.backward()
-        grads.append((mat.grad.cpu().numpy(), mom.grad.cpu().numpy(), float(chi)))
+        grads.append((mat.grad.cpu().numpy(), mom.grad.cpu().numpy(), float(chi.detach())))
         sol.close()
     for gm, gmom, chi in grads[1:]:
         assert chi == grads[0][2]

@@ -114,6 +114,8 @@ SIGNATURES = {
     "wql3d_adjoint_reset": [C.c_void_p],
     "wql3d_adjoint_step": [C.c_void_p, C.c_int, C.c_double],
     "wql3d_adjoint_add_receivers": [C.c_void_p, C.c_int, dp],
+    "wql3d_record_step": [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_void_p],
+    "wql3d_adjoint_step_recorded": [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p],
     "wql3d_adjoint_rhs": [C.c_void_p, C.c_int, dp, dp, dp],
     "wql3d_get_adjoint_fields": [C.c_void_p, C.c_int, dp],
     "wql3d_get_adjoint_gradient": [C.c_void_p, C.c_int, dp, dp],

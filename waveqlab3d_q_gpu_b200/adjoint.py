@@ -14,9 +14,14 @@ include/wql3d.h).
 
 Memory: sqrt(N)-step checkpointing with recomputation.  The forward run
 stores the fields every K = ceil(sqrt(N)) steps on the device; the reverse
-sweep restores each checkpoint, recomputes its K states into a device
-segment buffer, and reverses those steps.  Device storage is
-(ceil(N/K) + K) field states instead of N; the forward work is done twice.
+sweep restores each checkpoint, recomputes its K steps once while recording
+every step's five stage inputs into a device segment buffer
+(``wql3d_record_step``), and reverses those steps from the records
+(``wql3d_adjoint_step_recorded``).  Device storage is ceil(N/K) + 5 K field
+states instead of 5 N; the forward work is done twice.  With
+``record_stages=False`` the segment holds one state per step and every
+adjoint step recomputes its four inner stages (ceil(N/K) + K states, the
+forward work done almost three times).
 """
 from __future__ import annotations
 
@@ -35,7 +40,8 @@ from .problem import Problem
 class AdjointSolver:
     """Forward runs and adjoint sweeps of one elastic block on the current CUDA device."""
 
-    def __init__(self, problem: Problem, nsteps: int, checkpoint_every: Optional[int] = None):
+    def __init__(self, problem: Problem, nsteps: int, checkpoint_every: Optional[int] = None,
+                 record_stages: bool = True):
         if len(problem.blocks) != 1 or problem.response != "elastic":
             raise ValueError("the adjoint covers one elastic block")
         self.problem = problem
@@ -51,7 +57,10 @@ class AdjointSolver:
         _lib.check(L.wql3d_field_volume(self.h, 0, C.byref(ne)), "wql3d_field_volume")
         self.nchk = math.ceil(self.nsteps / self.K)
         self.ckpt = torch.empty((self.nchk, ne.value), dtype=torch.float64, device="cuda")
-        self.seg = torch.empty((self.K, ne.value), dtype=torch.float64, device="cuda")
+        self.record = bool(record_stages)
+        self.ne = ne.value
+        per = 5 if self.record else 1
+        self.seg = torch.empty((self.K, per * ne.value), dtype=torch.float64, device="cuda")
         blk = problem.blocks[0]
         self.nrec = 0 if blk.receivers is None else len(blk.receivers)
         self.nsrc = len(blk.sources)
@@ -100,14 +109,22 @@ class AdjointSolver:
             _lib.check(L.wql3d_load_fields(h, 0, self._ptr(self.ckpt[k])), "wql3d_load_fields")
             d.t = first * self.dt
             for j in range(steps):
+                if self.record:
+                    _lib.check(L.wql3d_record_step(h, float(self.dt), first + j + 1, int(self.problem.w_stride),
+                                                   self._ptr(self.seg[j])), "wql3d_record_step")
+                    continue
                 _lib.check(L.wql3d_store_fields(h, 0, self._ptr(self.seg[j])), "wql3d_store_fields")
                 if j + 1 < steps:
                     d.time_step_RK(first + j + 1)
             for j in range(steps - 1, -1, -1):
                 n = first + j
-                _lib.check(L.wql3d_load_fields(h, 0, self._ptr(self.seg[j])), "wql3d_load_fields")
-                d.t = n * self.dt
-                _lib.check(L.wql3d_adjoint_step(h, n + 1, float(self.dt)), "wql3d_adjoint_step")
+                if self.record:
+                    _lib.check(L.wql3d_adjoint_step_recorded(h, n + 1, float(self.dt), n * self.dt,
+                                                             self._ptr(self.seg[j])), "wql3d_adjoint_step_recorded")
+                else:
+                    _lib.check(L.wql3d_load_fields(h, 0, self._ptr(self.seg[j])), "wql3d_load_fields")
+                    d.t = n * self.dt
+                    _lib.check(L.wql3d_adjoint_step(h, n + 1, float(self.dt)), "wql3d_adjoint_step")
                 if self.nrec:
                     r = np.ascontiguousarray(res[n])
                     _lib.check(L.wql3d_adjoint_add_receivers(h, 0, _ptr(r)), "wql3d_adjoint_add_receivers")

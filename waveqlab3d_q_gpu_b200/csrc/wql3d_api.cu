@@ -1686,6 +1686,44 @@ int wql3d_adjoint_step(wql3d_domain *d, int n, double dt) {
   return WQL3D_OK;
 }
 
+int wql3d_record_step(wql3d_domain *d, double dt, int n, int w_stride, double *dev_out) {
+  if (!d || d->fp32 || d->nblocks != 1 || d->slab || (d->has_iface && d->iface.remote) || !dev_out)
+    return fail(WQL3D_EINVAL, "recording covers one-block FP64 domains and a device buffer");
+  Blk<double> &b = d->bd[0];
+  const size_t ne = (size_t)9 * b.vol;
+  DevTime h;
+  CK(cudaMemcpyAsync(&h, d->time, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  h.n = n;
+  CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
+  if (int rc = enqueue_sample<double>(d, w_stride)) return rc;
+  for (int s = 1; s <= 5; ++s) {
+    CK(cudaMemcpyAsync(dev_out + (s - 1) * ne, d->cur ? b.F1 : b.F0, sizeof(double) * ne, cudaMemcpyDeviceToDevice,
+                       d->stream));
+    if (int rc = enqueue_stage<double>(d, s, dt, F_ALL)) return rc;
+  }
+  k_advance<<<1, 32, 0, d->stream>>>(d->time, dt);
+  d->launches++;
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
+int wql3d_adjoint_step_recorded(wql3d_domain *d, int n, double dt, double t_n, const double *dev_in) {
+  if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
+  if (!dev_in) return fail(WQL3D_EINVAL, "null stage inputs");
+  (void)n;
+  Blk<double> &b = d->bd[0];
+  AdjBlk A = d->adj;
+  const size_t ne = (size_t)9 * b.vol;
+  for (int s = 0; s < 5; ++s) A.S[s] = const_cast<double *>(dev_in) + s * ne;
+  for (int s = 5; s >= 1; --s) {
+    adj_launch_stage(b, A, s, kRkB[s - 1] * dt, kRkA[s - 1], d->stream, &d->launches);
+    adj_launch_moment(b, A, t_n + kRkC[s - 1] * dt, d->stream, &d->launches);
+  }
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
 int wql3d_adjoint_add_receivers(wql3d_domain *d, int bi, const double *res) {
   if (!d || !d->adj_on) return fail(WQL3D_ESTATE, "adjoint not enabled");
   if (bi != 0 || !res) return fail(WQL3D_EINVAL, "block / residuals");
