@@ -276,6 +276,15 @@ int wql3d_device_bytes(wql3d_domain *d, int64_t *bytes);
 int wql3d_kernel_launches(wql3d_domain *d, int64_t *launches);
 const char *wql3d_last_error(void);
 
+/* Curvilinear block mesh by 3-D transfinite interpolation on the device
+   (Gen3_Curve_Mesh of Curve_Grid_3D3, src/grid.f90:2292-2418, :473-1909):
+   faces holds the six boundary surfaces, x / y / z each, in the order left,
+   right (q = 0 / 1; ns x nr, r fastest), top, bottom (r = 0 / 1; ns x nq),
+   front, back (s = 0 / 1; nr x nq); coords receives 3 x ns x nr x nq with q
+   fastest (the wql3d_block_desc.coords layout with host_nb 0).  A set-up
+   call: it allocates and frees its device buffers. */
+int wql3d_tfi_grid(const double *faces, int32_t nq, int32_t nr, int32_t ns, double *coords);
+
 /* Parameter updates between runs (the inversion loop of an adjoint driver):
    material lambda, mu, rho of one block (3 components, host_nb 0) and the
    moment tensors of its sources (nsrc x 6: mxx myy mzz mxy mxz myz). */

@@ -80,6 +80,7 @@ def lib() -> C.CDLL:
         L.orc_adjoint_rhs.restype = C.c_int
         L.orc_adjoint_rhs.argtypes = [vp, C.c_int, dp, dp, dp]
         L.orc_adjoint_moment.argtypes = [vp, C.c_int, C.c_double, dp, dp]
+        L.orc_tfi_grid.argtypes = [dp, C.c_int, C.c_int, C.c_int, dp]
         _LIB = L
     return _LIB
 
@@ -410,3 +411,13 @@ class OracleDomain:
         mb = (C.c_double * 2)()
         lib().orc_final_state(self.handle, C.byref(mf), C.byref(me), mb)
         return mf.value, me.value, (mb[0], mb[1])
+
+
+def tfi_grid(faces: np.ndarray, nqrs) -> np.ndarray:
+    """Transfinite-interpolation block mesh (Gen3_Curve_Mesh of
+    src/grid.f90:2292-2418) from packed surfaces; (3, ns, nr, nq)."""
+    nq, nr, ns = nqrs
+    f = np.ascontiguousarray(faces, dtype=np.float64)
+    out = np.zeros((3, ns, nr, nq))
+    lib().orc_tfi_grid(_dptr(f), int(nq), int(nr), int(ns), _dptr(out))
+    return out

@@ -2275,3 +2275,48 @@ void orc_adjoint_moment(void *dv, int bi, double t, const double *Rin, double *g
     }
   }
 }
+
+/* ======================================================================== */
+/* Transfinite interpolation of a block from its six boundary surfaces,      */
+/* Gen3_Curve_Mesh of src/grid.f90:2292-2418.  faces: left, right (3 x ns x  */
+/* nr), top, bottom (3 x ns x nq), front, back (3 x nr x nq), first index    */
+/* slowest; out: 3 x ns x nr x nq, q fastest.                                */
+/* ======================================================================== */
+void orc_tfi_grid(const double *faces, int nq, int nr, int ns, double *out) {
+  const long nLR = 3L * ns * nr, nTB = 3L * ns * nq;
+  const double *Lf = faces, *Rf = Lf + nLR, *Tf = Rf + nLR, *Bf = Tf + nTB, *Ff = Bf + nTB, *Kf = Ff + 3L * nr * nq;
+  const double hq = 1.0 / (double)(nq - 1), hr = 1.0 / (double)(nr - 1), hs = 1.0 / (double)(ns - 1);
+  const long npt = (long)nq * nr * ns;
+#define TL(c, j, k) Lf[((long)(c) * ns + (k)) * nr + (j)]
+#define TR(c, j, k) Rf[((long)(c) * ns + (k)) * nr + (j)]
+#define TT(c, i, k) Tf[((long)(c) * ns + (k)) * nq + (i)]
+#define TB(c, i, k) Bf[((long)(c) * ns + (k)) * nq + (i)]
+#define TF(c, i, j) Ff[((long)(c) * nr + (j)) * nq + (i)]
+#define TK(c, i, j) Kf[((long)(c) * nr + (j)) * nq + (i)]
+  for (int c = 0; c < 3; ++c)
+    for (int k = 0; k < ns; ++k)
+      for (int j = 0; j < nr; ++j)
+        for (int i = 0; i < nq; ++i) {
+          const double q = (double)i * hq, r = (double)j * hr, s = (double)k * hs;
+          const double U = (1.0 - q) * TL(c, j, k) + q * TR(c, j, k);
+          const double V = (1.0 - r) * TT(c, i, k) + r * TB(c, i, k);
+          const double W = (1.0 - s) * TF(c, i, j) + s * TK(c, i, j);
+          const double UW = (1.0 - q) * ((1.0 - r) * TL(c, 0, k) + r * TL(c, nr - 1, k)) +
+                            q * ((1.0 - r) * TR(c, 0, k) + r * TR(c, nr - 1, k));
+          const double UV = (1.0 - r) * ((1.0 - s) * TT(c, i, 0) + s * TT(c, i, ns - 1)) +
+                            r * ((1.0 - s) * TB(c, i, 0) + s * TB(c, i, ns - 1));
+          const double VW = (1.0 - s) * ((1.0 - q) * TF(c, 0, j) + q * TF(c, nq - 1, j)) +
+                            s * ((1.0 - q) * TK(c, 0, j) + q * TK(c, nq - 1, j));
+          const double UVW1 = (1.0 - q) * ((1.0 - r) * ((1.0 - s) * TT(c, 0, 0) + s * TT(c, 0, ns - 1)) +
+                                           r * ((1.0 - s) * TB(c, 0, 0) + s * TB(c, 0, ns - 1)));
+          const double UVW2 = q * ((1.0 - r) * ((1.0 - s) * TT(c, nq - 1, 0) + s * TT(c, nq - 1, ns - 1)) +
+                                   r * ((1.0 - s) * TB(c, nq - 1, 0) + s * TB(c, nq - 1, ns - 1)));
+          out[(long)c * npt + ((long)k * nr + j) * nq + i] = U + V + W - UV - UW - VW + UVW1 + UVW2;
+        }
+#undef TL
+#undef TR
+#undef TT
+#undef TB
+#undef TF
+#undef TK
+}

@@ -98,6 +98,7 @@ SIGNATURES = {
     "wql3d_last_error": [],
     "wql3d_max_abs_noalloc": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p],
     "wql3d_reset_samples": [C.c_void_p],
+    "wql3d_tfi_grid": [dp, C.c_int32, C.c_int32, C.c_int32, dp],
     "wql3d_batch_create": [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)],
     "wql3d_batch_run": [C.c_void_p, C.c_double, C.c_int32, C.c_int32],
     "wql3d_batch_tuning": [C.c_void_p, ip, ip, ip, C.POINTER(C.c_float)],
