@@ -6,13 +6,14 @@
 module wql3d_c
   use iso_c_binding
   implicit none
-  integer(c_int), parameter :: WQL3D_ABI_VERSION = 3
+  integer(c_int), parameter :: WQL3D_ABI_VERSION = 4
   integer(c_int), parameter :: WQL3D_FP64 = 0, WQL3D_FP32_COMPENSATED = 1
   integer(c_int), parameter :: WQL3D_FD_TRADITIONAL6 = 0, WQL3D_FD_UPWIND4 = 1
   integer(c_int), parameter :: WQL3D_MESH_CARTESIAN = 0, WQL3D_MESH_CURVILINEAR = 1
   integer(c_int), parameter :: WQL3D_IFACE_LOCKED = 0, WQL3D_IFACE_SLIP_WEAKENING = 1, WQL3D_IFACE_LINEAR = 2
   integer(c_int), parameter :: WQL3D_IFACE_RATE_STATE = 3
-  integer(c_int), parameter :: WQL3D_FAULT_MAPS = 0, WQL3D_FAULT_TPV5 = 1, WQL3D_FAULT_TPV101 = 2, WQL3D_FAULT_TPV102 = 3
+  integer(c_int), parameter :: WQL3D_FAULT_MAPS = 0, WQL3D_FAULT_TPV5 = 1, WQL3D_FAULT_TPV101 = 2, WQL3D_FAULT_TPV102 = 3, &
+                                WQL3D_FAULT_TPV28 = 4
 
   type, bind(C) :: wql3d_block_desc
      integer(c_int32_t) :: nq, nr, ns, mesh, f32_literal
@@ -33,6 +34,7 @@ module wql3d_c
      integer(c_int32_t) :: coupling, fault_problem, serial_shared
      real(c_double)     :: fs, fd, Dc
      type(c_ptr)        :: iface_tau0, iface_fs
+     real(c_double)     :: fault_stress(6)
      integer(c_int32_t) :: max_samples
      integer(c_int32_t) :: mms
      real(c_double)     :: mms_nt, mms_nx, mms_ny, mms_nz

@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define WQL3D_ABI_VERSION 3
+#define WQL3D_ABI_VERSION 4
 
 /* status codes */
 #define WQL3D_OK 0
@@ -83,6 +83,9 @@ extern "C" {
 #define WQL3D_FAULT_TPV5 1
 #define WQL3D_FAULT_TPV101 2          /* rate-and-state TPV101 / TPV102 prestress and parameters */
 #define WQL3D_FAULT_TPV102 3
+#define WQL3D_FAULT_TPV28 4           /* slip-weakening TPV28: fault_stress projected on each fault point's
+                                         (n, m, l) basis plus the nucleation shear, fs / fd / Dc of
+                                         src/Interface_Condition.f90:1459-1474, 2049-2076 */
 
 /* fault outputs of wql3d_get_fault_output (src/domain.f90:782-845,
    src/fault_output.f90:73-122): [component][ns][nr] doubles */
@@ -141,13 +144,15 @@ typedef struct wql3d_domain_desc {
   double strength_s[8];        /* fQ8 S strengths */
   double strength_p[8];        /* fQ8 P strengths */
   int32_t coupling;            /* WQL3D_IFACE_* (two blocks) */
-  int32_t fault_problem;       /* WQL3D_FAULT_MAPS or WQL3D_FAULT_TPV5 */
+  int32_t fault_problem;       /* WQL3D_FAULT_* */
   int32_t serial_shared;       /* 1: both sides' interface solves add to the slip rate (twice per
                                   stage), as in the reference's one-process two-block run;
                                   0: once per stage, as in its one-rank-per-block run */
   double fs, fd, Dc;           /* slip-weakening parameters */
   const double *iface_tau0;    /* optional (3, ns, nr): initial tractions n, m, l on the interface */
   const double *iface_fs;      /* optional (ns, nr) static friction map */
+  double fault_stress[6];      /* WQL3D_FAULT_TPV28 background stress (sxx, syy, szz, sxy, sxz, syz);
+                                  all zero: (-60, 0, 60, 0, 29.38, 0) of src/initial_stress_condition.f90:78-84 */
   int32_t max_samples;         /* receiver samples kept on the device */
   /* manufactured solution (src/mms.f90:136-235): when mms != 0 every point's
      rates get the forcing u*_t - L(u*) and the face SATs the exact boundary

@@ -42,6 +42,7 @@ class OrcIface(C.Structure):
         ("fs", C.c_double), ("fd", C.c_double), ("Dc", C.c_double), ("alpha_lin", C.c_double),
         ("tau0_n", C.POINTER(C.c_double)), ("tau0_l", C.POINTER(C.c_double)),
         ("tau0_m", C.POINTER(C.c_double)), ("fs_map", C.POINTER(C.c_double)),
+        ("s0", C.c_double * 6),
     ]
 
 
@@ -194,6 +195,8 @@ class OracleDomain:
             I.double_ds = 1 if ip.serial_shared else 0
             I.problem = FAULT_PROBLEMS[ip.problem]
             I.fs, I.fd, I.Dc = ip.fs, ip.fd, ip.Dc
+            if ip.stress is not None:
+                I.s0[:] = [float(v) for v in ip.stress]
             for name in ("tau0_n", "tau0_l", "tau0_m", "fs_map"):
                 a = getattr(ip, name)
                 if a is not None:

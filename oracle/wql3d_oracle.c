@@ -1559,8 +1559,30 @@ static double boxcar(double x, double w) {
 }
 
 /* initial tractions on the fault: src/Interface_Condition.f90:1802-1830 (TPV5),
-   or the per-point maps of the description */
-static void fault_prestress(const oiface *I, long k, const double x[3], double *T0n, double *T0m, double *T0l) {
+   :2049-2076 with src/initial_stress_condition.f90:78-84 (TPV28: the uniform
+   stress tensor projected on the point's (n, m, l) basis plus the nucleation
+   shear), or the per-point maps of the description */
+static void fault_prestress(const oiface *I, long k, const double x[3], const double n[3], const double m[3],
+                            const double l[3], double *T0n, double *T0m, double *T0l) {
+  if (I->d.problem == ORC_FAULT_TPV28) {
+    static const double tpv28[6] = {-60.0, 0.0, 60.0, 0.0, 29.38, 0.0};
+    const double *s0 = tpv28;
+    for (int c = 0; c < 6; ++c)
+      if (I->d.s0[c] != 0.0) s0 = I->d.s0;
+    const double sxx = s0[0], syy = s0[1], szz = s0[2], sxy = s0[3], sxz = s0[4], syz = s0[5];
+    const double Tx = n[0] * sxx + n[1] * sxy + n[2] * sxz;
+    const double Ty = n[0] * sxy + n[1] * syy + n[2] * syz;
+    const double Tz = n[0] * sxz + n[1] * syz + n[2] * szz;
+    *T0n = n[0] * Tx + n[1] * Ty + n[2] * Tz;
+    *T0m = m[0] * Tx + m[1] * Ty + m[2] * Tz;
+    *T0l = l[0] * Tx + l[1] * Ty + l[2] * Tz;
+    const double r = sqrt((x[1] - 7.5) * (x[1] - 7.5) + x[2] * x[2]);
+    double nuke = 0.0;
+    if (r <= 1.4) nuke = 11.60;
+    else if (r >= 1.4 && r <= 2.0) nuke = 5.8 * (1.0 + cos(PI_WP * (r - 1.4) / 0.6));
+    *T0l = *T0l + nuke;
+    return;
+  }
   if (I->d.problem == ORC_FAULT_TPV5) {
     double tl = 70.0;
     tl = tl + 8.0 * boxcar(x[1] - 7.5, 1.5) * boxcar(x[2] + 7.5, 1.5);
@@ -1578,6 +1600,9 @@ static double fault_strength(const oiface *I, long k, const double x[3], double 
   if (I->d.problem == ORC_FAULT_TPV5) {
     fs = 0.677; fd = 0.525; Dc = 0.4;
     fs = fs + 1.0e10 * (1.0 - boxcar(x[1], 15.0) * boxcar(x[2], 15.0));
+  } else if (I->d.problem == ORC_FAULT_TPV28) { /* src/Interface_Condition.f90:1459-1474 */
+    fs = 0.677; fd = 0.373; Dc = 0.4;
+    fs = fs + 1.0e10 * (1.0 - boxcar(x[1], 15.0) * boxcar(x[2], 18.0));
   } else {
     fs = I->fsm[k]; fd = I->d.fd; Dc = I->d.Dc;
   }
@@ -1640,12 +1665,13 @@ static void linear_friction(const double *U, const double *V, double *P, double 
 
 /* Slip_Weakening_Friction with the closed-form solve,
    src/Interface_Condition.f90:745-916 and 1095-1168 */
-static void slip_weakening(const oiface *I, long k, const double x[3], const double *U, const double *V, double *P,
-                           double *Q, double Z1s, double Z2s, double Z1p, double Z2p, double slip) {
+static void slip_weakening(const oiface *I, long k, const double x[3], const double n[3], const double m[3],
+                           const double l[3], const double *U, const double *V, double *P, double *Q, double Z1s,
+                           double Z2s, double Z1p, double Z2p, double slip) {
   char_t c;
   characteristics(U, V, Z1s, Z2s, Z1p, Z2p, &c);
   double T0n, T0m, T0l;
-  fault_prestress(I, k, x, &T0n, &T0m, &T0l);
+  fault_prestress(I, k, x, n, m, l, &T0n, &T0m, &T0l);
   P[0] = (c.q[0] - c.phi[0]) / Z2p; P[3] = c.phi[0];
   Q[0] = (c.p[0] + c.phi[0]) / Z1p; Q[3] = c.phi[0];
   double tau_lock = sqrt((T0l + c.phi[2]) * (T0l + c.phi[2]) + (T0m + c.phi[1]) * (T0m + c.phi[1]));
@@ -1926,7 +1952,7 @@ void orc_iface_couple(odom *D, int ib, double t, int stage) {
           rate_state(x, t, n, m, l, u, v, P, Q, Z1s, Z2s, Z1p, Z2p, I->W[k], &Vrs);
           break;
         case ORC_IFACE_SLIP_WEAKENING:
-          slip_weakening(I, k, x, u, v, P, Q, Z1s, Z2s, Z1p, Z2p, I->S[3][k]);
+          slip_weakening(I, k, x, n, m, l, u, v, P, Q, Z1s, Z2s, Z1p, Z2p, I->S[3][k]);
           break;
         case ORC_IFACE_LINEAR:
           linear_friction(u, v, P, Q, Z1s, Z2s, Z1p, Z2p, 1.0e14);
@@ -1946,7 +1972,7 @@ void orc_iface_couple(odom *D, int ib, double t, int stage) {
       if (stage == 1 && record) {
         double T0n = 0.0, T0m = 0.0, T0l = 0.0;
         if (I->d.coupling == ORC_IFACE_RATE_STATE) rs_prestress(x, t, n, m, l, &T0n, &T0m, &T0l);
-        else if (I->d.coupling != ORC_IFACE_LOCKED) fault_prestress(I, k, x, &T0n, &T0m, &T0l);
+        else if (I->d.coupling != ORC_IFACE_LOCKED) fault_prestress(I, k, x, n, m, l, &T0n, &T0m, &T0l);
         /* Couple_Interface_x overwrites components 1:3 with v_hat - u_hat */
         for (int c = 0; c < 3; ++c) {
           double sv = Q[c] - P[c];

@@ -29,7 +29,7 @@ enum {
 /* interface coupling laws, src/Interface_Condition.f90 */
 enum { ORC_FD_TRADITIONAL6 = 0, ORC_FD_UPWIND4 = 1 };
 enum { ORC_IFACE_LOCKED = 0, ORC_IFACE_SLIP_WEAKENING = 1, ORC_IFACE_LINEAR = 2, ORC_IFACE_RATE_STATE = 3 };
-enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1, ORC_FAULT_TPV101 = 2, ORC_FAULT_TPV102 = 3 };
+enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1, ORC_FAULT_TPV101 = 2, ORC_FAULT_TPV102 = 3, ORC_FAULT_TPV28 = 4 };
 /* fault outputs, src/domain.f90:782-845 and src/fault_output.f90:73-122; layout [comp][ns][nr] */
 enum { ORC_FO_S = 0, ORC_FO_SVEL = 1, ORC_FO_UHAT = 2, ORC_FO_VHAT = 3, ORC_FO_STATE = 4, ORC_FO_TRUP = 5 };
 
@@ -70,13 +70,17 @@ typedef struct {
   int double_ds;           /* 1: one-process two-block run (src/domain.f90:615-644): Interface_RHS runs
                               once per block side on the shared iface, so DS and DW grow twice per stage */
   int problem;             /* ORC_FAULT_MAPS: prestress/static friction from the maps below;
-                              ORC_FAULT_TPV5: src/Interface_Condition.f90:1283-1299, 1822-1830 */
+                              ORC_FAULT_TPV5: src/Interface_Condition.f90:1283-1299, 1822-1830;
+                              ORC_FAULT_TPV28: :1459-1474, 2049-2076 */
   /* slip-weakening / linear friction parameters (uniform over the fault) */
   double fs, fd, Dc, alpha_lin;
   const double *tau0_n;    /* optional per-face-point initial normal traction (nr*ns) */
   const double *tau0_l;    /* optional initial shear traction along l (nr*ns) */
   const double *tau0_m;    /* optional initial shear traction along m (nr*ns) */
   const double *fs_map;    /* optional per-point static friction (nr*ns) */
+  /* ORC_FAULT_TPV28 background stress (sxx, syy, szz, sxy, sxz, syz); all zero:
+     the tensor of src/initial_stress_condition.f90:78-84 */
+  double s0[6];
 } orc_iface_desc;
 
 void *orc_create(int nblocks, const orc_desc *blocks, const orc_iface_desc *iface);

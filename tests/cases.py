@@ -250,3 +250,28 @@ def tpv101_case(serial_shared=False, n=21, t_final=0.5, problem="TPV101"):
     p = tpv5_case(serial_shared=serial_shared, n=n, t_final=t_final)
     p.interface = InterfaceParams(coupling="rate-and-state_friction", problem=problem, serial_shared=serial_shared)
     return p
+
+
+def tpv28_case(grid, serial_shared=False, n=21, t_final=0.5):
+    """test_problems/test_rup_curv_fric.in of the reference: two 21^3
+    curvilinear blocks on [-3,0] and [0,3] x [6,9] x [-1.5,1.5] whose shared
+    q-face carries the 'analytical_test_problem' fault profile (lc = 1 on
+    block 1, rc = 1 on block 2; src/grid.f90:777-829), TPV28 slip-weakening
+    prestress and strength (src/Interface_Condition.f90:1459-1474, 2049-2076),
+    free surface at y = 6, absorbing elsewhere, CFL 0.5, stations at the fault
+    centre on each side.  grid(surfaces, nqrs) builds the volume mesh (the
+    oracle's or the device's transfinite interpolation)."""
+    from waveqlab3d_q_gpu_b200.mesh import block_surfaces
+    from waveqlab3d_q_gpu_b200.problem import InterfaceParams
+    blocks = []
+    for side in range(2):
+        a = (-3.0, 6.0, -1.5) if side == 0 else (0.0, 6.0, -1.5)
+        b = (0.0, 9.0, 1.5) if side == 0 else (3.0, 9.0, 1.5)
+        lc, rc = (1.0, 0.0) if side == 0 else (0.0, 1.0)
+        X = grid(block_surfaces((n, n, n), a, b, lc, rc, "analytical_test_problem"), (n, n, n))
+        blocks.append(Block(nqrs=(n, n, n), aqrs=a, bqrs=b, rho_s_p=(2.67, 3.464, 6.0),
+                            lqrs=(1, 2, 1) if side == 0 else (0, 2, 1), rqrs=(0, 1, 1) if side == 0 else (1, 1, 1),
+                            coords=X, receivers=np.array([[0.0, 7.5, 0.0]])))
+    ip = InterfaceParams(coupling="slip-weakening_friction", problem="TPV28", serial_shared=serial_shared)
+    return Problem(blocks=blocks, response="elastic", type_of_mesh="curvilinear", t_final=t_final, CFL=0.5,
+                   interface=ip, w_stride=1)

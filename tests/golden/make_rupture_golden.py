@@ -1,6 +1,8 @@
-"""Write tests/golden/tpv5_cartesian_truth.npz from the reference's archived
-rupture output (test_problems/truth/1, the TPV5 two-block Cartesian problem of
-test_problems/test_rup_cart_fric.in).
+"""Write tests/golden/tpv5_cartesian_truth.npz and tpv28_curvilinear_truth.npz
+from the reference's archived rupture output: test_problems/truth/1 (the TPV5
+two-block Cartesian problem of test_problems/test_rup_cart_fric.in) and
+test_problems/truth/2 (the TPV28 two-block curvilinear problem of
+test_problems/test_rup_curv_fric.in).
 
 The archived files are float32 in the layout python/read_binary.py reads:
 46 samples x ncomp x 21 x 21 (y fastest).  Only the first NSAMP samples are
@@ -21,17 +23,22 @@ NSEIS = 12
 FILES = (("S", 4), ("Svel", 3), ("Uface", 9), ("Vface", 9), ("Uhat", 6), ("Vhat", 6), ("trup", 1))
 
 
-def main(ref: str) -> str:
-    base = os.path.join(ref, "test_problems", "truth", "1", "test_rup_cart_fric")
+def one(ref: str, truth: str, stem: str, fname: str) -> str:
+    base = os.path.join(ref, "test_problems", "truth", truth, stem)
     out = {}
     for name, nc in FILES:
         a = np.fromfile(base + "_interface." + name, dtype=np.float32).reshape(46, nc, 21, 21)
         out[name] = a[:NSAMP].copy()
     out["seis_block1"] = np.loadtxt(base + "_21_11_11.dat")[:NSEIS]
     out["seis_block2"] = np.loadtxt(base + "_1_11_11.dat")[:NSEIS]
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tpv5_cartesian_truth.npz")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), fname)
     np.savez_compressed(path, **out)
     return path
+
+
+def main(ref: str) -> str:
+    return "\n".join([one(ref, "1", "test_rup_cart_fric", "tpv5_cartesian_truth.npz"),
+                      one(ref, "2", "test_rup_curv_fric", "tpv28_curvilinear_truth.npz")])
 
 
 if __name__ == "__main__":

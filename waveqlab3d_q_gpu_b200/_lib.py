@@ -11,7 +11,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libwql3d.so")
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 OK = 0
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENONFINITE", -5: "ESTATE"}
 
@@ -44,7 +44,7 @@ class DomainDesc(C.Structure):
         ("strength_s", C.c_double * 8), ("strength_p", C.c_double * 8),
         ("coupling", C.c_int32), ("fault_problem", C.c_int32), ("serial_shared", C.c_int32),
         ("fs", C.c_double), ("fd", C.c_double), ("Dc", C.c_double),
-        ("iface_tau0", dp), ("iface_fs", dp),
+        ("iface_tau0", dp), ("iface_fs", dp), ("fault_stress", C.c_double * 6),
         ("max_samples", C.c_int32),
         ("mms", C.c_int32), ("mms_nt", C.c_double), ("mms_nx", C.c_double), ("mms_ny", C.c_double),
         ("mms_nz", C.c_double),

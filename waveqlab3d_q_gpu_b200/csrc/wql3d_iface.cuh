@@ -101,6 +101,101 @@ inline void tpv5_point(const double x[3], double *T0n, double *T0m, double *T0l,
   *fs = 0.677 + 1.0e10 * (1.0 - host_boxcar(x[1], 15.0) * host_boxcar(x[2], 15.0));
 }
 
+// TPV28 background stress (src/initial_stress_condition.f90:78-84), unless
+// the description gives one
+inline const double *tpv28_stress(const wql3d_domain_desc &desc) {
+  static const double s0[6] = {-60.0, 0.0, 60.0, 0.0, 29.38, 0.0};
+  for (int c = 0; c < 6; ++c)
+    if (desc.fault_stress[c] != 0.0) return desc.fault_stress;
+  return s0;
+}
+
+// TPV28 prestress and static friction at one fault point
+// (src/Interface_Condition.f90:2049-2076 and 1459-1474): the stress tensor
+// as tractions on n, rotated onto (n, m, l), plus the nucleation shear on T0_l
+inline void tpv28_point(const double s0[6], const double x[3], const double n[3], const double m[3],
+                        const double l[3], double *T0n, double *T0m, double *T0l, double *fs) {
+  const double sxx = s0[0], syy = s0[1], szz = s0[2], sxy = s0[3], sxz = s0[4], syz = s0[5];
+  const double Tx = n[0] * sxx + n[1] * sxy + n[2] * sxz;
+  const double Ty = n[0] * sxy + n[1] * syy + n[2] * syz;
+  const double Tz = n[0] * sxz + n[1] * syz + n[2] * szz;
+  *T0n = n[0] * Tx + n[1] * Ty + n[2] * Tz;
+  *T0m = m[0] * Tx + m[1] * Ty + m[2] * Tz;
+  *T0l = l[0] * Tx + l[1] * Ty + l[2] * Tz;
+  const double r = std::sqrt((x[1] - 7.5) * (x[1] - 7.5) + x[2] * x[2]);
+  double nuke = 0.0;
+  if (r <= 1.4) nuke = 11.60;
+  else if (r >= 1.4 && r <= 2.0) nuke = 5.8 * (1.0 + std::cos(3.141592653589793 * (r - 1.4) / 0.6));
+  *T0l = *T0l + nuke;
+  *fs = 0.677 + 1.0e10 * (1.0 - host_boxcar(x[1], 15.0) * host_boxcar(x[2], 18.0));
+}
+
+// fault_problem range check shared by the interface setups
+inline bool fault_problem_ok(const wql3d_domain_desc &desc) {
+  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_RATE_STATE) return false;
+  if (desc.fault_problem < WQL3D_FAULT_MAPS || desc.fault_problem > WQL3D_FAULT_TPV28) return false;
+  return (desc.coupling == WQL3D_IFACE_RATE_STATE) == rs_problem(desc.fault_problem);
+}
+
+// slip-weakening fd and Dc: the problem's own (TPV5 0.525 / 0.4, TPV28
+// 0.373 / 0.4; src/Interface_Condition.f90:1283-1299, 1459-1474) or the
+// description's
+inline void fault_weakening(const wql3d_domain_desc &desc, double *fd, double *Dc) {
+  *fd = desc.fd;
+  *Dc = desc.Dc;
+  if (desc.fault_problem == WQL3D_FAULT_TPV5) { *fd = 0.525; *Dc = 0.4; }
+  if (desc.fault_problem == WQL3D_FAULT_TPV28) { *fd = 0.373; *Dc = 0.4; }
+}
+
+// Per-point prestress / strength maps of one block's interface face (face 1:
+// its q-max face at q = xend = nq, face 0: its q-min face), and the
+// rate-and-state a and nucleation maps.  The TPV28 prestress is projected on
+// the block's own face basis, as each side's Interface_RHS call does.
+template <typename T>
+int fault_maps(const wql3d_domain_desc &desc, const Blk<T> &b, int face, const std::vector<double> &coords, int xend,
+               std::vector<double> &t0, std::vector<double> &f, std::vector<double> &ra, std::vector<double> &nuc,
+               cudaStream_t s) {
+  const int ny = b.ny, nz = b.nz;
+  const long long n = (long long)ny * nz;
+  t0.assign((size_t)(3 * n), 0.0);
+  f.assign((size_t)n, desc.fs);
+  ra.assign((size_t)n, 0.0);
+  nuc.assign((size_t)n, 0.0);
+  std::vector<T> B;
+  if (desc.fault_problem == WQL3D_FAULT_TPV28) {
+    B.resize((size_t)(9 * n));
+    if (cudaMemcpyAsync(B.data(), b.nrm[face], sizeof(T) * 9 * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return WQL3D_ECUDA;
+  }
+  const double *s0 = tpv28_stress(desc);
+  const long long nb = (long long)b.nx * ny * nz;
+  for (int z = 1; z <= nz; ++z)
+    for (int y = 1; y <= ny; ++y) {
+      const long long k = (long long)(y - 1) + (long long)ny * (z - 1);
+      const long long q = (long long)(xend - 1) + (long long)b.nx * ((y - 1) + (long long)ny * (z - 1));
+      const double x[3] = {coords[(size_t)q], coords[(size_t)(nb + q)], coords[(size_t)(2 * nb + q)]};
+      if (rs_problem(desc.fault_problem)) {
+        rs_point(x, &ra[(size_t)k], &nuc[(size_t)k]);
+      } else if (desc.fault_problem == WQL3D_FAULT_TPV5) {
+        tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
+      } else if (desc.fault_problem == WQL3D_FAULT_TPV28) {
+        double l[3], m[3], nv[3];
+        for (int c = 0; c < 3; ++c) {
+          l[c] = (double)B[(size_t)((0 + c) * n + k)];
+          m[c] = (double)B[(size_t)((3 + c) * n + k)];
+          nv[c] = (double)B[(size_t)((6 + c) * n + k)];
+        }
+        tpv28_point(s0, x, nv, m, l, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
+      } else {
+        if (desc.iface_tau0)
+          for (int c = 0; c < 3; ++c) t0[(size_t)(c * n + k)] = desc.iface_tau0[c * n + k];
+        if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
+      }
+    }
+  return WQL3D_OK;
+}
+
 // init_vel_state's state for TPV101 / TPV102 (src/Interface_Condition.f90:2722-2786):
 // W from the t = 0 traction on one block's interface face (basis of face
 // `face`, coordinates at q = xend): theta = L0/V0 exp((a log(2 sinh(T0_l/(a
@@ -156,17 +251,14 @@ int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, co
                 const std::vector<double> &coords0, const std::vector<double> &coords1, AllocT &mem,
                 cudaStream_t s) {
   if (b0.ny != b1.ny || b0.nz != b1.nz) return WQL3D_EINVAL;
-  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_RATE_STATE) return WQL3D_EINVAL;
-  if (desc.fault_problem < WQL3D_FAULT_MAPS || desc.fault_problem > WQL3D_FAULT_TPV102) return WQL3D_EINVAL;
-  if ((desc.coupling == WQL3D_IFACE_RATE_STATE) != rs_problem(desc.fault_problem)) return WQL3D_EINVAL;
+  if (!fault_problem_ok(desc)) return WQL3D_EINVAL;
   const int ny = b0.ny, nz = b0.nz;
   const long long n = (long long)ny * nz;
   I.ny = ny;
   I.nz = nz;
   I.coupling = desc.coupling;
   I.serial = desc.serial_shared ? 1 : 0;
-  I.fd = desc.fd;
-  I.Dc = desc.Dc;
+  fault_weakening(desc, &I.fd, &I.Dc);
   if (mem.get(&I.S, 4 * n) || mem.get(&I.DS, 4 * n) || mem.get(&I.W, n) || mem.get(&I.DW, n) ||
       mem.get(&I.Svel, 3 * n) || mem.get(&I.Uhat, 6 * n) || mem.get(&I.Vhat, 6 * n) || mem.get(&I.trup, n))
     return WQL3D_ENOMEM;
@@ -179,27 +271,13 @@ int setup_iface(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b0, co
   std::vector<double> tr((size_t)n, 1.0e9);
   if (cudaMemcpyAsync(I.trup, tr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return WQL3D_ECUDA;
-  const int nq[2] = {b0.nx, b1.nx};
+  const Blk<T> *bs[2] = {&b0, &b1};
   const std::vector<double> *cs[2] = {&coords0, &coords1};
   for (int side = 0; side < 2; ++side) {
-    std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs), ra((size_t)n, 0.0), nuc((size_t)n, 0.0);
-    const int xend = side == 0 ? nq[0] : 1;
-    const long long nb = (long long)nq[side] * ny * nz;
-    for (int z = 1; z <= nz; ++z)
-      for (int y = 1; y <= ny; ++y) {
-        long long k = (long long)(y - 1) + (long long)ny * (z - 1);
-        long long q = (long long)(xend - 1) + (long long)nq[side] * ((y - 1) + (long long)ny * (z - 1));
-        double x[3] = {(*cs[side])[(size_t)q], (*cs[side])[(size_t)(nb + q)], (*cs[side])[(size_t)(2 * nb + q)]};
-        if (rs_problem(desc.fault_problem)) {
-          rs_point(x, &ra[(size_t)k], &nuc[(size_t)k]);
-        } else if (desc.fault_problem == WQL3D_FAULT_TPV5) {
-          tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
-        } else {
-          if (desc.iface_tau0)
-            for (int c = 0; c < 3; ++c) t0[(size_t)(c * n + k)] = desc.iface_tau0[c * n + k];
-          if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
-        }
-      }
+    std::vector<double> t0, f, ra, nuc;
+    const int face = side == 0 ? 1 : 0;
+    const int xend = side == 0 ? b0.nx : 1;
+    if (int rc = fault_maps<T>(desc, *bs[side], face, *cs[side], xend, t0, f, ra, nuc, s)) return rc;
     if (mem.get(&I.t0[side], 3 * n) || mem.get(&I.fs[side], n) || mem.get(&I.ra[side], n) || mem.get(&I.nuc[side], n))
       return WQL3D_ENOMEM;
     if (cudaMemcpyAsync(I.t0[side], t0.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -222,17 +300,14 @@ template <typename T, typename AllocT>
 int setup_iface_remote(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> &b, const std::vector<double> &coords,
                        int side, AllocT &mem, cudaStream_t s) {
   if (side != 1 && side != 2) return WQL3D_EINVAL;
-  if (desc.coupling < WQL3D_IFACE_LOCKED || desc.coupling > WQL3D_IFACE_RATE_STATE) return WQL3D_EINVAL;
-  if (desc.fault_problem < WQL3D_FAULT_MAPS || desc.fault_problem > WQL3D_FAULT_TPV102) return WQL3D_EINVAL;
-  if ((desc.coupling == WQL3D_IFACE_RATE_STATE) != rs_problem(desc.fault_problem)) return WQL3D_EINVAL;
+  if (!fault_problem_ok(desc)) return WQL3D_EINVAL;
   const int ny = b.ny, nz = b.nz;
   const long long n = (long long)ny * nz;
   I.ny = ny;
   I.nz = nz;
   I.coupling = desc.coupling;
   I.serial = 0;
-  I.fd = desc.fd;
-  I.Dc = desc.Dc;
+  fault_weakening(desc, &I.fd, &I.Dc);
   I.remote = side;
   if (mem.get(&I.S, 4 * n) || mem.get(&I.DS, 4 * n) || mem.get(&I.W, n) || mem.get(&I.DW, n) ||
       mem.get(&I.Svel, 3 * n) || mem.get(&I.Uhat, 6 * n) || mem.get(&I.Vhat, 6 * n) || mem.get(&I.trup, n))
@@ -248,24 +323,9 @@ int setup_iface_remote(IfaceDev &I, const wql3d_domain_desc &desc, const Blk<T> 
   std::vector<double> tr((size_t)n, 1.0e9);
   if (cudaMemcpyAsync(I.trup, tr.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return WQL3D_ECUDA;
-  std::vector<double> t0((size_t)(3 * n), 0.0), f((size_t)n, desc.fs), ra((size_t)n, 0.0), nuc((size_t)n, 0.0);
+  std::vector<double> t0, f, ra, nuc;
   const int xend = side == 1 ? b.nx : 1;
-  const long long nb = (long long)b.nx * ny * nz;
-  for (int z = 1; z <= nz; ++z)
-    for (int y = 1; y <= ny; ++y) {
-      long long k = (long long)(y - 1) + (long long)ny * (z - 1);
-      long long q = (long long)(xend - 1) + (long long)b.nx * ((y - 1) + (long long)ny * (z - 1));
-      double x[3] = {coords[(size_t)q], coords[(size_t)(nb + q)], coords[(size_t)(2 * nb + q)]};
-      if (rs_problem(desc.fault_problem)) {
-        rs_point(x, &ra[(size_t)k], &nuc[(size_t)k]);
-      } else if (desc.fault_problem == WQL3D_FAULT_TPV5) {
-        tpv5_point(x, &t0[(size_t)k], &t0[(size_t)(n + k)], &t0[(size_t)(2 * n + k)], &f[(size_t)k]);
-      } else {
-        if (desc.iface_tau0)
-          for (int c = 0; c < 3; ++c) t0[(size_t)(c * n + k)] = desc.iface_tau0[c * n + k];
-        if (desc.iface_fs) f[(size_t)k] = desc.iface_fs[k];
-      }
-    }
+  if (int rc = fault_maps<T>(desc, b, side == 1 ? 1 : 0, coords, xend, t0, f, ra, nuc, s)) return rc;
   if (mem.get(&I.t0[side - 1], 3 * n) || mem.get(&I.fs[side - 1], n) || mem.get(&I.ra[side - 1], n) ||
       mem.get(&I.nuc[side - 1], n))
     return WQL3D_ENOMEM;

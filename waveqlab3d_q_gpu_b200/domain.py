@@ -105,6 +105,8 @@ class Domain:
         d.serial_shared = 1 if ip.serial_shared else 0
         d.fault_problem = FAULT_PROBLEMS[ip.problem]
         d.fs, d.fd, d.Dc = ip.fs, ip.fd, ip.Dc
+        if ip.stress is not None:
+            d.fault_stress[:] = [float(v) for v in ip.stress]
         if nb == 2 or remote_block is not None:
             nq, nr, ns = problem.blocks[0].nqrs
             if ip.tau0_n is not None or ip.tau0_m is not None or ip.tau0_l is not None:

@@ -35,9 +35,9 @@ STF_CODES = {
 RESPONSES = {"elastic": 0, "anelastic-Q4": 1, "anelastic-Q8": 2, "anelastic-fQ8": 3}
 
 COUPLINGS = {"locked": 0, "slip-weakening_friction": 1, "linear_friction": 2, "rate-and-state_friction": 3}
-# fault prestress / strength: per-point maps, or the reference's TPV5 formulas;
-# TPV101 / TPV102: prestress and rate-and-state parameters of the reference
-FAULT_PROBLEMS = {None: 0, "maps": 0, "TPV5": 1, "TPV101": 2, "TPV102": 3}
+# fault prestress / strength: per-point maps, or the reference's TPV5 / TPV28
+# formulas; TPV101 / TPV102: prestress and rate-and-state parameters of the reference
+FAULT_PROBLEMS = {None: 0, "maps": 0, "TPV5": 1, "TPV101": 2, "TPV102": 3, "TPV28": 4}
 
 # Kennedy-Carpenter (5,4) low-storage coefficients, src/time_step.f90:53-62
 RK_A = (
@@ -162,6 +162,10 @@ class InterfaceParams:
     # output (test_problems/truth/1) follows.
     serial_shared: bool = False
     problem: Optional[str] = None         # 'TPV5': prestress and strength of src/Interface_Condition.f90
+    # 'TPV28': background stress (sxx, syy, szz, sxy, sxz, syz) projected on
+    # each fault point's (n, m, l) basis; None: the tensor of
+    # src/initial_stress_condition.f90:78-84, (-60, 0, 60, 0, 29.38, 0)
+    stress: Optional[tuple] = None
 
 
 @dataclass
