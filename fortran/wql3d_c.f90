@@ -8,7 +8,8 @@ module wql3d_c
   implicit none
   integer(c_int), parameter :: WQL3D_ABI_VERSION = 4
   integer(c_int), parameter :: WQL3D_FP64 = 0, WQL3D_FP32_COMPENSATED = 1
-  integer(c_int), parameter :: WQL3D_FD_TRADITIONAL6 = 0, WQL3D_FD_UPWIND4 = 1
+  integer(c_int), parameter :: WQL3D_FD_TRADITIONAL6 = 0, WQL3D_FD_UPWIND4 = 1, WQL3D_FD_UPWIND6 = 2, &
+                                WQL3D_FD_UPWIND_DRP6 = 3
   integer(c_int), parameter :: WQL3D_MESH_CARTESIAN = 0, WQL3D_MESH_CURVILINEAR = 1
   integer(c_int), parameter :: WQL3D_IFACE_LOCKED = 0, WQL3D_IFACE_SLIP_WEAKENING = 1, WQL3D_IFACE_LINEAR = 2
   integer(c_int), parameter :: WQL3D_IFACE_RATE_STATE = 3

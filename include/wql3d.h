@@ -59,6 +59,10 @@ extern "C" {
 #define WQL3D_FD_TRADITIONAL6 0       /* traditional 6th-order SBP, src/JU_xJU_yJU_z6.f90:12-809, :16088-16640 */
 #define WQL3D_FD_UPWIND4 1            /* upwind 4th order: forward operator on velocities, backward on stresses,
                                          src/JU_xJU_yJU_z6.f90:1439-2033, :17865-18400 (SAT tau0 = 144/49) */
+#define WQL3D_FD_UPWIND6 2            /* upwind 6th order, src/JU_xJU_yJU_z6.f90:2665-3688, :18958-19510
+                                         (tau0 = 42300/13613) */
+#define WQL3D_FD_UPWIND_DRP6 3        /* upwind DRP 6th order, src/JU_xJU_yJU_z6.f90:10556-12058 and
+                                         JJU_x6_interior_upwind_drp (tau0 = 3.39644507697204) */
 
 /* arithmetic */
 #define WQL3D_FP64 0

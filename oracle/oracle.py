@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
         L.orc_adjoint_rhs.argtypes = [vp, C.c_int, dp, dp, dp]
         L.orc_adjoint_moment.argtypes = [vp, C.c_int, C.c_double, dp, dp]
         L.orc_tfi_grid.argtypes = [dp, C.c_int, C.c_int, C.c_int, dp]
+        L.orc_upwind_row.restype = C.c_int
+        L.orc_upwind_row.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, dp]
         _LIB = L
     return _LIB
 
@@ -424,3 +426,13 @@ def tfi_grid(faces: np.ndarray, nqrs) -> np.ndarray:
     out = np.zeros((3, ns, nr, nq))
     lib().orc_tfi_grid(_dptr(f), int(nq), int(nr), int(ns), _dptr(out))
     return out
+
+
+def upwind_row(fd: int, plus: bool, i: int, n: int):
+    """(indices, coefficients) of row i (1-based) of the upwind operator fd's
+    D+ (plus) or D- on n points."""
+    idx = np.zeros(16, dtype=np.int32)
+    c = np.zeros(16)
+    k = lib().orc_upwind_row(int(fd), 1 if plus else 0, int(i), int(n),
+                             idx.ctypes.data_as(C.POINTER(C.c_int)), _dptr(c))
+    return idx[:k].copy(), c[:k].copy()

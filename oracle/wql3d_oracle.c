@@ -83,15 +83,31 @@ static void sbp_stencil(int i, int n, int *cnt, int *idx, double *c) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* Upwind-4 SBP operator pair, src/JU_xJU_yJU_z6.f90:1439-2033 (near         */
-/* boundary) and :17865-18400 (interior).  Velocities take the forward       */
-/* operator D+, stresses the backward operator D-.  Left closure rows 1..4   */
-/* in the order the reference writes their terms; the right closure of each  */
-/* operator is the negated mirror of the other operator's left rows.  The    */
-/* near-boundary routine writes the interior rows with 15-digit literals,    */
-/* the interior routine with exact fractions.                                */
+/* Upwind SBP operator pairs: velocities take the forward operator D+,       */
+/* stresses the backward operator D-.  Per operator: the width of the        */
+/* closure (rows 1..w at each end; the strict interior starts at w + 1), the */
+/* interior stencils (first offsets and coefficients, as the near-boundary   */
+/* routine writes them and as the interior routine does), and the left       */
+/* closure rows of both operators in the order the reference writes their    */
+/* terms.  The right closure of each operator is the negated mirror of the   */
+/* other operator's left rows, terms in the same order.                      */
+/*   upwind-4:     src/JU_xJU_yJU_z6.f90:1439-2033, :17865-18400             */
+/*   upwind-6:     src/JU_xJU_yJU_z6.f90:2665-3688, :18958-19510             */
+/*   upwind-DRP-6: src/JU_xJU_yJU_z6.f90:10556-12058, and its interior       */
+/*                 routine JJU_x6_interior_upwind_drp                         */
 /* ------------------------------------------------------------------------ */
-static const sbp_row g_up4_plus[4] = {
+#define UP_MAXT 13
+typedef struct { int n; int idx[UP_MAXT]; double c[UP_MAXT]; } up_row;
+typedef struct {
+  int width;                        /* closure rows per end */
+  int taps;                         /* interior taps */
+  int of, ob;                       /* first interior offset of D+ / D- */
+  double nbf[10], nbb[10];          /* interior rows of the near-boundary routine */
+  double inf_[10], inb[10];         /* coefficients of the strict-interior routine */
+  const up_row *plus, *minus;       /* left closure rows 1..width */
+} upwind_op;
+
+static const up_row g_up4_plus[4] = {
     {4, {4, 3, 2, 1}, {0.030612244897959, -0.591836734693878, 2.091836734693878, -1.530612244897959}},
     {5, {5, 4, 3, 2, 1}, {0.065573770491803, -0.234972677595628, 0.811475409836066, -0.180327868852459,
                           -0.461748633879781}},
@@ -99,34 +115,158 @@ static const sbp_row g_up4_plus[4] = {
                              -0.475609756097561, 0.089430894308943}},
     {7, {7, 6, 5, 4, 3, 2, 1}, {0.080536912751678, -0.483221476510067, 1.449664429530201, -0.785234899328859,
                                 -0.218120805369128, -0.073825503355705, 0.030201342281879}}};
-static const sbp_row g_up4_minus[4] = {
+static const up_row g_up4_minus[4] = {
     {4, {4, 3, 2, 1}, {-0.091836734693878, -0.224489795918367, 1.724489795918367, -1.408163265306122}},
     {4, {4, 3, 2, 1}, {0.060109289617486, 0.319672131147541, 0.180327868852459, -0.560109289617486}},
     {4, {4, 3, 2, 1}, {0.264227642276423, 0.707317073170732, -1.207317073170732, 0.235772357723577}},
     {5, {5, 4, 3, 2, 1}, {0.241610738255034, 0.785234899328859, -1.305369127516778, 0.288590604026846,
                           -0.010067114093960}}};
 
-/* Row of D+ (plus = 1) or D- (plus = 0) at 1-based i of n points. */
-static void up4_stencil(int plus, int i, int n, int *cnt, int *idx, double *c) {
-  static const double cp[5] = {-0.250000000000000, -0.833333333333333, 1.500000000000000, -0.500000000000000,
-                               0.083333333333333};
-  static const double cm[5] = {-0.083333333333333, 0.500000000000000, -1.500000000000000, 0.833333333333333,
-                               0.250000000000000};
-  if (i >= 5 && i <= n - 4) {
-    *cnt = 5;
-    for (int k = 0; k < 5; ++k) {
-      idx[k] = plus ? i - 1 + k : i - 3 + k;
-      c[k] = plus ? cp[k] : cm[k];
+static const up_row g_up6_plus[6] = {
+    {6, {6, 5, 4, 3, 2, 1}, {0.054021710000147, 0.023993033880123, -0.302855902188632, -0.275607596716317,
+                             2.093702214477299, -1.593253459452621}},
+    {6, {6, 5, 4, 3, 2, 1}, {-0.039560344515975, 0.030739159126096, 0.105980141988699, 0.393228064437077,
+                             -0.029551468764759, -0.460835552271137}},
+    {7, {7, 6, 5, 4, 3, 2, 1}, {-0.026915887850467, 0.197069524204597, -0.589452745232692, 1.258766829227482,
+                                -0.306540940575249, -0.629259919521358, 0.096333139747688}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {-0.013345690454124, 0.106765523632994, -0.330443502642251, 0.946962507015985,
+                                   -0.318292975073623, -0.243684445410829, -0.240558007429252, 0.092596590361100}},
+    {9, {9, 8, 7, 6, 5, 4, 3, 2, 1}, {-0.018365004463716, 0.146920035709731, -0.550950133911491, 1.406282074938901,
+                                      -0.593528379527062, -0.450132219590077, 0.041897570295664, 0.033485250803205,
+                                      -0.015609194255155}},
+    {10, {10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {-0.016424481602299, 0.131395852818395, -0.492734448068983,
+                                           1.313958528183954, -0.572337434946968, -0.357460227911152,
+                                           -0.025427590054054, -0.005338567444210, 0.040531470682718,
+                                           -0.016163101657400}}};
+static const up_row g_up6_minus[6] = {
+    {6, {6, 5, 4, 3, 2, 1}, {0.052048915548040, 0.044953974933765, -0.366971721882124, -0.189297839436616,
+                             2.039450367044345, -1.580183696207410}},
+    {6, {6, 5, 4, 3, 2, 1}, {-0.029492540133095, -0.021790841692085, 0.215422101432619, 0.279404147185598,
+                             0.029551468764759, -0.473094335557797}},
+    {6, {6, 5, 4, 3, 2, 1}, {0.008748664712219, -0.061405392278187, 0.491468255323896, 0.306540940575249,
+                             -0.885608401570530, 0.140255933237354}},
+    {6, {6, 5, 4, 3, 2, 1}, {0.020661154127888, 0.327107204245208, 0.318292975073623, -0.624133691970994,
+                             -0.118346128899150, 0.076418487423426}},
+    {7, {7, 6, 5, 4, 3, 2, 1}, {-0.036730008927433, 0.399693508760138, 0.593528379527062, -1.303115093827634,
+                                0.402190050630647, -0.047235828122731, -0.008331008040049}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {-0.032848963204599, 0.394187558455186, 0.572337434946968, -1.257688453771463,
+                                   0.406675342006739, -0.120254802392339, 0.054367610816546, -0.016775726857039}}};
+static const up_row g_drp6_plus[8] = {
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.033005239880522, -0.025881634391799, 0.263392722344631, -0.030209714180198,
+        -0.506938949737935, -0.350517535783371, 2.412053651292632, -1.728893299663438}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.008828095360976, 0.029911851210588, -0.170162903794152, 0.094426023794218,
+        0.250037914252055, 0.250891381680726, -0.020053857114091, -0.443878505390320}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.086554962191340, 0.357259827206167, -0.022134128148434, -1.484851853641141,
+        2.378309161955782, -0.045718284610534, -1.531087089237169, 0.434777328666669}},
+    {9, {9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.002634349609551, 0.079463252429367, -0.299393382304440, 0.407288103594466,
+        0.281750824243924, -0.012373610391183, -0.330330927617320, -0.204468804842354,
+        0.080698894497091}},
+    {10, {10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.011812293127050, 0.027365145744332, -0.517048981121307, 1.165933921548919,
+        0.122648484113833, -0.373648890457135, -1.160735576719516, 1.025653483809176,
+        -0.176618285456005, -0.101737008335247}},
+    {11, {11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.003705846074975, 0.008585210073693, 0.061269988439591, -0.203098167192540,
+        0.696367795879953, -0.264391437780108, 0.124789282744944, -0.548404955515763,
+        0.002073955135157, 0.176979071835593, -0.050464897545544}},
+    {12, {12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.005172307293959, 0.011982511897672, 0.085515480593458, -0.535851035654166,
+        1.560836153489656, -0.905179927543220, -0.052231816759526, -0.486889270320233,
+        0.517428663501413, -0.137956948397386, -0.108190216650142, 0.055708713136433}},
+    {13, {13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.004715630209601, 0.010924543318908, 0.077965086132063, -0.488539289714622,
+        1.474420378868455, -0.892828448398233, -0.032767235755012, -0.248685062282352,
+        0.170930500243401, -0.110359853738840, 0.038849792028224, 0.017743142086478,
+        -0.012937922578870}}};
+static const up_row g_drp6_minus[8] = {
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.044374156234105, -0.174198378773702, 0.220245640409051, 0.139299657443443,
+        -0.495449593250587, -0.370787168310084, 2.304067463556378, -1.667551777308605}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.011723708576681, 0.065174528307485, -0.148801997699767, 0.046588172420165,
+        0.241839854684496, 0.251551333921227, 0.020053857114091, -0.464682040171017}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        -0.156241518792227, 0.505832529848511, -0.010613520806507, -1.646697927315869,
+        2.378062811419621, 0.045718284610534, -1.527070237729393, 0.411009578765331}},
+    {8, {8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.061651661535115, -0.263535772373310, 0.389840903051706, 0.258864496540571,
+        0.012373610391183, -0.330365147571788, -0.211400033956727, 0.082570282383251}},
+    {9, {9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.014765366408812, -0.428167834093026, 1.111936792339292, -0.397762766470929,
+        0.373648890457135, -1.263356736209345, 0.924846902011930, -0.357974171524791,
+        0.022063557080921}},
+    {10, {10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.004632307593719, -0.036811404344754, 0.195432746208080, 0.037422964670561,
+        0.264391437780108, -0.038478253000180, -0.572948637727217, 0.004325161232786,
+        0.202384868750895, -0.060351191163998}},
+    {11, {11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.006465384117449, -0.051378252453327, 0.137238553533049, 0.035940522255854,
+        0.905179927543220, -0.971931417829373, -0.510533260717342, 0.587831838812040,
+        -0.097436350250351, -0.049653902328415, 0.008276957317196}},
+    {12, {12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1}, {
+        0.005894537762001, -0.046841926748699, 0.125121388228069, 0.105630116695053,
+        0.892828448398233, -1.423025682605699, 0.258439188609325, 0.206413079068906,
+        -0.142243577826732, 0.021522078805545, -0.013360802114642, 0.009623151728641}}};
+
+/* D+ of the interior routines is -(D-) mirrored: nbb / inb are the reversed,
+   negated nbf / inf_ (kept written out as each routine writes them) */
+static const upwind_op g_upwind4 = {
+    4, 5, -1, -3,
+    {-0.250000000000000, -0.833333333333333, 1.500000000000000, -0.500000000000000, 0.083333333333333},
+    {-0.083333333333333, 0.500000000000000, -1.500000000000000, 0.833333333333333, 0.250000000000000},
+    {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0},
+    {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0},
+    g_up4_plus, g_up4_minus};
+static const upwind_op g_upwind6 = {
+    6, 7, -2, -4,
+    {1.0 / 30.0, -2.0 / 5.0, -7.0 / 12.0, 4.0 / 3.0, -1.0 / 2.0, 2.0 / 15.0, -1.0 / 60.0},
+    {1.0 / 60.0, -2.0 / 15.0, 1.0 / 2.0, -4.0 / 3.0, 7.0 / 12.0, 2.0 / 5.0, -1.0 / 30.0},
+    {1.0 / 30.0, -0.4, -7.0 / 12.0, 4.0 / 3.0, -0.5, 2.0 / 15.0, -1.0 / 60.0},
+    {1.0 / 60.0, -2.0 / 15.0, 0.5, -4.0 / 3.0, 7.0 / 12.0, 0.4, -1.0 / 30.0},
+    g_up6_plus, g_up6_minus};
+static const upwind_op g_drp6 = {
+    8, 10, -4, -5,
+    {-0.005952380952381, 0.047301587301587, -0.126349206349206, -0.106666666666667, -0.888888888888889,
+     1.488888888888889, -0.493333333333333, 0.078730158730159, 0.011031746031746, -0.004761904761905},
+    {0.004761904761905, -0.011031746031746, -0.078730158730159, 0.493333333333333, -1.488888888888889,
+     0.888888888888889, 0.106666666666667, 0.126349206349206, -0.047301587301587, 0.005952380952381},
+    {-1.0 / 168.0, 149.0 / 3150.0, -199.0 / 1575.0, -8.0 / 75.0, -8.0 / 9.0, 67.0 / 45.0, -37.0 / 75.0,
+     124.0 / 1575.0, 139.0 / 12600.0, -1.0 / 210.0},
+    {1.0 / 210.0, -139.0 / 12600.0, -124.0 / 1575.0, 37.0 / 75.0, -67.0 / 45.0, 8.0 / 9.0, 8.0 / 75.0,
+     199.0 / 1575.0, -149.0 / 3150.0, 1.0 / 168.0},
+    g_drp6_plus, g_drp6_minus};
+
+/* the block's upwind operator, NULL for traditional-6 */
+static const upwind_op *upwind_of(int fd) {
+  if (fd == ORC_FD_UPWIND4) return &g_upwind4;
+  if (fd == ORC_FD_UPWIND6) return &g_upwind6;
+  if (fd == ORC_FD_UPWIND_DRP6) return &g_drp6;
+  return NULL;
+}
+
+/* Row of D+ (plus = 1) or D- (plus = 0) at 1-based i of n points, with the
+   near-boundary routine's interior coefficients */
+static void up_stencil(const upwind_op *op, int plus, int i, int n, int *cnt, int *idx, double *c) {
+  const int w = op->width;
+  if (i > w && i <= n - w) {
+    *cnt = op->taps;
+    for (int k = 0; k < op->taps; ++k) {
+      idx[k] = i + (plus ? op->of : op->ob) + k;
+      c[k] = plus ? op->nbf[k] : op->nbb[k];
     }
     return;
   }
-  if (i >= n - 3) { /* negated mirror of the other operator's left row n+1-i */
-    const sbp_row *r = plus ? &g_up4_minus[n - i] : &g_up4_plus[n - i];
+  if (i > n - w) { /* negated mirror of the other operator's left row n+1-i */
+    const up_row *r = plus ? &op->minus[n - i] : &op->plus[n - i];
     *cnt = r->n;
     for (int k = 0; k < r->n; ++k) { idx[k] = n + 1 - r->idx[k]; c[k] = -r->c[k]; }
     return;
   }
-  const sbp_row *r = plus ? &g_up4_plus[i - 1] : &g_up4_minus[i - 1];
+  const up_row *r = plus ? &op->plus[i - 1] : &op->minus[i - 1];
   *cnt = r->n;
   for (int k = 0; k < r->n; ++k) { idx[k] = r->idx[k]; c[k] = r->c[k]; }
 }
@@ -514,19 +654,20 @@ static void jju6(const oblk *b, int x, int y, int z, double *const X[3], double 
 }
 
 /* ------------------------------------------------------------------------ */
-/* Near-boundary derivative JJU_x4_upwind, src/JU_xJU_yJU_z6.f90:1439-2033:  */
-/* velocities X(p) * D+ u, stresses D-((X J) F) with the reference's         */
-/* association ((c X) J) F of each term.                                     */
+/* Near-boundary upwind derivative (JJU_x4_upwind, JJU_x6_upwind,           */
+/* JJU_x6_upwind_drp of src/JU_xJU_yJU_z6.f90): velocities X(p) * D+ u,      */
+/* stresses D-((X J) F) with the reference's association ((c X) J) F of each */
+/* term.                                                                     */
 /* ------------------------------------------------------------------------ */
-static void jju_up4(const oblk *b, int x, int y, int z, double *const X[3], double Ju[9]) {
+static void jju_up(const oblk *b, const upwind_op *op, int x, int y, int z, double *const X[3], double Ju[9]) {
   double Jd[3][9];
-  int cnt, idx[8];
-  double c[8];
+  int cnt, idx[UP_MAXT];
+  double c[UP_MAXT];
   const long p0 = ID(b, x, y, z);
   const int pos[3] = {x, y, z}, nn[3] = {b->nx, b->ny, b->nz};
   for (int a = 0; a < 3; ++a) {
     for (int plus = 1; plus >= 0; --plus) {
-      up4_stencil(plus, pos[a], nn[a], &cnt, idx, c);
+      up_stencil(op, plus, pos[a], nn[a], &cnt, idx, c);
       for (int f = plus ? 0 : 3; f < (plus ? 3 : 9); ++f) {
         double s = 0.0;
         for (int k = 0; k < cnt; ++k) {
@@ -687,8 +828,10 @@ static void anelastic_point(oblk *b, long p, int x, int y, int z, double exx, do
 /* ------------------------------------------------------------------------ */
 static void interior_bounds(const oblk *b, int lo[3], int hi[3]) {
   /* src/RHS_Interior.f90:199-214, src/JU_xJU_yJU_z6.f90:16158-16173; the
-     upwind-4 width is 4 (src/JU_xJU_yJU_z6.f90:17915-17931) */
-  const int w = b->d.fd == ORC_FD_UPWIND4 ? 4 : 6;
+     upwind widths: 4 for upwind-4 (src/JU_xJU_yJU_z6.f90:17915-17931), 6 for
+     upwind-6, 8 for upwind-DRP-6 (src/RHS_Interior.f90:614-630, 1218-1234) */
+  const upwind_op *op = upwind_of(b->d.fd);
+  const int w = op ? op->width : 6;
   int ix = w, iy = w, iz = w, fx = w, fy = w, fz = w;
   const int *pm = b->d.pml;
   int np = b->d.npml;
@@ -706,16 +849,17 @@ static void interior_bounds(const oblk *b, int lo[3], int hi[3]) {
 static void rhs_near_boundaries(oblk *b) {
   int lo[3], hi[3];
   interior_bounds(b, lo, hi);
+  const upwind_op *op = upwind_of(b->d.fd);
 #pragma omp parallel for schedule(static)
   for (int z = 1; z <= b->nz; ++z)
     for (int y = 1; y <= b->ny; ++y)
       for (int x = 1; x <= b->nx; ++x) {
         if ((lo[2] <= z && z <= hi[2]) && (lo[1] <= y && y <= hi[1]) && (lo[0] <= x && x <= hi[0])) continue;
         double Ux[9], Uy[9], Uz[9], DU[9];
-        if (b->d.fd == ORC_FD_UPWIND4) { /* src/RHS_Interior.f90:443-470 */
-          jju_up4(b, x, y, z, b->mx, Ux);
-          jju_up4(b, x, y, z, b->my, Uy);
-          jju_up4(b, x, y, z, b->mz, Uz);
+        if (op) { /* src/RHS_Interior.f90:443-470, 614-660, 1218-1260 */
+          jju_up(b, op, x, y, z, b->mx, Ux);
+          jju_up(b, op, x, y, z, b->my, Uy);
+          jju_up(b, op, x, y, z, b->mz, Uz);
         } else {
           jju6(b, x, y, z, b->mx, Ux);
           jju6(b, x, y, z, b->my, Uy);
@@ -786,21 +930,22 @@ static void interior_rates(oblk *b, long p, int x, int y, int z, int curv, const
 }
 
 /* ------------------------------------------------------------------------ */
-/* Strict interior JJU_x4_interior_upwind, src/JU_xJU_yJU_z6.f90:17865-18400 */
-/* forward differences (-1/4, -5/6, 3/2, -1/2, 1/12 at offsets -1..3) of the */
-/* velocities, backward (-1/12, 1/2, -3/2, 5/6, 1/4 at -3..1) of the         */
-/* stresses; Cartesian: diagonal metric at the point, 1/rho; curvilinear:    */
-/* metric at the point for the velocities, (F X) J at the taps for stresses. */
+/* Strict interior of the upwind operators (JJU_x4_interior_upwind,         */
+/* src/JU_xJU_yJU_z6.f90:17865-18400; JJU_x6_interior_upwind, :18958-19510;  */
+/* JJU_x6_interior_upwind_drp): forward differences of the velocities at     */
+/* offsets of .. of + taps - 1, backward differences of the stresses at      */
+/* ob .. ob + taps - 1; Cartesian: diagonal metric at the point, 1/rho;      */
+/* curvilinear: metric at the point for the velocities, (F X) J at the taps  */
+/* for the stresses.                                                         */
 /* ------------------------------------------------------------------------ */
-static void rhs_interior_up4(oblk *b) {
+static void rhs_interior_up(oblk *b, const upwind_op *op) {
   int lo[3], hi[3];
   interior_bounds(b, lo, hi);
-  static const double cf[5] = {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0};
-  static const double cb[5] = {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0};
-  double cfx[5], cfy[5], cfz[5], cbx[5], cby[5], cbz[5];
-  for (int k = 0; k < 5; ++k) {
-    cfx[k] = cf[k] / b->hq; cfy[k] = cf[k] / b->hr; cfz[k] = cf[k] / b->hs;
-    cbx[k] = cb[k] / b->hq; cby[k] = cb[k] / b->hr; cbz[k] = cb[k] / b->hs;
+  const int T = op->taps;
+  double cfx[10], cfy[10], cfz[10], cbx[10], cby[10], cbz[10];
+  for (int k = 0; k < T; ++k) {
+    cfx[k] = op->inf_[k] / b->hq; cfy[k] = op->inf_[k] / b->hr; cfz[k] = op->inf_[k] / b->hs;
+    cbx[k] = op->inb[k] / b->hq; cby[k] = op->inb[k] / b->hr; cbz[k] = op->inb[k] / b->hs;
   }
   const long sx = 1, sy = b->NX, sz = (long)b->NX * b->NY;
   const int curv = b->d.mesh == 1;
@@ -810,10 +955,10 @@ static void rhs_interior_up4(oblk *b) {
       for (int x = lo[0]; x <= hi[0]; ++x) {
         const long p = ID(b, x, y, z);
         double DFx[9] = {0}, DFy[9] = {0}, DFz[9] = {0};
-        for (int s = -1; s <= 3; ++s) {
-          const int k = s + 1;
-          const long fx = p + s * sx, fy = p + s * sy, fz = p + s * sz;                  /* forward taps */
-          const long bx = p + (s - 2) * sx, by = p + (s - 2) * sy, bz = p + (s - 2) * sz;  /* backward taps */
+        for (int k = 0; k < T; ++k) {
+          const long s = op->of + k, t = op->ob + k;
+          const long fx = p + s * sx, fy = p + s * sy, fz = p + s * sz;  /* forward taps */
+          const long bx = p + t * sx, by = p + t * sy, bz = p + t * sz;  /* backward taps */
           if (curv) {
             for (int f = 0; f < 3; ++f) {
               const double *Ff = b->F[f];
@@ -848,8 +993,8 @@ static void rhs_interior_up4(oblk *b) {
 }
 
 static void rhs_interior(oblk *b) {
-  if (b->d.fd == ORC_FD_UPWIND4) {
-    rhs_interior_up4(b);
+  if (upwind_of(b->d.fd)) {
+    rhs_interior_up(b, upwind_of(b->d.fd));
     return;
   }
   int lo[3], hi[3];
@@ -1510,6 +1655,17 @@ void orc_final_state(void *dv, double *maxF, double *maxEta, double *maxB) {
   *maxEta = me;
 }
 
+/* Row of an upwind operator (ORC_FD_UPWIND*; plus = 1: D+, 0: D-) at 1-based
+   i of n points: up to 13 (1-based index, coefficient) pairs; returns the
+   count, 0 for a traditional-6 code */
+int orc_upwind_row(int fd, int plus, int i, int n, int *idx, double *c) {
+  const upwind_op *op = upwind_of(fd);
+  if (!op) return 0;
+  int cnt = 0;
+  up_stencil(op, plus, i, n, &cnt, idx, c);
+  return cnt;
+}
+
 /* Q4 / Q8 fixed coefficients */
 void orc_q4_coefficients(double fmin, double fmax, double *tau, double *weight) {
   double taumin = 1.0 / (2.0 * PI_WP * fmax), taumax = 1.0 / (2.0 * PI_WP * fmin);
@@ -2025,7 +2181,7 @@ int orc_get_fault(void *dv, int kind, double *out) {
 /* For the rates R-bar of one stage, orc_adjoint_rhs adds L^T R-bar to the  */
 /* field adjoint and (dL/dp F)^T R-bar to the material gradient, where L is */
 /* this file's set_rates + impose_boundary_condition for one elastic block  */
-/* (rhs_interior, rhs_near_boundaries with jju6 / jju_up4, face SATs; no    */
+/* (rhs_interior, rhs_near_boundaries with jju6 / jju_up, face SATs; no     */
 /* PML, memory variables, interface or sources) and F the block's current   */
 /* fields.  Written as the scatter transpose of those loops: every          */
 /* accumulation DF[f][p] += c * F[g][q] there becomes Fbar[g][q] +=         */
@@ -2059,17 +2215,18 @@ static void rates_adjoint(const double R[9], double a1, double lam, double mu, d
           R[8] * (Uz[1] + Uy[2]);
 }
 
-/* scatter transpose of one near-boundary derivative (jju6 or jju_up4) for
+/* scatter transpose of one near-boundary derivative (jju6 or jju_up) for
    metric row X: Ub = adjoint of Ju; adds to Fbar */
 static void jju_adjoint(const oblk *b, int x, int y, int z, double *const X[3], const double Ub[9], double **Fbar) {
   const long p0 = ID(b, x, y, z);
   const int pos[3] = {x, y, z}, nn[3] = {b->nx, b->ny, b->nz};
   const double ih[3] = {1.0 / b->hq, 1.0 / b->hr, 1.0 / b->hs};
-  int cnt, idx[8];
-  double c[8];
+  int cnt, idx[UP_MAXT];
+  double c[UP_MAXT];
+  const upwind_op *op = upwind_of(b->d.fd);
   for (int a = 0; a < 3; ++a)
     for (int grp = 0; grp < 2; ++grp) { /* 0: velocities, 1: stresses */
-      if (b->d.fd == ORC_FD_UPWIND4) up4_stencil(grp == 0, pos[a], nn[a], &cnt, idx, c);
+      if (op) up_stencil(op, grp == 0, pos[a], nn[a], &cnt, idx, c);
       else sbp_stencil(pos[a], nn[a], &cnt, idx, c);
       for (int k = 0; k < cnt; ++k) {
         const int q3[3] = {a == 0 ? idx[k] : x, a == 1 ? idx[k] : y, a == 2 ? idx[k] : z};
@@ -2153,8 +2310,9 @@ int orc_adjoint_rhs(void *dv, int bi, const double *Rin, double *Fbout, double *
         const int interior = lo[2] <= z && z <= hi[2] && lo[1] <= y && y <= hi[1] && lo[0] <= x && x <= hi[0];
         double Ux[9] = {0}, Uy[9] = {0}, Uz[9] = {0}, Ubx[9], Uby[9], Ubz[9];
         if (!interior) {
-          if (b->d.fd == ORC_FD_UPWIND4) {
-            jju_up4(b, x, y, z, b->mx, Ux); jju_up4(b, x, y, z, b->my, Uy); jju_up4(b, x, y, z, b->mz, Uz);
+          if (upwind_of(b->d.fd)) {
+            const upwind_op *op = upwind_of(b->d.fd);
+            jju_up(b, op, x, y, z, b->mx, Ux); jju_up(b, op, x, y, z, b->my, Uy); jju_up(b, op, x, y, z, b->mz, Uz);
           } else {
             jju6(b, x, y, z, b->mx, Ux); jju6(b, x, y, z, b->my, Uy); jju6(b, x, y, z, b->mz, Uz);
           }
@@ -2166,13 +2324,14 @@ int orc_adjoint_rhs(void *dv, int bi, const double *Rin, double *Fbout, double *
           continue;
         }
         /* strict interior: the forward's DFx / DFy / DFz as plain sums of tap terms */
-        double ws[2][8];  /* per tap: coefficient / h */
-        int offs[2][8], ntap[2];
-        if (b->d.fd == ORC_FD_UPWIND4) {
-          static const double cf[5] = {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0};
-          static const double cb[5] = {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0};
-          ntap[0] = ntap[1] = 5;
-          for (int k = 0; k < 5; ++k) { ws[0][k] = cf[k]; offs[0][k] = k - 1; ws[1][k] = cb[k]; offs[1][k] = k - 3; }
+        double ws[2][10];  /* per tap: coefficient / h */
+        int offs[2][10], ntap[2];
+        if (upwind_of(b->d.fd)) {
+          const upwind_op *op = upwind_of(b->d.fd);
+          ntap[0] = ntap[1] = op->taps;
+          for (int k = 0; k < op->taps; ++k) {
+            ws[0][k] = op->inf_[k]; offs[0][k] = op->of + k; ws[1][k] = op->inb[k]; offs[1][k] = op->ob + k;
+          }
         } else {
           static const double cc[6] = {-1.0 / 60.0, 0.15, -0.75, 0.75, -0.15, 1.0 / 60.0};
           static const int oo[6] = {-3, -2, -1, 1, 2, 3};

@@ -27,7 +27,7 @@ enum {
 };
 
 /* interface coupling laws, src/Interface_Condition.f90 */
-enum { ORC_FD_TRADITIONAL6 = 0, ORC_FD_UPWIND4 = 1 };
+enum { ORC_FD_TRADITIONAL6 = 0, ORC_FD_UPWIND4 = 1, ORC_FD_UPWIND6 = 2, ORC_FD_UPWIND_DRP6 = 3 };
 enum { ORC_IFACE_LOCKED = 0, ORC_IFACE_SLIP_WEAKENING = 1, ORC_IFACE_LINEAR = 2, ORC_IFACE_RATE_STATE = 3 };
 enum { ORC_FAULT_MAPS = 0, ORC_FAULT_TPV5 = 1, ORC_FAULT_TPV101 = 2, ORC_FAULT_TPV102 = 3, ORC_FAULT_TPV28 = 4 };
 /* fault outputs, src/domain.f90:782-845 and src/fault_output.f90:73-122; layout [comp][ns][nr] */
@@ -59,9 +59,11 @@ typedef struct {
      exact boundary data in the face SATs when mms != 0 */
   int mms;
   double mms_nt, mms_nx, mms_ny, mms_nz;
-  /* derivative operator (fd_type / order of &problem_list): ORC_FD_TRADITIONAL6
-     or ORC_FD_UPWIND4 (velocities by the forward, stresses by the backward
-     upwind SBP operator, src/JU_xJU_yJU_z6.f90:1439-2033, :17865-18400) */
+  /* derivative operator (fd_type / order of &problem_list): ORC_FD_TRADITIONAL6,
+     or an upwind pair, velocities by the forward and stresses by the backward
+     operator: ORC_FD_UPWIND4 (src/JU_xJU_yJU_z6.f90:1439-2033, :17865-18400),
+     ORC_FD_UPWIND6 (:2665-3688, :18958-19510), ORC_FD_UPWIND_DRP6 (:10556-12058
+     and JJU_x6_interior_upwind_drp) */
   int fd;
 } orc_desc;
 
@@ -112,6 +114,9 @@ void orc_final_state(void *d, double *maxF, double *maxEta, double *maxB);
 void orc_mms_exact(void *d, int b, double t, double *out);
 
 /* coefficient builders, src/anelastic_q4_model.f90:97-111, src/anelastic_q8_model.f90:100-116 */
+/* row of an upwind operator (ORC_FD_UPWIND*; plus: D+ or D-) at 1-based i of
+   n points, up to 13 taps; returns the tap count (0 for traditional-6) */
+int orc_upwind_row(int fd, int plus, int i, int n, int *idx, double *c);
 void orc_q4_coefficients(double fmin, double fmax, double *tau, double *weight);
 void orc_q8_coefficients(double fmin, double fmax, double *tau, double *weight);
 /* modulus correction, src/material.f90:156-298 (Q4), :330-485 (Q8) */

@@ -23,6 +23,11 @@ LOCKED_PIN_BLOCK_MAX = (2.0699e03, 1.6389e03)
 # 5 digits (ACCELERATOR_RUNTIME.md:176-177, NVHPC_shutdown_regression_fix.md:35-41)
 UPWIND4_PIN = {"anelastic-Q8": (1.8221e02, 1.4544e01), "anelastic-Q4": (1.8221e02, 1.1049e01)}
 
+# inputfile/test_elastic_upwind_o6.in / test_elastic_upwind_drp_o6.in: the
+# 41^3 case of ``pin_case`` with fd_type 'upwind' / 'upwind_drp', order 6;
+# published final max|field|, 5 digits (PHASE2_SCRATCH_MEMORY_AUDIT.md:190-191)
+ORDER6_PIN = {("upwind", 6): 1.6563e02, ("upwind_drp", 6): 1.6567e02}
+
 
 def pin_case(**kw):
     b = Block(nqrs=(41, 41, 41), aqrs=(-2.0, -2.0, -2.0), bqrs=(2.0, 2.0, 2.0), rho_s_p=(2.7, 3.464, 6.0),

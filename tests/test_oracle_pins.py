@@ -2,8 +2,8 @@
 import numpy as np
 import pytest
 
-from cases import (LOCKED_PIN_BLOCK_MAX, PIN_MAX_FIELD, UPWIND4_PIN, locked_pin_case, pin_case, round_sig,
-                   upwind4_pin_case)
+from cases import (LOCKED_PIN_BLOCK_MAX, ORDER6_PIN, PIN_MAX_FIELD, UPWIND4_PIN, locked_pin_case, pin_case,
+                   round_sig, upwind4_pin_case)
 
 
 def test_elastic_traditional_o6_final_state(oracle_lib):
@@ -49,6 +49,56 @@ def test_anelastic_upwind4_dynamic_final_state(oracle_lib, response):
         d.run(p.nt())
         mf, me, _ = d.final_state()
         assert (round_sig(mf), round_sig(me)) == UPWIND4_PIN[response], (mf, me)
+
+
+@pytest.mark.parametrize("fd_type,order", sorted(ORDER6_PIN))
+def test_elastic_order6_upwind_final_state(oracle_lib, fd_type, order):
+    """inputfile/test_elastic_upwind_o6.in -> 1.6563E+02 and
+    test_elastic_upwind_drp_o6.in -> 1.6567E+02 (5 printed digits): the
+    upwind-6 and upwind-DRP-6 interiors (6 steps do not reach the closures;
+    test_upwind_pairs_are_sbp pins those)."""
+    p = pin_case(fd_type=fd_type, order=order)
+    assert p.nt() == 6
+    d = oracle_lib.OracleDomain(p)
+    d.run(p.nt())
+    mf, me, _ = d.final_state()
+    assert round_sig(mf) == ORDER6_PIN[(fd_type, order)], mf
+    assert me == 0.0
+
+
+@pytest.mark.parametrize("fd,degree", [(1, 2), (2, 3), (3, 3)])
+def test_upwind_pairs_are_sbp(oracle_lib, fd, degree):
+    """The transcribed closure tables of upwind-4 / upwind-6 / upwind-DRP-6:
+    a diagonal norm H > 0 with H D+ + (H D-)^T = diag(-1, 0, .., 0, 1) exists
+    (the upwind summation-by-parts property) and H (D+ - D-) is symmetric
+    negative semidefinite (the upwind dissipation); every closure row
+    differentiates polynomials of the closure degree exactly.  A wrong digit,
+    sign or mirror in a table breaks all three."""
+    n = 41
+    Dp, Dm = np.zeros((n, n)), np.zeros((n, n))
+    for i in range(1, n + 1):
+        for plus, D in ((True, Dp), (False, Dm)):
+            idx, c = oracle_lib.upwind_row(fd, plus, i, n)
+            for j, v in zip(idx, c):
+                D[i - 1, j - 1] += v
+            x = idx.astype(np.float64) - i
+            for k in range(degree + 1):
+                exact = 1.0 if k == 1 else 0.0
+                assert abs(np.sum(c * x ** k) - exact) < 1e-12 * max(1.0, np.abs(x).max() ** k), (i, plus, k)
+    B = np.zeros((n, n))
+    B[0, 0], B[-1, -1] = -1.0, 1.0
+    A = np.zeros((n * n, n))
+    for i in range(n):
+        for j in range(n):
+            A[i * n + j, i] += Dp[i, j]
+            A[i * n + j, j] += Dm[j, i]
+    h = np.linalg.lstsq(A, B.ravel(), rcond=None)[0]
+    H = np.diag(h)
+    assert h.min() > 0.2
+    assert np.abs(H @ Dp + (H @ Dm).T - B).max() < 1e-13
+    S = H @ (Dp - Dm)
+    assert np.abs(S - S.T).max() < 1e-13
+    assert np.linalg.eigvalsh(0.5 * (S + S.T)).max() < 1e-13
 
 
 def test_dt_and_nt_follow_block_time_step():

@@ -27,12 +27,16 @@ static void launch_curv_fused(Blk<T> &b, const StageCtx &c, const StageArgs &a) 
   }
   const unsigned gr = (unsigned)((npts + 127) / 128);
   const int mb = tuning().fused_minb;
+  StageArgs la = a;
+  la.pf = tuning().mvpf;
   if (sizeof(T) == 8) {
-    if (mb == 2) launch_fused_mb<T, 2>(b, c, a, gr);
-    else launch_fused_mb<T, 3>(b, c, a, gr);
+    if (mb == 2) launch_fused_mb<T, 2>(b, c, la, gr);
+    else if (mb == 4) launch_fused_mb<T, 4>(b, c, la, gr);
+    else launch_fused_mb<T, 3>(b, c, la, gr);
   } else {
-    if (mb == 6) launch_fused_mb<T, 6>(b, c, a, gr);
-    else launch_fused_mb<T, 4>(b, c, a, gr);
+    if (mb == 6) launch_fused_mb<T, 6>(b, c, la, gr);
+    else if (mb == 5) launch_fused_mb<T, 5>(b, c, la, gr);
+    else launch_fused_mb<T, 4>(b, c, la, gr);
   }
   ++*c.launches;
 }

@@ -11,6 +11,7 @@
 #include "wql3d_stage.cuh"
 #include "wql3d_adjoint.cuh"
 #include "wql3d_batch.cuh"
+#include "wql3d_upwind.h"
 
 #include <algorithm>
 #include <cmath>
@@ -53,24 +54,6 @@ const int kSbpCnt[6] = {6, 5, 5, 6, 7, 8};
 const int kSbpIdx[6][8] = {{6, 5, 4, 3, 2, 1, 0, 0}, {6, 5, 4, 3, 1, 0, 0, 0}, {6, 5, 4, 2, 1, 0, 0, 0},
                            {7, 6, 5, 3, 2, 1, 0, 0}, {8, 7, 6, 4, 3, 2, 1, 0}, {9, 8, 7, 5, 4, 3, 2, 1}};
 double kSbpC[2][6][8];
-
-// upwind-4 left closure rows 1..4 of D+ ([0], velocities) and D- ([1],
-// stresses), absolute 1-based tap indices and coefficients in the order of
-// src/JU_xJU_yJU_z6.f90:1488-1570
-const int kUp4Cnt[2][4] = {{4, 5, 6, 7}, {4, 4, 4, 5}};
-const int kUp4Idx[2][4][8] = {{{4, 3, 2, 1}, {5, 4, 3, 2, 1}, {6, 5, 4, 3, 2, 1}, {7, 6, 5, 4, 3, 2, 1}},
-                              {{4, 3, 2, 1}, {4, 3, 2, 1}, {4, 3, 2, 1}, {5, 4, 3, 2, 1}}};
-const double kUp4C[2][4][8] = {
-    {{0.030612244897959, -0.591836734693878, 2.091836734693878, -1.530612244897959},
-     {0.065573770491803, -0.234972677595628, 0.811475409836066, -0.180327868852459, -0.461748633879781},
-     {0.097560975609756, -0.585365853658537, 1.581300813008130, -0.707317073170732, -0.475609756097561,
-      0.089430894308943},
-     {0.080536912751678, -0.483221476510067, 1.449664429530201, -0.785234899328859, -0.218120805369128,
-      -0.073825503355705, 0.030201342281879}},
-    {{-0.091836734693878, -0.224489795918367, 1.724489795918367, -1.408163265306122},
-     {0.060109289617486, 0.319672131147541, 0.180327868852459, -0.560109289617486},
-     {0.264227642276423, 0.707317073170732, -1.207317073170732, 0.235772357723577},
-     {0.241610738255034, 0.785234899328859, -1.305369127516778, 0.288590604026846, -0.010067114093960}}};
 
 void sbp_tables() {
   static bool done = false;
@@ -489,49 +472,66 @@ int setup_block(wql3d_domain *d, int bi) {
     b.rowo = dro;
   }
   b.fd = bd.fd_operator;
-  {
-    // upwind-4 closure rows (src/JU_xJU_yJU_z6.f90:1488-1660): D+ left rows
-    // 1..4 and D- left rows 1..4 in the reference's summation order; the right
-    // rows of each operator are the negated mirror of the other's left rows
-    std::vector<double> rc(16 * 8, 0.0);
-    std::vector<int> ro(16 * 8, 0);
-    for (int r = 0; r < 4; ++r)
-      for (int k = 0; k < kUp4Cnt[0][r]; ++k) {
-        rc[r * 8 + k] = kUp4C[0][r][k];                       // D+ left
-        ro[r * 8 + k] = kUp4Idx[0][r][k] - (r + 1);
-        rc[(12 + r) * 8 + k] = -kUp4C[0][r][k];               // D- right (mirror of D+ left)
-        ro[(12 + r) * 8 + k] = (r + 1) - kUp4Idx[0][r][k];
+  if (const UpwindTable *up = upwind_table(b.fd)) {
+    // device rows of the upwind pair: D+ left, D+ right, D- left, D- right
+    // (w rows each), then the near-boundary routine's D+ and D- interior
+    // rows; offsets relative to the point, kUpSlots slots per row.  The right
+    // rows of each operator are the negated mirror of the other's left rows.
+    const int w = up->width, nrow = 4 * w + 2;
+    std::vector<double> rc((size_t)nrow * kUpSlots, 0.0);
+    std::vector<int> ro((size_t)nrow * kUpSlots, 0), rn((size_t)nrow, 0);
+    for (int r = 0; r < w; ++r) {
+      rn[r] = rn[3 * w + r] = up->pcnt[r];
+      for (int k = 0; k < up->pcnt[r]; ++k) {
+        rc[(size_t)r * kUpSlots + k] = up->pc[r][k];                    // D+ left
+        ro[(size_t)r * kUpSlots + k] = up->pidx[r][k] - (r + 1);
+        rc[(size_t)(3 * w + r) * kUpSlots + k] = -up->pc[r][k];         // D- right (mirror of D+ left)
+        ro[(size_t)(3 * w + r) * kUpSlots + k] = (r + 1) - up->pidx[r][k];
       }
-    for (int r = 0; r < 4; ++r)
-      for (int k = 0; k < kUp4Cnt[1][r]; ++k) {
-        rc[(8 + r) * 8 + k] = kUp4C[1][r][k];                 // D- left
-        ro[(8 + r) * 8 + k] = kUp4Idx[1][r][k] - (r + 1);
-        rc[(4 + r) * 8 + k] = -kUp4C[1][r][k];                // D+ right (mirror of D- left)
-        ro[(4 + r) * 8 + k] = (r + 1) - kUp4Idx[1][r][k];
+      rn[2 * w + r] = rn[w + r] = up->mcnt[r];
+      for (int k = 0; k < up->mcnt[r]; ++k) {
+        rc[(size_t)(2 * w + r) * kUpSlots + k] = up->mc[r][k];          // D- left
+        ro[(size_t)(2 * w + r) * kUpSlots + k] = up->midx[r][k] - (r + 1);
+        rc[(size_t)(w + r) * kUpSlots + k] = -up->mc[r][k];             // D+ right (mirror of D- left)
+        ro[(size_t)(w + r) * kUpSlots + k] = (r + 1) - up->midx[r][k];
       }
+    }
+    rn[4 * w] = rn[4 * w + 1] = up->taps;
+    for (int k = 0; k < up->taps; ++k) {
+      rc[(size_t)(4 * w) * kUpSlots + k] = up->nbf[k];
+      ro[(size_t)(4 * w) * kUpSlots + k] = up->of + k;
+      rc[(size_t)(4 * w + 1) * kUpSlots + k] = up->nbb[k];
+      ro[(size_t)(4 * w + 1) * kUpSlots + k] = up->ob + k;
+    }
     double *drc;
-    int *dro;
+    int *dro, *drn;
     CK(d->mem.get(&drc, rc.size()));
     CK(d->mem.get(&dro, ro.size()));
+    CK(d->mem.get(&drn, rn.size()));
     CK(cudaMemcpyAsync(drc, rc.data(), sizeof(double) * rc.size(), cudaMemcpyHostToDevice, d->stream));
     CK(cudaMemcpyAsync(dro, ro.data(), sizeof(int) * ro.size(), cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(drn, rn.data(), sizeof(int) * rn.size(), cudaMemcpyHostToDevice, d->stream));
     CK(cudaStreamSynchronize(d->stream));
     b.urowc = drc;
     b.urowo = dro;
-    // interior forward / backward coefficients over h (src/JU_xJU_yJU_z6.f90:17885-17889, 17910-17911)
-    const double cf[5] = {-1.0 / 4.0, -5.0 / 6.0, 3.0 / 2.0, -1.0 / 2.0, 1.0 / 12.0};
-    const double cb[5] = {-1.0 / 12.0, 1.0 / 2.0, -3.0 / 2.0, 5.0 / 6.0, 1.0 / 4.0};
+    b.urown = drn;
+    b.uw = w;
+    b.utaps = up->taps;
+    b.uof = up->of;
+    b.uob = up->ob;
+    // strict-interior coefficients over h
     const double hh[3] = {1.0 / (double)(h.nq - 1), 1.0 / (double)(h.nr - 1), 1.0 / (double)(nsg - 1)};
     for (int a = 0; a < 3; ++a)
-      for (int k = 0; k < 5; ++k) {
-        b.ufw[a][k] = (T)(cf[k] / hh[a]);
-        b.ubw[a][k] = (T)(cb[k] / hh[a]);
+      for (int k = 0; k < up->taps; ++k) {
+        b.ufw[a][k] = (T)(up->inf[k] / hh[a]);
+        b.ubw[a][k] = (T)(up->inb[k] / hh[a]);
       }
   }
   // strict interior bounds, src/JU_xJU_yJU_z6.f90:16158-16173 (traditional-6,
-  // width 6) and :17915-17931 (upwind-4, width 4)
+  // width 6), :17915-17931 (upwind-4, width 4), src/RHS_Interior.f90:614-630
+  // (upwind-6, 6) and :1218-1234 (upwind-DRP-6, 8)
   int np = bd.npml;
-  const int w = b.fd == WQL3D_FD_UPWIND4 ? 4 : 6;
+  const int w = upwind_table(b.fd) ? upwind_table(b.fd)->width : 6;
   int ix = bd.pml[0] ? std::max(np, w) : w, fx = bd.pml[1] ? std::max(np, w) : w;
   int iy = bd.pml[2] ? std::max(np, w) : w, fy = bd.pml[3] ? std::max(np, w) : w;
   int iz = bd.pml[4] ? std::max(np, w) : w, fz = bd.pml[5] ? std::max(np, w) : w;
@@ -1073,7 +1073,7 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
     return cleanup(fail(WQL3D_ENOMEM, "reduction scratch"));
   for (int i = 0; i < desc->nblocks; ++i) {
     const int fd = desc->block[i].fd_operator;
-    if (fd != WQL3D_FD_TRADITIONAL6 && fd != WQL3D_FD_UPWIND4)
+    if (fd < WQL3D_FD_TRADITIONAL6 || fd > WQL3D_FD_UPWIND_DRP6)
       return cleanup(fail(WQL3D_EINVAL, "unknown fd_operator"));
     if (fd != WQL3D_FD_TRADITIONAL6 && desc->slab_ns_global > 0)
       return cleanup(fail(WQL3D_EINVAL, "upwind blocks are not split into s-slabs"));

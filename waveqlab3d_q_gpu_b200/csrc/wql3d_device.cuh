@@ -92,13 +92,17 @@ struct Blk {
   int sep;              // Cartesian block whose metric is diagonal to roundoff (separable shell)
   const double *rowc;   // closure rows 0..11 (left 1..6, right n..n-5): 8 signed coefficients each
   const int *rowo;      // matching tap offsets relative to the point
-  // derivative operator: 0 traditional-6, 1 upwind-4 (forward D+ on the
-  // velocities, backward D- on the stresses); upwind closure rows 0..15:
-  // D+ left 1..4, D+ right n..n-3, D- left 1..4, D- right n..n-3
+  // derivative operator (WQL3D_FD_*): traditional-6, or an upwind pair
+  // (forward D+ on the velocities, backward D- on the stresses) of closure
+  // width uw.  Upwind rows, 16 slots each: D+ left 1..uw, D+ right n..n-uw+1,
+  // D- left, D- right, then the near-boundary routine's D+ and D- interior
+  // rows; urown holds each row's tap count, urowo the offsets from the point.
   int fd;
+  int uw, utaps, uof, uob;   // width, interior taps, first interior offset of D+ / D-
   const double *urowc;
   const int *urowo;
-  T ufw[3][5], ubw[3][5];  // upwind-4 interior forward / backward coefficients over h per axis
+  const int *urown;
+  T ufw[3][10], ubw[3][10];  // strict-interior forward / backward coefficients over h per axis
   // open faces of an s-slab of a larger block (ghost planes hold the
   // neighbour's data): the central row applies up to the face on that axis
   int open_lo[3], open_hi[3];
@@ -144,6 +148,7 @@ struct StageArgs {
   int stage;            // 1..5
   double A, Bdt, dt;
   const DevTime *time;
+  int pf = 0;           // k_curv_fused: 1 = L2 prefetch of the memory variables on entry
 };
 
 template <typename T>
@@ -707,39 +712,24 @@ __device__ void jju6_all(const Blk<T> &b, const T *F, int x, int y, int z, long 
   }
 }
 
-// Row of the upwind-4 operator D+ (plus) or D- at 1-based i of n points:
-// interior rows with the near-boundary routine's 15-digit literals
-// (src/JU_xJU_yJU_z6.f90:1488-1505), closures from the block's tables.
+// Device row of the block's upwind operator D+ (plus) or D- at 1-based i of
+// n points: closures from the left / right rows (the right rows win where
+// both apply, n < 2w, as the reference assigns them last), the
+// near-boundary routine's interior row elsewhere (the layout of Blk::urowc).
 template <typename T>
-__device__ __forceinline__ void up4_row(const Blk<T> &b, bool plus, int i, int n, Row &r) {
-  if (i >= 5 && i <= n - 4) {
-    r.cnt = 5;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) r.off[k] = plus ? k - 1 : k - 3;
-    if (plus) {
-      r.c[0] = -0.250000000000000; r.c[1] = -0.833333333333333; r.c[2] = 1.500000000000000;
-      r.c[3] = -0.500000000000000; r.c[4] = 0.083333333333333;
-    } else {
-      r.c[0] = -0.083333333333333; r.c[1] = 0.500000000000000; r.c[2] = -1.500000000000000;
-      r.c[3] = 0.833333333333333; r.c[4] = 0.250000000000000;
-    }
-    return;
-  }
-  const int row = (plus ? 0 : 8) + (i <= 4 ? i - 1 : 4 + (n - i));
-  r.cnt = 8;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    r.off[k] = __ldg(b.urowo + row * 8 + k);
-    r.c[k] = __ldg(b.urowc + row * 8 + k);
-  }
+__device__ __forceinline__ int up_row(const Blk<T> &b, bool plus, int i, int n) {
+  const int w = b.uw;
+  if (i > n - w) return (plus ? w : 3 * w) + (n - i);
+  if (i <= w) return (plus ? 0 : 2 * w) + (i - 1);
+  return 4 * w + (plus ? 0 : 1);
 }
 
-// Near-boundary upwind-4 derivatives of all nine fields for the three metric
-// rows, JJU_x4_upwind (src/JU_xJU_yJU_z6.f90:1439-2033): velocities
-// X_r,a(p) * D+_a(u), stresses D-_a(X_r,a J s) with each term associated as
-// ((c X) J) s.
+// Near-boundary upwind derivatives of all nine fields for the three metric
+// rows (JJU_x4_upwind, JJU_x6_upwind, JJU_x6_upwind_drp of
+// src/JU_xJU_yJU_z6.f90): velocities X_r,a(p) * D+_a(u), stresses
+// D-_a(X_r,a J s) with each term associated as ((c X) J) s.
 template <typename T>
-__device__ void jju_up4_all(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T U[3][9]) {
+__device__ void jju_up_all(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T U[3][9]) {
   const int pos[3] = {x, y, z};
   const int nn[3] = {b.nx, b.ny, b.nz};
   const long long st[3] = {1, b.sy, b.sz};
@@ -751,14 +741,12 @@ __device__ void jju_up4_all(const Blk<T> &b, const T *F, int x, int y, int z, lo
     for (int f = 0; f < 9; ++f) U[r][f] = 0;
 #pragma unroll 1
   for (int a = 0; a < 3; ++a) {
-    Row rp, rm;
-    up4_row(b, true, pos[a], nn[a], rp);
-    up4_row(b, false, pos[a], nn[a], rm);
+    const int rp = up_row(b, true, pos[a], nn[a]), rm = up_row(b, false, pos[a], nn[a]);
     T sv[3] = {0, 0, 0};
-    for (int k = 0; k < rp.cnt; ++k) {
-      const T c = (T)rp.c[k];
-      if (c == (T)0) continue;
-      const long long q = p + (long long)rp.off[k] * st[a];
+    const int np = __ldg(b.urown + rp);
+    for (int k = 0; k < np; ++k) {
+      const T c = (T)__ldg(b.urowc + rp * 16 + k);
+      const long long q = p + (long long)__ldg(b.urowo + rp * 16 + k) * st[a];
 #pragma unroll
       for (int f = 0; f < 3; ++f) sv[f] = sv[f] + c * ld(F + f * V + q);
     }
@@ -767,10 +755,10 @@ __device__ void jju_up4_all(const Blk<T> &b, const T *F, int x, int y, int z, lo
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int f = 0; f < 6; ++f) acc[r][f] = 0;
-    for (int k = 0; k < rm.cnt; ++k) {
-      const T c = (T)rm.c[k];
-      if (c == (T)0) continue;
-      const long long q = p + (long long)rm.off[k] * st[a];
+    const int nm = __ldg(b.urown + rm);
+    for (int k = 0; k < nm; ++k) {
+      const T c = (T)__ldg(b.urowc + rm * 16 + k);
+      const long long q = p + (long long)__ldg(b.urowo + rm * 16 + k) * st[a];
       const T Jq = ld(b.J + q);
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
@@ -790,21 +778,22 @@ __device__ void jju_up4_all(const Blk<T> &b, const T *F, int x, int y, int z, lo
   }
 }
 
-// Strict-interior upwind-4 derivative terms, JJU_x4_interior_upwind
-// (src/JU_xJU_yJU_z6.f90:17865-18400): forward differences of the
-// velocities at offsets -1..3, backward of the stresses at -3..1; Cartesian
-// with the diagonal metric at the point, curvilinear with the metric at the
-// point for the velocities and (s X) J at the taps for the stresses.
+// Strict-interior upwind derivative terms (JJU_x4_interior_upwind,
+// src/JU_xJU_yJU_z6.f90:17865-18400; JJU_x6_interior_upwind, :18958-19510;
+// JJU_x6_interior_upwind_drp): forward differences of the velocities at
+// offsets uof .., backward of the stresses at uob ..; Cartesian with the
+// diagonal metric at the point, curvilinear with the metric at the point for
+// the velocities and (s X) J at the taps for the stresses.
 template <typename T, int MESH>
-__device__ __forceinline__ void up4_interior(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T DFx[9],
+__device__ __forceinline__ void up_interior(const Blk<T> &b, const T *F, int x, int y, int z, long long p, T DFx[9],
                                              T DFy[9], T DFz[9]) {
   const long long V = b.vol;
   const long long st[3] = {1, b.sy, b.sz};
   if (MESH == MESH_CART) {
     const T mx = ld(b.mq + x), my = ld(b.mr + y), mz = ld(b.ms + z);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const int s = k - 1;
+#pragma unroll 1
+    for (int k = 0; k < b.utaps; ++k) {
+      const long long s = b.uof + k, t = b.uob + k;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const T *Fc = F + c * V;
@@ -815,9 +804,9 @@ __device__ __forceinline__ void up4_interior(const Blk<T> &b, const T *F, int x,
 #pragma unroll
       for (int c = 3; c < 9; ++c) {
         const T *Fc = F + c * V;
-        DFx[c] = DFx[c] + mx * b.ubw[0][k] * ld(Fc + p + (s - 2) * st[0]);
-        DFy[c] = DFy[c] + my * b.ubw[1][k] * ld(Fc + p + (s - 2) * st[1]);
-        DFz[c] = DFz[c] + mz * b.ubw[2][k] * ld(Fc + p + (s - 2) * st[2]);
+        DFx[c] = DFx[c] + mx * b.ubw[0][k] * ld(Fc + p + t * st[0]);
+        DFy[c] = DFy[c] + my * b.ubw[1][k] * ld(Fc + p + t * st[1]);
+        DFz[c] = DFz[c] + mz * b.ubw[2][k] * ld(Fc + p + t * st[2]);
       }
     }
   } else {
@@ -825,8 +814,8 @@ __device__ __forceinline__ void up4_interior(const Blk<T> &b, const T *F, int x,
 #pragma unroll
     for (int k = 0; k < 9; ++k) mp[k] = ld(b.met + k * V + p);
 #pragma unroll 1
-    for (int k = 0; k < 5; ++k) {
-      const int s = k - 1;
+    for (int k = 0; k < b.utaps; ++k) {
+      const long long s = b.uof + k, t = b.uob + k;
       const long long q0 = p + s * st[0], q1 = p + s * st[1], q2 = p + s * st[2];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -836,7 +825,7 @@ __device__ __forceinline__ void up4_interior(const Blk<T> &b, const T *F, int x,
         DFy[c] = DFy[c] + mp[3] * b.ufw[0][k] * f0 + mp[4] * b.ufw[1][k] * f1 + mp[5] * b.ufw[2][k] * f2;
         DFz[c] = DFz[c] + mp[6] * b.ufw[0][k] * f0 + mp[7] * b.ufw[1][k] * f1 + mp[8] * b.ufw[2][k] * f2;
       }
-      const long long r0 = p + (s - 2) * st[0], r1 = p + (s - 2) * st[1], r2 = p + (s - 2) * st[2];
+      const long long r0 = p + t * st[0], r1 = p + t * st[1], r2 = p + t * st[2];
       const T J0 = ld(b.J + r0), J1 = ld(b.J + r1), J2 = ld(b.J + r2);
       T m0[3], m1[3], m2[3];  // metric row r, q- / r- / s-entry at the backward taps
 #pragma unroll
@@ -938,8 +927,8 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
     T DFx[9], DFy[9], DFz[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) { DFx[c] = 0; DFy[c] = 0; DFz[c] = 0; }
-    if (b.fd == 1) {
-      up4_interior<T, MESH>(b, F, x, y, z, p, DFx, DFy, DFz);
+    if (b.fd != 0) {
+      up_interior<T, MESH>(b, F, x, y, z, p, DFx, DFy, DFz);
     } else if (MESH == MESH_CART) {
       const T mx = ld(b.mq + x), my = ld(b.mr + y), mz = ld(b.ms + z);
 #pragma unroll
@@ -1046,7 +1035,7 @@ __device__ void point_update(const Blk<T> &b, const StageArgs &a, int x, int y, 
       rhoJ_inv = (T)1 / rho;
     } else {
       T U[3][9];
-      if (b.fd == 1) jju_up4_all<T>(b, F, x, y, z, p, U);
+      if (b.fd != 0) jju_up_all<T>(b, F, x, y, z, p, U);
       else jju6_all<T>(b, F, x, y, z, p, U);
 #pragma unroll
       for (int f = 0; f < 9; ++f) { Ux[f] = U[0][f]; Uy[f] = U[1][f]; Uz[f] = U[2][f]; }
@@ -1839,6 +1828,16 @@ __global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a)
   if (integrate && b.FC) {
 #pragma unroll
     for (int c = 0; c < 9; ++c) prefetch_l2(b.FC + c * V + p);
+  }
+  if (RESP != RESP_EL && a.pf) {
+    // the memory-variable stream is read after the derivative gathers: ask
+    // for it now so that its DRAM latency overlaps them
+    constexpr int NM = RESP == RESP_Q4 ? 4 : 8;
+#pragma unroll 8
+    for (int c = 0; c < 6 * NM; ++c) {
+      prefetch_l2(b.eta + (long long)c * V + p);
+      prefetch_l2(b.deta + (long long)c * V + p);
+    }
   }
   AxisSlab sx = {false, false}, sy = {false, false}, sz = {false, false};
   if (b.npml > 0) {

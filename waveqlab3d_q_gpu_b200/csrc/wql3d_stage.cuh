@@ -37,7 +37,8 @@ struct Tuning {
   int generic = 0;    // 1: every point through the generic per-point kernel
   int lean = 1;       // curvilinear update: k_curv_point (0: generic point update k_curv_update)
   int curv_fused = 1; // curvilinear stage in one pass, k_curv_fused (0: derivative / memory-variable / point passes)
-  int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default) or 2 in FP64, 4 (default) or 6 in FP32
+  int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default), 2 or 4 in FP64; 4 (default), 5 or 6 in FP32
+  int mvpf = 0;       // k_curv_fused: L2 prefetch of the memory variables on entry
 };
 
 inline Tuning tuning() {
@@ -45,6 +46,7 @@ inline Tuning tuning() {
     Tuning r;
     if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = atoi(e) > 0 ? atoi(e) : 1;
     if (const char *e = getenv("WQL3D_FUSED_MINB")) r.fused_minb = atoi(e);
+    if (const char *e = getenv("WQL3D_MV_PREFETCH")) r.mvpf = atoi(e);
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
       if (strcmp(e, "curv_generic_update") == 0) r.lean = 0;

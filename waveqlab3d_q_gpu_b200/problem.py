@@ -39,6 +39,11 @@ COUPLINGS = {"locked": 0, "slip-weakening_friction": 1, "linear_friction": 2, "r
 # formulas; TPV101 / TPV102: prestress and rate-and-state parameters of the reference
 FAULT_PROBLEMS = {None: 0, "maps": 0, "TPV5": 1, "TPV101": 2, "TPV102": 3, "TPV28": 4}
 
+# derivative operators (fd_type, order) -> WQL3D_FD_* and their SAT penalties
+# (src/RHS_Interior.f90:36-128, src/block.f90:242-300)
+FD_OPERATORS = {("traditional", 6): 0, ("upwind", 4): 1, ("upwind", 6): 2, ("upwind_drp", 6): 3}
+SAT_PENALTY = {1: 144.0 / 49.0, 2: 42300.0 / 13613.0, 3: 3.39644507697204}
+
 # Kennedy-Carpenter (5,4) low-storage coefficients, src/time_step.f90:53-62
 RK_A = (
     0.0,
@@ -201,24 +206,26 @@ class Problem:
     interface: InterfaceParams = field(default_factory=InterfaceParams)
     tau0: float = TAU0_TRADITIONAL6
     mms: Optional[MMSParams] = None
-    # derivative operator of &problem_list: fd_type 'traditional' (order 6)
-    # or 'upwind' (order 4: forward operator on the velocities, backward on
-    # the stresses, src/JU_xJU_yJU_z6.f90:1439-2033)
+    # derivative operator of &problem_list: fd_type 'traditional' (order 6),
+    # 'upwind' (order 4 or 6) or 'upwind_drp' (order 6); the upwind pairs take
+    # the forward operator on the velocities, the backward on the stresses
+    # (src/JU_xJU_yJU_z6.f90:1439-3688, 10556-12058)
     fd_type: str = "traditional"
     order: int = 6
 
     def fd_operator(self) -> int:
-        """Operator code of the C descriptors: 0 traditional-6, 1 upwind-4."""
-        if self.fd_type == "traditional" and self.order == 6:
-            return 0
-        if self.fd_type == "upwind" and self.order == 4:
-            return 1
-        raise ValueError("unsupported operator fd_type=%r order=%r" % (self.fd_type, self.order))
+        """Operator code of the C descriptors: 0 traditional-6, 1 upwind-4,
+        2 upwind-6, 3 upwind-DRP-6."""
+        code = FD_OPERATORS.get((self.fd_type, self.order))
+        if code is None:
+            raise ValueError("unsupported operator fd_type=%r order=%r" % (self.fd_type, self.order))
+        return code
 
     def sat_penalty(self) -> float:
-        """SAT penalty tau0 of the operator, src/block.f90:242-258: 1/0.315949074074074
-        for traditional-6, 144/49 for upwind-4."""
-        return 144.0 / 49.0 if self.fd_operator() == 1 else self.tau0
+        """SAT penalty tau0 of the operator, src/block.f90:242-300:
+        1/0.315949074074074 for traditional-6, 144/49 for upwind-4,
+        42300/13613 for upwind-6, 3.39644507697204 for upwind-DRP-6."""
+        return SAT_PENALTY.get(self.fd_operator(), self.tau0)
 
     def dt(self) -> float:
         """Global time step, src/domain.f90:150-171 and src/block.f90:495-510.
