@@ -92,6 +92,10 @@ module wql3d_c
      integer(c_int) function wql3d_get_fault_output(d, kind, out) bind(C)
        import; type(c_ptr), value :: d; integer(c_int), value :: kind; real(c_double), intent(out) :: out(*)
      end function
+     integer(c_int) function wql3d_get_plane(d, block, axis, index, c0, ncomp, out) bind(C)
+       import; type(c_ptr), value :: d; integer(c_int), value :: block, axis, index, c0, ncomp
+       real(c_double), intent(out) :: out(*)
+     end function
      integer(c_int) function wql3d_final_state(d, max_field, max_memory, block_max) bind(C)
        import; type(c_ptr), value :: d; real(c_double), intent(out) :: max_field, max_memory, block_max(*)
      end function

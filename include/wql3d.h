@@ -203,6 +203,14 @@ int wql3d_get_interface(wql3d_domain *d, double *out);                    /* per
    (src/domain.f90:782-845).  The face traces (Uface, Vface) are the fields
    at block 1's q-max and block 2's q-min faces (wql3d_get_fields). */
 int wql3d_get_fault_output(wql3d_domain *d, int kind, double *out);
+/* components c0 .. c0 + ncomp - 1 (0-based; 0..2 velocities, 3..8 stresses)
+   of block `block`'s fields on the plane of 1-based index `index` normal to
+   axis (1: q, 2: r, 3: s), gathered on the device: out holds n1 x n2 x ncomp
+   doubles, the first in-plane index (q, or r for axis 1) fastest.  Replaces
+   extract_local_plane (src/plane_output.f90:594-653, the plane writer's
+   velocities) and the F(:, location, :, 1:9) sections of write_slice
+   (src/slice_output.f90:79-94); the file formats are the host's. */
+int wql3d_get_plane(wql3d_domain *d, int block, int axis, int index, int c0, int ncomp, double *out);
 
 /* time integration: one RK stage (time_step.f90:109-147 loop body),
    one time step (time_step_RK) and a graph-captured run of many steps.

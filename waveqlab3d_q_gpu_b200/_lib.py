@@ -66,6 +66,7 @@ SIGNATURES = {
     "wql3d_get_metrics": [C.c_void_p, C.c_int, dp],
     "wql3d_get_interface": [C.c_void_p, dp],
     "wql3d_get_fault_output": [C.c_void_p, C.c_int, dp],
+    "wql3d_get_plane": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp],
     "wql3d_set_time": [C.c_void_p, C.c_double],
     "wql3d_get_time": [C.c_void_p, dp],
     "wql3d_stage": [C.c_void_p, C.c_int, C.c_double],

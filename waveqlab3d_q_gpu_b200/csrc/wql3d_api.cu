@@ -173,6 +173,9 @@ struct wql3d_domain {
   bool adj_on = false;
   AdjBlk adj;
   double *adj_res = nullptr;   // receiver residuals of one sample (device)
+  // plane extraction (wql3d_get_plane): largest plane x 9 components
+  double *plane = nullptr;
+  long long plane_cap = 0;
 };
 
 namespace {
@@ -324,6 +327,26 @@ __global__ void k_fill_component(Blk<T> b, T *F, int c, T v) {
   int x, y, z;
   if (!flat_point(b, x, y, z)) return;
   F[(long long)c * b.vol + pidx(b, x, y, z)] = v;
+}
+
+// Components c0 .. c0 + nc - 1 of the fields on the plane of 1-based index
+// `index` normal to axis dir (0: q, 1: r, 2: s) into a dense buffer: the
+// first in-plane index (q, or r for dir 0) fastest, then the second, then
+// the component (the extract_local_plane / write_slice layouts of
+// src/plane_output.f90:594-653 and src/slice_output.f90:79-94).
+template <typename T>
+__global__ void k_plane_gather(Blk<T> b, const T *F, int dir, int index, int c0, int nc, double *out) {
+  const int n1 = dir == 0 ? b.ny : b.nx, n2 = dir == 2 ? b.ny : b.nz;
+  const long long total = (long long)n1 * n2 * nc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int i1 = (int)(i % n1), i2 = (int)((i / n1) % n2), c = (int)(i / ((long long)n1 * n2));
+    int x, y, z;
+    if (dir == 0) { x = index; y = i1 + 1; z = i2 + 1; }
+    else if (dir == 1) { x = i1 + 1; y = index; z = i2 + 1; }
+    else { x = i1 + 1; y = i2 + 1; z = index; }
+    out[i] = (double)F[(long long)(c0 + c) * b.vol + pidx(b, x, y, z)];
+  }
 }
 
 template <typename T>
@@ -1072,6 +1095,12 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
   if (d->mem.get(&d->red, 592) != cudaSuccess || d->mem.get(&d->flag, 1) != cudaSuccess)
     return cleanup(fail(WQL3D_ENOMEM, "reduction scratch"));
   for (int i = 0; i < desc->nblocks; ++i) {
+    const long long nq = desc->block[i].nq, nr = desc->block[i].nr, ns = desc->block[i].ns;
+    d->plane_cap = std::max(d->plane_cap, 9 * std::max(nq * nr, std::max(nq * ns, nr * ns)));
+  }
+  if (d->mem.get(&d->plane, (size_t)d->plane_cap, false) != cudaSuccess)
+    return cleanup(fail(WQL3D_ENOMEM, "plane buffer"));
+  for (int i = 0; i < desc->nblocks; ++i) {
     const int fd = desc->block[i].fd_operator;
     if (fd < WQL3D_FD_TRADITIONAL6 || fd > WQL3D_FD_UPWIND_DRP6)
       return cleanup(fail(WQL3D_EINVAL, "unknown fd_operator"));
@@ -1791,6 +1820,29 @@ int wql3d_field_volume(wql3d_domain *d, int bi, int64_t *elements) {
   DOM_CHECK(d, bi);
   if (!elements) return fail(WQL3D_EINVAL, "null argument");
   *elements = (int64_t)9 * (d->fp32 ? d->bf[bi].vol : d->bd[bi].vol);
+  return WQL3D_OK;
+}
+
+int wql3d_get_plane(wql3d_domain *d, int bi, int axis, int index, int c0, int ncomp, double *out) {
+  DOM_CHECK(d, bi);
+  const HostBlock &h = d->hb[bi];
+  const int n[3] = {h.nq, h.nr, h.ns};
+  if (!out || axis < 1 || axis > 3 || index < 1 || index > n[axis - 1] || c0 < 0 || ncomp < 1 || c0 + ncomp > 9)
+    return fail(WQL3D_EINVAL, "plane");
+  const int dir = axis - 1;
+  const long long total = (long long)(dir == 0 ? h.nr : h.nq) * (dir == 2 ? h.nr : h.ns) * ncomp;
+  if (total > d->plane_cap) return fail(WQL3D_EINVAL, "plane");
+  const unsigned g = (unsigned)std::min<long long>((total + 255) / 256, 4096);
+  if (d->fp32)
+    k_plane_gather<float><<<g, 256, 0, d->stream>>>(d->bf[bi], d->cur ? d->bf[bi].F1 : d->bf[bi].F0, dir, index, c0,
+                                                    ncomp, d->plane);
+  else
+    k_plane_gather<double><<<g, 256, 0, d->stream>>>(d->bd[bi], d->cur ? d->bd[bi].F1 : d->bd[bi].F0, dir, index, c0,
+                                                     ncomp, d->plane);
+  ++d->launches;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d->plane, sizeof(double) * total, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
   return WQL3D_OK;
 }
 

@@ -165,6 +165,22 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous global -> shared copies (sm_80+ cp.async, still the lightest
+// path for element-granular halo gathers on sm_100a).  src_size 0 zero-fills.
+// ---------------------------------------------------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  int sz = valid ? BYTES : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gsrc), "n"(BYTES), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// wait until at most K of this thread's committed groups are still in flight
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
 // central (interior) SBP row at 1-based i of n points on axis a: 7 <= i <= n-6,
 // or up to an open face of a slab
 template <typename T>
@@ -1449,22 +1465,67 @@ __device__ __forceinline__ void slab_strain(const Blk<T> &b, int x, int y, int z
 // that of :3361-3477 (fQ8) as s_l (2 mu e) + (p_l (lambda + 2 mu) tr -
 // s_l 2 mu tr), so only per-point scalars and the per-mechanism constants
 // are live: the same products in another association (rounding level).
+// Rates and update of the N memory variables of stress component c at one
+// point: ev / dv hold eta and deta on entry, the values to store on return;
+// the sum of the old eta is subtracted from the stress rate s[3 + c].
+template <typename T, int RESP, int N>
+__device__ __forceinline__ void mv_component(const Blk<T> &b, const StageArgs &a, int c, int active, T fn, T ft, T fs,
+                                             T l2m, T two_mu, const T e[6], T tr, T s[9], bool do_rhs, T ev[N],
+                                             T dv[N]) {
+  const T A = (T)a.A, Bdt = (T)a.Bdt;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (a.flags & F_SCALE) dv[i] = A * dv[i];
+  if (do_rhs) {
+    T sum = ev[0];
+#pragma unroll
+    for (int i = 1; i < N; ++i) sum = sum + ev[i];
+    s[3 + c] = s[3 + c] - sum;
+    const T ge = (c < 3 ? fn : fs) * e[c];
+    const T gt = ft * tr, l2t = l2m * tr, m2t = two_mu * tr;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if (RESP == RESP_FQ8) {
+        if (b.coarse && (i + 1) != active) continue;
+        const T ss = b.ss[i], ps = b.ps[i];
+        if (c < 3) dv[i] = dv[i] + ((ss * ge + (ps * l2t - ss * m2t)) - ev[i]) * b.itau[i];
+        else dv[i] = dv[i] + (ss * ge - ev[i]) * b.itau[i];
+      } else {
+        const T w = b.w[i];
+        if (c < 3) dv[i] = dv[i] + ((w * ge + w * gt) - ev[i]) * b.itau[i];
+        else dv[i] = dv[i] + (w * ge - ev[i]) * b.itau[i];
+      }
+    }
+  }
+  if (a.flags & F_UPDATE) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) ev[i] = ev[i] + Bdt * dv[i];
+  }
+}
+
+// per-point factors of the memory-variable rates
+template <typename T, int RESP>
+__device__ __forceinline__ void mv_factors(const Blk<T> &b, long long p, T lam, T mu, T &fn, T &ft, T &fs, T &l2m,
+                                           T &two_mu) {
+  T qs = 0, qp = 0;
+  if (RESP != RESP_FQ8) { qs = ld(b.qs + p); qp = ld(b.qp + p); }
+  two_mu = (T)2 * mu;
+  l2m = lam + (T)2 * mu;
+  fn = RESP == RESP_FQ8 ? two_mu : two_mu * qs;               // normal strain factor
+  ft = RESP == RESP_FQ8 ? (T)0 : (l2m * qp - two_mu * qs);    // trace factor (Q4/Q8)
+  fs = RESP == RESP_FQ8 ? mu : mu * qs;                        // shear strain factor
+}
+
 template <typename T, int RESP>
 __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p, T lam,
                                                T mu, const T e[6], T tr, T s[9], bool do_rhs) {
   constexpr int N = RESP == RESP_Q4 ? 4 : 8;
   const long long V = b.vol;
-  T qs = 0, qp = 0;
-  if (RESP != RESP_FQ8) { qs = ld(b.qs + p); qp = ld(b.qp + p); }
   const int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
   T *__restrict__ ep = b.eta + p;
   T *__restrict__ dp = b.deta + p;
-  const T A = (T)a.A, Bdt = (T)a.Bdt;
-  const T two_mu = (T)2 * mu, l2m = lam + (T)2 * mu;
-  // per-point factors of the rates
-  const T fn = RESP == RESP_FQ8 ? two_mu : two_mu * qs;               // normal strain factor
-  const T ft = RESP == RESP_FQ8 ? (T)0 : (l2m * qp - two_mu * qs);    // trace factor (Q4/Q8)
-  const T fs = RESP == RESP_FQ8 ? mu : mu * qs;                        // shear strain factor
+  T fn, ft, fs, l2m, two_mu;
+  mv_factors<T, RESP>(b, p, lam, mu, fn, ft, fs, l2m, two_mu);
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
     T ev[N], dv[N];
@@ -1473,35 +1534,70 @@ __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs 
       ev[i] = ep[(long long)(c * N + i) * V];
       dv[i] = dp[(long long)(c * N + i) * V];
     }
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-      if (a.flags & F_SCALE) dv[i] = A * dv[i];
-    if (do_rhs) {
-      T sum = ev[0];
-#pragma unroll
-      for (int i = 1; i < N; ++i) sum = sum + ev[i];
-      s[3 + c] = s[3 + c] - sum;
-      const T ge = (c < 3 ? fn : fs) * e[c];
-      const T gt = ft * tr, l2t = l2m * tr, m2t = two_mu * tr;
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        if (RESP == RESP_FQ8) {
-          if (b.coarse && (i + 1) != active) continue;
-          const T ss = b.ss[i], ps = b.ps[i];
-          if (c < 3) dv[i] = dv[i] + ((ss * ge + (ps * l2t - ss * m2t)) - ev[i]) * b.itau[i];
-          else dv[i] = dv[i] + (ss * ge - ev[i]) * b.itau[i];
-        } else {
-          const T w = b.w[i];
-          if (c < 3) dv[i] = dv[i] + ((w * ge + w * gt) - ev[i]) * b.itau[i];
-          else dv[i] = dv[i] + (w * ge - ev[i]) * b.itau[i];
-        }
-      }
-    }
+    mv_component<T, RESP, N>(b, a, c, active, fn, ft, fs, l2m, two_mu, e, tr, s, do_rhs, ev, dv);
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       dp[(long long)(c * N + i) * V] = dv[i];
-      if (a.flags & F_UPDATE) ep[(long long)(c * N + i) * V] = ev[i] + Bdt * dv[i];
+      if (a.flags & F_UPDATE) ep[(long long)(c * N + i) * V] = ev[i];
     }
+  }
+}
+
+// Memory-variable ring of k_curv_fused: per thread RING component slots of
+// N eta + N deta values in shared memory ([slot][2N][128], thread fastest),
+// filled by cp.async so that the memory-variable stream is in flight while
+// the derivative gathers run.
+template <typename T, int N>
+__device__ __forceinline__ void mv_ring_fill(const Blk<T> &b, long long p, int c, T *ring, int slot) {
+  const long long V = b.vol;
+  T *dst = ring + (long long)slot * 2 * N * 128 + threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    cp_async<sizeof(T)>(dst + i * 128, b.eta + (long long)(c * N + i) * V + p, true);
+    cp_async<sizeof(T)>(dst + (N + i) * 128, b.deta + (long long)(c * N + i) * V + p, true);
+  }
+  cp_async_commit();
+}
+
+__device__ __forceinline__ void cp_async_wait_upto(int k) {
+  // k is a compile-time constant after unrolling; map it to the immediate
+  if (k <= 0) cp_async_wait<0>();
+  else if (k == 1) cp_async_wait<1>();
+  else if (k == 2) cp_async_wait<2>();
+  else if (k == 3) cp_async_wait<3>();
+  else if (k == 4) cp_async_wait<4>();
+  else cp_async_wait<5>();
+}
+
+template <typename T, int RESP, int RING>
+__device__ __forceinline__ void anelastic_ring(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p,
+                                               T lam, T mu, const T e[6], T tr, T s[9], bool do_rhs, T *ring) {
+  constexpr int N = RESP == RESP_Q4 ? 4 : 8;
+  const long long V = b.vol;
+  const int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
+  T *__restrict__ ep = b.eta + p;
+  T *__restrict__ dp = b.deta + p;
+  T fn, ft, fs, l2m, two_mu;
+  mv_factors<T, RESP>(b, p, lam, mu, fn, ft, fs, l2m, two_mu);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    // components c .. min(c + RING - 1, 5) are committed; wait for c
+    cp_async_wait_upto((c + RING - 1 < 5 ? c + RING - 1 : 5) - c);
+    const T *src = ring + (long long)(c % RING) * 2 * N * 128 + threadIdx.x;
+    T ev[N], dv[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      ev[i] = src[i * 128];
+      dv[i] = src[(N + i) * 128];
+    }
+    mv_component<T, RESP, N>(b, a, c, active, fn, ft, fs, l2m, two_mu, e, tr, s, do_rhs, ev, dv);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      dp[(long long)(c * N + i) * V] = dv[i];
+      if (a.flags & F_UPDATE) ep[(long long)(c * N + i) * V] = ev[i];
+    }
+    // the slot's values are consumed (the stores above depend on them)
+    if (c + RING < 6) mv_ring_fill<T, N>(b, p, c + RING, ring, c % RING);
   }
 }
 
@@ -1813,11 +1909,21 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
 // rates take the PML correction from Q before this stage's Q update, as in
 // the split passes.
 // ---------------------------------------------------------------------------
-template <typename T, int RESP, int MINB>
+// RING > 0: the memory variables arrive through the shared-memory ring of
+// anelastic_ring (dynamic shared memory RING * 2 * N * 128 values), its
+// first RING components requested on entry.
+template <typename T, int RESP, int MINB, int RING = 0>
 __global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   int x, y, z;
   if (!flat_point(b, x, y, z)) return;
   const long long p = pidx(b, x, y, z);
+  constexpr int NMV = RESP == RESP_Q4 ? 4 : 8;
+  T *ring = reinterpret_cast<T *>(smraw);
+  if (RING > 0 && RESP != RESP_EL) {
+#pragma unroll
+    for (int c = 0; c < RING; ++c) mv_ring_fill<T, NMV>(b, p, c, ring, c);
+  }
   const long long V = b.vol;
   const T *__restrict__ F = a.cur ? b.F1 : b.F0;
   T *__restrict__ Fn = a.cur ? b.F0 : b.F1;
@@ -1913,7 +2019,8 @@ __global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a)
   if (RESP != RESP_EL) {
     const T lm = rhs ? lam : b.M[p], mm = rhs ? mu : b.M[V + p];
     T s6[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    anelastic_lean<T, RESP>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs);
+    if (RING > 0) anelastic_ring<T, RESP, RING>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs, ring);
+    else anelastic_lean<T, RESP>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs);
     if (rhs) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) df[3 + c] = df[3 + c] + s6[3 + c];
@@ -2017,18 +2124,6 @@ __global__ void __launch_bounds__(128, 3) k_shell(Blk<T> b, StageArgs a, int cou
   point_update<T, MESH, RESP, SEP>(b, a, x, y, z);
 }
 
-// ---------------------------------------------------------------------------
-// Asynchronous global -> shared copies (sm_80+ cp.async, still the lightest
-// path for element-granular halo gathers on sm_100a).  src_size 0 zero-fills.
-// ---------------------------------------------------------------------------
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc, bool valid) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  int sz = valid ? BYTES : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gsrc), "n"(BYTES), "r"(sz) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Strict interior of a Cartesian block, src/JU_xJU_yJU_z6.f90:16426-16636,

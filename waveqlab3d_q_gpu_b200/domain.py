@@ -357,6 +357,19 @@ class Domain:
         _lib.check(_lib.load().wql3d_get_fault_output(self.handle, kind, _ptr(a)), "wql3d_get_fault_output")
         return a
 
+    def plane(self, b: int, axis: int, index: int, c0: int = 0, ncomp: int = 9) -> np.ndarray:
+        """Field components c0 .. c0 + ncomp - 1 of block b on the plane of
+        1-based ``index`` normal to ``axis`` (1: q, 2: r, 3: s), gathered on
+        the device (wql3d_get_plane): (ncomp, n2, n1), n1 the first in-plane
+        axis (q, or r for axis 1)."""
+        nq, nr, ns = self.blocks[b].nqrs
+        n1 = nr if axis == 1 else nq
+        n2 = nr if axis == 3 else ns
+        a = np.zeros((ncomp, n2, n1))
+        _lib.check(_lib.load().wql3d_get_plane(self.handle, b, int(axis), int(index), int(c0), int(ncomp), _ptr(a)),
+                   "wql3d_get_plane")
+        return a
+
     def seismograms(self, b: int = 0) -> np.ndarray:
         blk = self.blocks[b]
         nrec = 0 if blk.receivers is None else len(blk.receivers)
