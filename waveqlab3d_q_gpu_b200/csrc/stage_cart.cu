@@ -26,13 +26,33 @@ static void launch_shell(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
   ++*c.launches;
 }
 
+template <typename T, int RESP>
+static void launch_both(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
+  if (c.side && tuning().overlap) {
+    // the shell (latency-bound, one thread per scattered point) on the side
+    // stream next to the bandwidth-bound interior tiles; both read the
+    // current fields and write disjoint points
+    StageCtx sc = c;
+    sc.stream = c.side;
+    cudaEventRecord(c.fork, c.stream);
+    cudaStreamWaitEvent(c.side, c.fork, 0);
+    launch_shell<T, RESP>(b, sc, a);
+    cudaEventRecord(c.join, c.side);
+    launch_interior<T, RESP>(b, c, a);
+    cudaStreamWaitEvent(c.stream, c.join, 0);
+    return;
+  }
+  launch_interior<T, RESP>(b, c, a);
+  launch_shell<T, RESP>(b, c, a);
+}
+
 template <typename T>
 void launch_cart_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
   switch (c.response) {
-    case RESP_EL: launch_interior<T, RESP_EL>(b, c, a); launch_shell<T, RESP_EL>(b, c, a); break;
-    case RESP_Q4: launch_interior<T, RESP_Q4>(b, c, a); launch_shell<T, RESP_Q4>(b, c, a); break;
-    case RESP_Q8: launch_interior<T, RESP_Q8>(b, c, a); launch_shell<T, RESP_Q8>(b, c, a); break;
-    default: launch_interior<T, RESP_FQ8>(b, c, a); launch_shell<T, RESP_FQ8>(b, c, a); break;
+    case RESP_EL: launch_both<T, RESP_EL>(b, c, a); break;
+    case RESP_Q4: launch_both<T, RESP_Q4>(b, c, a); break;
+    case RESP_Q8: launch_both<T, RESP_Q8>(b, c, a); break;
+    default: launch_both<T, RESP_FQ8>(b, c, a); break;
   }
 }
 

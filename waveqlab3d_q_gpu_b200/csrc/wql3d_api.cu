@@ -149,6 +149,10 @@ struct wql3d_domain {
   int response = 0;
   int nmech = 0;
   cudaStream_t stream = nullptr;
+  // second stream for the Cartesian near-boundary shell, forked from and
+  // joined back to `stream` every stage (the shell overlaps the interior)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   Alloc mem;
   HostBlock hb[2];
   Blk<double> bd[2];
@@ -894,7 +898,7 @@ template <typename T>
 void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = false) {
   Blk<T> &b = blk<T>(d, bi);
   const int mesh = d->hb[bi].mesh;
-  StageCtx c{d->stream, d->response, &d->launches};
+  StageCtx c{d->stream, d->response, &d->launches, d->side, d->fork, d->join};
   const bool special = tuning().generic || b.mms || b.fd != WQL3D_FD_TRADITIONAL6;
   if (fused && mesh == WQL3D_MESH_CARTESIAN && a.flags == F_ALL && !special)
     launch_cart_stage<T>(b, c, a);
@@ -1083,10 +1087,17 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
   auto cleanup = [&](int code) {
     cudaStreamSynchronize(d->stream);
     d->mem.release();
+    if (d->side) cudaStreamDestroy(d->side);
+    if (d->fork) cudaEventDestroy(d->fork);
+    if (d->join) cudaEventDestroy(d->join);
     cudaStreamDestroy(d->stream);
     delete d;
     return code;
   };
+  if (cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->join, cudaEventDisableTiming) != cudaSuccess)
+    return cleanup(fail(WQL3D_ECUDA, "side stream creation failed"));
   if (d->mem.get(&d->time, 1) != cudaSuccess) return cleanup(fail(WQL3D_ENOMEM, "time"));
   DevTime t0 = {0.0, 1, 0, 0, 0};
   if (cudaMemcpyAsync(d->time, &t0, sizeof(t0), cudaMemcpyHostToDevice, d->stream) != cudaSuccess ||
@@ -1164,8 +1175,12 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
 int wql3d_domain_destroy(wql3d_domain *d) {
   if (!d) return WQL3D_OK;
   cudaStreamSynchronize(d->stream);
+  if (d->side) cudaStreamSynchronize(d->side);
   if (d->graph) cudaGraphExecDestroy(d->graph);
   d->mem.release();
+  if (d->side) cudaStreamDestroy(d->side);
+  if (d->fork) cudaEventDestroy(d->fork);
+  if (d->join) cudaEventDestroy(d->join);
   cudaStreamDestroy(d->stream);
   delete d;
   return WQL3D_OK;

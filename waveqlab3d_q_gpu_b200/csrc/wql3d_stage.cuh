@@ -29,6 +29,10 @@ struct StageCtx {
   cudaStream_t stream;
   int response;       // RESP_*
   int64_t *launches;  // kernel-launch counter of the owning domain
+  // optional second stream and fork / join events: the Cartesian shell runs
+  // there, concurrently with the interior (disjoint points, read-only F)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 // tuning switches read once per translation unit from the environment
@@ -40,6 +44,7 @@ struct Tuning {
   int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default), 2 or 4 in FP64; 4 (default), 5 or 6 in FP32
   int mvpf = 0;       // k_curv_fused: L2 prefetch of the memory variables on entry
   int mvring = 0;     // k_curv_fused: memory variables through a shared-memory ring of 2, 3 or 6 components
+  int overlap = 1;    // Cartesian stage: shell on the side stream, concurrent with the interior
 };
 
 inline Tuning tuning() {
@@ -49,6 +54,7 @@ inline Tuning tuning() {
     if (const char *e = getenv("WQL3D_FUSED_MINB")) r.fused_minb = atoi(e);
     if (const char *e = getenv("WQL3D_MV_PREFETCH")) r.mvpf = atoi(e);
     if (const char *e = getenv("WQL3D_MV_RING")) r.mvring = atoi(e);
+    if (const char *e = getenv("WQL3D_SHELL_OVERLAP")) r.overlap = atoi(e);
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
       if (strcmp(e, "curv_generic_update") == 0) r.lean = 0;

@@ -41,8 +41,9 @@ class FaultOutput:
     def write_fault(self):
         """write_fault + the Vface write of write_fault_output (state before the step)."""
         d = self.domain
-        self._put("Uface", d.fields(0)[:, :, :, -1])
-        self._put("Vface", d.fields(1)[:, :, :, 0])
+        # the two interface faces through the device plane gather
+        self._put("Uface", d.plane(0, 1, d.blocks[0].nqrs[0]))
+        self._put("Vface", d.plane(1, 1, 1))
         self._put("S", d.fault("S"))
         self._put("state", d.fault("state"))
 
