@@ -32,6 +32,16 @@ class _FakeDomain:
     def fault(self, name):
         return self._grid(dict(FILES)[name], 1000.0 * self.step + 0.5)
 
+    @property
+    def blocks(self):
+        from types import SimpleNamespace
+        return [SimpleNamespace(nqrs=(self.nq, self.nr, self.ns))] * 2
+
+    def plane(self, b, axis, index, c0=0, ncomp=9):
+        # the device plane gather of Domain.plane, on the fake fields
+        assert axis == 1
+        return self.fields(b)[c0:c0 + ncomp, :, :, index - 1]
+
     def time_step_RK(self, n):
         self.step = n
 

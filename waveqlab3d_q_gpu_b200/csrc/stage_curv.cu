@@ -18,29 +18,6 @@ static void launch_fused_mb(Blk<T> &b, const StageCtx &c, const StageArgs &a, un
   }
 }
 
-// fused stage with the memory-variable ring of RING component slots
-template <typename T, int MB, int RING, int RESP>
-static void launch_fused_ring_r(const StageCtx &c, Blk<T> &b, const StageArgs &a, unsigned gr) {
-  constexpr int N = RESP == RESP_Q4 ? 4 : 8;
-  const int sm = RING * 2 * N * 128 * (int)sizeof(T);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_curv_fused<T, RESP, MB, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    attr = true;
-  }
-  k_curv_fused<T, RESP, MB, RING><<<gr, 128, sm, c.stream>>>(b, a);
-}
-
-template <typename T, int MB, int RING>
-static void launch_fused_ring(Blk<T> &b, const StageCtx &c, const StageArgs &a, unsigned gr) {
-  switch (c.response) {
-    case RESP_EL: k_curv_fused<T, RESP_EL, MB><<<gr, 128, 0, c.stream>>>(b, a); break;
-    case RESP_Q4: launch_fused_ring_r<T, MB, RING, RESP_Q4>(c, b, a, gr); break;
-    case RESP_Q8: launch_fused_ring_r<T, MB, RING, RESP_Q8>(c, b, a, gr); break;
-    default: launch_fused_ring_r<T, MB, RING, RESP_FQ8>(c, b, a, gr); break;
-  }
-}
-
 template <typename T>
 static void launch_curv_fused(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
   const long long npts = (long long)b.nx * b.ny * b.nz;
@@ -51,12 +28,10 @@ static void launch_curv_fused(Blk<T> &b, const StageCtx &c, const StageArgs &a) 
   const unsigned gr = (unsigned)((npts + 127) / 128);
   const int mb = tuning().fused_minb;
   StageArgs la = a;
-  la.pf = tuning().mvpf;
-  const int ring = tuning().mvring;
-  if (ring == 2) launch_fused_ring<T, sizeof(T) == 8 ? 3 : 4, 2>(b, c, la, gr);
-  else if (ring == 3) launch_fused_ring<T, sizeof(T) == 8 ? 3 : 4, 3>(b, c, la, gr);
-  else if (ring == 6) launch_fused_ring<T, sizeof(T) == 8 ? 2 : 4, 6>(b, c, la, gr);
-  else if (sizeof(T) == 8) {
+  // L2 prefetch of the memory variables: on by default in FP32 only (measured
+  // 2.7 % faster there, 4.5 % slower in FP64)
+  la.pf = tuning().mvpf >= 0 ? tuning().mvpf : (sizeof(T) == 4 ? 1 : 0);
+  if (sizeof(T) == 8) {
     if (mb == 2) launch_fused_mb<T, 2>(b, c, la, gr);
     else if (mb == 4) launch_fused_mb<T, 4>(b, c, la, gr);
     else launch_fused_mb<T, 3>(b, c, la, gr);

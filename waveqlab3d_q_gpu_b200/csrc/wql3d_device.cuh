@@ -177,9 +177,6 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc, bool 
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-// wait until at most K of this thread's committed groups are still in flight
-template <int K>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
 
 // central (interior) SBP row at 1-based i of n points on axis a: 7 <= i <= n-6,
 // or up to an open face of a slab
@@ -1458,16 +1455,15 @@ __device__ __forceinline__ void slab_strain(const Blk<T> &b, int x, int y, int z
   q0 = Qp[c0 * PV]; q1 = Qp[c1 * PV]; q2 = Qp[c2 * PV];
 }
 
-// memory variables of one point: eta sums subtracted from s[3:9] (when
-// do_rhs), rates scaled / accumulated, eta integrated (F_UPDATE).  The rate
-// of src/RHS_Interior.f90:2599-2908 (Q4 / Q8) is regrouped per component as
-// w_l * (2 mu Qs^-1 e) + w_l * (((lambda + 2 mu) Qp^-1 - 2 mu Qs^-1) tr) and
-// that of :3361-3477 (fQ8) as s_l (2 mu e) + (p_l (lambda + 2 mu) tr -
-// s_l 2 mu tr), so only per-point scalars and the per-mechanism constants
-// are live: the same products in another association (rounding level).
 // Rates and update of the N memory variables of stress component c at one
 // point: ev / dv hold eta and deta on entry, the values to store on return;
-// the sum of the old eta is subtracted from the stress rate s[3 + c].
+// the sum of the old eta is subtracted from the stress rate s[3 + c] (when
+// do_rhs), the rates scaled / accumulated, eta integrated (F_UPDATE).  The
+// rate of src/RHS_Interior.f90:2599-2908 (Q4 / Q8) is regrouped per component
+// as w_l * (2 mu Qs^-1 e) + w_l * (((lambda + 2 mu) Qp^-1 - 2 mu Qs^-1) tr)
+// and that of :3361-3477 (fQ8) as s_l (2 mu e) + (p_l (lambda + 2 mu) tr -
+// s_l 2 mu tr), so only per-point scalars and the per-mechanism constants
+// are live: the same products in another association (rounding level).
 template <typename T, int RESP, int N>
 __device__ __forceinline__ void mv_component(const Blk<T> &b, const StageArgs &a, int c, int active, T fn, T ft, T fs,
                                              T l2m, T two_mu, const T e[6], T tr, T s[9], bool do_rhs, T ev[N],
@@ -1516,6 +1512,7 @@ __device__ __forceinline__ void mv_factors(const Blk<T> &b, long long p, T lam, 
   fs = RESP == RESP_FQ8 ? mu : mu * qs;                        // shear strain factor
 }
 
+// memory variables of one point, straight from and to global memory
 template <typename T, int RESP>
 __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p, T lam,
                                                T mu, const T e[6], T tr, T s[9], bool do_rhs) {
@@ -1540,64 +1537,6 @@ __device__ __forceinline__ void anelastic_lean(const Blk<T> &b, const StageArgs 
       dp[(long long)(c * N + i) * V] = dv[i];
       if (a.flags & F_UPDATE) ep[(long long)(c * N + i) * V] = ev[i];
     }
-  }
-}
-
-// Memory-variable ring of k_curv_fused: per thread RING component slots of
-// N eta + N deta values in shared memory ([slot][2N][128], thread fastest),
-// filled by cp.async so that the memory-variable stream is in flight while
-// the derivative gathers run.
-template <typename T, int N>
-__device__ __forceinline__ void mv_ring_fill(const Blk<T> &b, long long p, int c, T *ring, int slot) {
-  const long long V = b.vol;
-  T *dst = ring + (long long)slot * 2 * N * 128 + threadIdx.x;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    cp_async<sizeof(T)>(dst + i * 128, b.eta + (long long)(c * N + i) * V + p, true);
-    cp_async<sizeof(T)>(dst + (N + i) * 128, b.deta + (long long)(c * N + i) * V + p, true);
-  }
-  cp_async_commit();
-}
-
-__device__ __forceinline__ void cp_async_wait_upto(int k) {
-  // k is a compile-time constant after unrolling; map it to the immediate
-  if (k <= 0) cp_async_wait<0>();
-  else if (k == 1) cp_async_wait<1>();
-  else if (k == 2) cp_async_wait<2>();
-  else if (k == 3) cp_async_wait<3>();
-  else if (k == 4) cp_async_wait<4>();
-  else cp_async_wait<5>();
-}
-
-template <typename T, int RESP, int RING>
-__device__ __forceinline__ void anelastic_ring(const Blk<T> &b, const StageArgs &a, int x, int y, int z, long long p,
-                                               T lam, T mu, const T e[6], T tr, T s[9], bool do_rhs, T *ring) {
-  constexpr int N = RESP == RESP_Q4 ? 4 : 8;
-  const long long V = b.vol;
-  const int active = 1 + ((x - 1) & 1) + 2 * ((y - 1) & 1) + 4 * ((z - 1) & 1);
-  T *__restrict__ ep = b.eta + p;
-  T *__restrict__ dp = b.deta + p;
-  T fn, ft, fs, l2m, two_mu;
-  mv_factors<T, RESP>(b, p, lam, mu, fn, ft, fs, l2m, two_mu);
-#pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    // components c .. min(c + RING - 1, 5) are committed; wait for c
-    cp_async_wait_upto((c + RING - 1 < 5 ? c + RING - 1 : 5) - c);
-    const T *src = ring + (long long)(c % RING) * 2 * N * 128 + threadIdx.x;
-    T ev[N], dv[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      ev[i] = src[i * 128];
-      dv[i] = src[(N + i) * 128];
-    }
-    mv_component<T, RESP, N>(b, a, c, active, fn, ft, fs, l2m, two_mu, e, tr, s, do_rhs, ev, dv);
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      dp[(long long)(c * N + i) * V] = dv[i];
-      if (a.flags & F_UPDATE) ep[(long long)(c * N + i) * V] = ev[i];
-    }
-    // the slot's values are consumed (the stores above depend on them)
-    if (c + RING < 6) mv_ring_fill<T, N>(b, p, c + RING, ring, c % RING);
   }
 }
 
@@ -1909,21 +1848,11 @@ __global__ void __launch_bounds__(MAXT, MINB) k_curv_point(Blk<T> b, StageArgs a
 // rates take the PML correction from Q before this stage's Q update, as in
 // the split passes.
 // ---------------------------------------------------------------------------
-// RING > 0: the memory variables arrive through the shared-memory ring of
-// anelastic_ring (dynamic shared memory RING * 2 * N * 128 values), its
-// first RING components requested on entry.
-template <typename T, int RESP, int MINB, int RING = 0>
+template <typename T, int RESP, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a) {
-  extern __shared__ __align__(16) unsigned char smraw[];
   int x, y, z;
   if (!flat_point(b, x, y, z)) return;
   const long long p = pidx(b, x, y, z);
-  constexpr int NMV = RESP == RESP_Q4 ? 4 : 8;
-  T *ring = reinterpret_cast<T *>(smraw);
-  if (RING > 0 && RESP != RESP_EL) {
-#pragma unroll
-    for (int c = 0; c < RING; ++c) mv_ring_fill<T, NMV>(b, p, c, ring, c);
-  }
   const long long V = b.vol;
   const T *__restrict__ F = a.cur ? b.F1 : b.F0;
   T *__restrict__ Fn = a.cur ? b.F0 : b.F1;
@@ -2019,8 +1948,7 @@ __global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a)
   if (RESP != RESP_EL) {
     const T lm = rhs ? lam : b.M[p], mm = rhs ? mu : b.M[V + p];
     T s6[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (RING > 0) anelastic_ring<T, RESP, RING>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs, ring);
-    else anelastic_lean<T, RESP>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs);
+    anelastic_lean<T, RESP>(b, a, x, y, z, p, lm, mm, e, tr, s6, rhs);
     if (rhs) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) df[3 + c] = df[3 + c] + s6[3 + c];

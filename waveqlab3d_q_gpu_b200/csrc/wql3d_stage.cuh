@@ -42,8 +42,7 @@ struct Tuning {
   int lean = 1;       // curvilinear update: k_curv_point (0: generic point update k_curv_update)
   int curv_fused = 1; // curvilinear stage in one pass, k_curv_fused (0: derivative / memory-variable / point passes)
   int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default), 2 or 4 in FP64; 4 (default), 5 or 6 in FP32
-  int mvpf = 0;       // k_curv_fused: L2 prefetch of the memory variables on entry
-  int mvring = 0;     // k_curv_fused: memory variables through a shared-memory ring of 2, 3 or 6 components
+  int mvpf = -1;      // k_curv_fused: L2 prefetch of the memory variables on entry (-1: FP32 only)
   int overlap = 1;    // Cartesian stage: shell on the side stream, concurrent with the interior
 };
 
@@ -53,7 +52,6 @@ inline Tuning tuning() {
     if (const char *e = getenv("WQL3D_ZCHUNK")) r.zchunk = atoi(e) > 0 ? atoi(e) : 1;
     if (const char *e = getenv("WQL3D_FUSED_MINB")) r.fused_minb = atoi(e);
     if (const char *e = getenv("WQL3D_MV_PREFETCH")) r.mvpf = atoi(e);
-    if (const char *e = getenv("WQL3D_MV_RING")) r.mvring = atoi(e);
     if (const char *e = getenv("WQL3D_SHELL_OVERLAP")) r.overlap = atoi(e);
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
