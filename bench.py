@@ -119,14 +119,15 @@ def load_peaks():
 
 
 def load_traffic(key):
-    """DRAM bytes per RK stage of the stage kernels from the committed ncu summary, if any."""
+    """(DRAM bytes per RK stage of the stage kernels, how they were measured)
+    from the committed ncu summary, or (None, None)."""
     try:
         with open(os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")) as f:
             t = json.load(f)
         rec = t.get(key)
-        return None if rec is None else float(rec["dram_bytes_per_stage"])
+        return (None, None) if rec is None else (float(rec["dram_bytes_per_stage"]), rec.get("how"))
     except Exception:
-        return None
+        return None, None
 
 
 class ClockSampler:
@@ -382,7 +383,7 @@ def main():
                          f"reference solver, OpenMP over z)"}
 
     if rank == 0:
-        traffic = load_traffic(name)
+        traffic, traffic_how = load_traffic(name)
         line = {
             "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": r64["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -394,7 +395,8 @@ def main():
             "e2e": e2e,
             "gpu_launches": r64["launches"],
             "roofline": {"bound": "hbm", "achieved": r64["achieved"], "peak": peak, "unit": "GB/s",
-                         "frac": r64["achieved"] / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "frac": r64["achieved"] / peak, "traffic": traffic, "traffic_how": traffic_how,
+                         "peak_kind": peak_kind,
                          "kernel": "one RK stage: stage kernels of both blocks + interface kernel",
                          "stage_ms": r64["stage_ms"], "alg_bytes_per_stage": words * 8},
             "cpu_baseline": cpu,

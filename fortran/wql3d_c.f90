@@ -82,6 +82,12 @@ module wql3d_c
      integer(c_int) function wql3d_scale_rate_array(rate, n, a, stream) bind(C)
        import; type(c_ptr), value :: rate, stream; integer(c_int64_t), value :: n; real(c_double), value :: a
      end function
+     integer(c_int) function wql3d_traditional_cartesian_rhs(field, rate, metricx, metricy, metricz, material, &
+          n1, n2, n3, nm, nmat, xlo, xhi, ylo, yhi, zlo, zhi, hq, hr, hs, stream) bind(C)
+       import; type(c_ptr), value :: field, rate, metricx, metricy, metricz, material, stream
+       integer(c_int32_t), value :: n1, n2, n3, nm, nmat, xlo, xhi, ylo, yhi, zlo, zhi
+       real(c_double), value :: hq, hr, hs
+     end function
      integer(c_int) function wql3d_update_state_array(state, rate, n, dt, stream) bind(C)
        import; type(c_ptr), value :: state, rate, stream; integer(c_int64_t), value :: n; real(c_double), value :: dt
      end function

@@ -269,6 +269,18 @@ int wql3d_try_traditional_rhs(wql3d_domain *d, int *handled);
 
 /* rk_vector backend on raw device arrays (rk_vector_openacc.f90:22-75) */
 int wql3d_scale_rate_array(double *rate, int64_t n, double coefficient, void *stream);
+/* try_traditional_cartesian_rhs seam of the reference's OpenACC build
+   (src/traditional_cartesian_rhs_openacc.f90): adds the strict-interior rates
+   of a Cartesian elastic traditional-6 block to `rate`, on the caller's device
+   arrays field / rate (n1, n2, n3, 9), metricx / metricy / metricz
+   (n1, n2, n3, nm) and material (n1, n2, n3, nmat), Fortran order, for the
+   1-based box xlo..xhi x ylo..yhi x zlo..zhi of those arrays (3 points inside
+   each side), spacings hq, hr, hs, on `stream`.  Products and sums in the
+   reference's order without fused multiply-add. */
+int wql3d_traditional_cartesian_rhs(const double *field, double *rate, const double *metricx, const double *metricy,
+                                    const double *metricz, const double *material, int32_t n1, int32_t n2, int32_t n3,
+                                    int32_t nm, int32_t nmat, int32_t xlo, int32_t xhi, int32_t ylo, int32_t yhi,
+                                    int32_t zlo, int32_t zhi, double hq, double hr, double hs, void *stream);
 int wql3d_update_state_array(double *state, const double *rate, int64_t n, double increment, void *stream);
 
 /* receivers: samples taken at stage 1 before the update (time_step.f90:137),

@@ -48,7 +48,7 @@ def test_abi_version_and_entry_points():
     names = set(re.findall(r"function (wql3d_\w+)\(", src))
     declared = set(re.findall(r"(wql3d_\w+)\s*\(", re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)))
     assert names and names <= declared
-    for f in ("rk_vector_wql3d.f90", "time_step_wql3d.f90"):
+    for f in ("rk_vector_wql3d.f90", "time_step_wql3d.f90", "traditional_cartesian_rhs_wql3d.f90"):
         body = open(os.path.join(ROOT, "fortran", f)).read()
         for used in re.findall(r"(wql3d_\w+)\(", body):
             assert used in names, (f, used)

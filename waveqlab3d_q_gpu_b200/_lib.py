@@ -88,6 +88,7 @@ SIGNATURES = {
     "wql3d_update_fields": [C.c_void_p, C.c_double],
     "wql3d_try_traditional_rhs": [C.c_void_p, C.POINTER(C.c_int)],
     "wql3d_scale_rate_array": [C.c_void_p, C.c_int64, C.c_double, C.c_void_p],
+    "wql3d_traditional_cartesian_rhs": [C.c_void_p] * 6 + [C.c_int32] * 11 + [C.c_double] * 3 + [C.c_void_p],
     "wql3d_update_state_array": [C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_void_p],
     "wql3d_get_seismograms": [C.c_void_p, C.c_int, dp, ip],
     "wql3d_receiver_index": [C.c_void_p, C.c_int, ip],

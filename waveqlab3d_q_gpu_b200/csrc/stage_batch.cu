@@ -97,18 +97,35 @@ __global__ void k_batch_advance(DevTime *const *times, int n, double dt) {
   tm->n = tm->n + 1;
 }
 
+// interior tiles (part 0) or near-boundary shell (part 1) of one class
 template <typename T, int RESP>
-void launch_class(const BatchClass<T> &C, const StageArgs &a, int zchunk, cudaStream_t s, int64_t *launches) {
-  if (C.tiles > 0) {
+void launch_class(const BatchClass<T> &C, const StageArgs &a, int zchunk, cudaStream_t s, int part,
+                  int64_t *launches) {
+  if (part == 0 && C.tiles > 0) {
     const size_t sm = SplitSmem<T, 4>::bytes;
     cudaFuncSetAttribute(k_batch_interior<T, RESP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_batch_interior<T, RESP><<<C.tiles, 256, sm, s>>>(C, a, zchunk);
     ++*launches;
   }
-  if (C.shell_ctas > 0) {
+  if (part == 1 && C.shell_ctas > 0) {
     if (C.sep) k_batch_shell<T, RESP, true><<<C.shell_ctas, 128, 0, s>>>(C, a);
     else k_batch_shell<T, RESP, false><<<C.shell_ctas, 128, 0, s>>>(C, a);
     ++*launches;
+  }
+}
+
+template <typename T>
+void launch_part(const BatchClass<T> *classes, int ncls, const StageArgs &a, int zchunk, cudaStream_t s, int part,
+                 int64_t *launches) {
+  for (int c = 0; c < ncls; ++c) {
+    const BatchClass<T> &C = classes[c];
+    if (C.nshots == 0) continue;
+    switch (C.resp) {
+      case RESP_EL: launch_class<T, RESP_EL>(C, a, zchunk, s, part, launches); break;
+      case RESP_Q4: launch_class<T, RESP_Q4>(C, a, zchunk, s, part, launches); break;
+      case RESP_Q8: launch_class<T, RESP_Q8>(C, a, zchunk, s, part, launches); break;
+      default: launch_class<T, RESP_FQ8>(C, a, zchunk, s, part, launches); break;
+    }
   }
 }
 
@@ -116,17 +133,20 @@ void launch_class(const BatchClass<T> &C, const StageArgs &a, int zchunk, cudaSt
 
 template <typename T>
 void launch_batch_stage(const BatchClass<T> *classes, int ncls, const StageArgs &a, int zchunk, cudaStream_t s,
-                        int64_t *launches) {
-  for (int c = 0; c < ncls; ++c) {
-    const BatchClass<T> &C = classes[c];
-    if (C.nshots == 0) continue;
-    switch (C.resp) {
-      case RESP_EL: launch_class<T, RESP_EL>(C, a, zchunk, s, launches); break;
-      case RESP_Q4: launch_class<T, RESP_Q4>(C, a, zchunk, s, launches); break;
-      case RESP_Q8: launch_class<T, RESP_Q8>(C, a, zchunk, s, launches); break;
-      default: launch_class<T, RESP_FQ8>(C, a, zchunk, s, launches); break;
-    }
+                        cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, int64_t *launches) {
+  if (side) {
+    // every class's shell on the side stream, next to the interior tiles
+    // (disjoint points of independent shots)
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    launch_part<T>(classes, ncls, a, zchunk, side, 1, launches);
+    cudaEventRecord(join, side);
+    launch_part<T>(classes, ncls, a, zchunk, s, 0, launches);
+    cudaStreamWaitEvent(s, join, 0);
+    return;
   }
+  launch_part<T>(classes, ncls, a, zchunk, s, 0, launches);
+  launch_part<T>(classes, ncls, a, zchunk, s, 1, launches);
 }
 
 template <typename T>
@@ -143,7 +163,7 @@ void launch_batch_advance(DevTime *const *times, int nshots, double dt, cudaStre
 }
 
 template void launch_batch_stage<WQL3D_REAL>(const BatchClass<WQL3D_REAL> *, int, const StageArgs &, int,
-                                             cudaStream_t, int64_t *);
+                                             cudaStream_t, cudaStream_t, cudaEvent_t, cudaEvent_t, int64_t *);
 template void launch_batch_sample<WQL3D_REAL>(const Blk<WQL3D_REAL> *, DevTime *const *, int, int, int,
                                               cudaStream_t, int64_t *);
 template void launch_batch_advance<WQL3D_REAL>(DevTime *const *, int, double, cudaStream_t, int64_t *);

@@ -353,6 +353,62 @@ __global__ void k_plane_gather(Blk<T> b, const T *F, int dir, int index, int c0,
   }
 }
 
+// Strict-interior rates of a Cartesian elastic traditional-6 block on the
+// caller's arrays (cartesian_elastic_o6_interior_kernel of
+// src/traditional_cartesian_rhs_openacc.f90): field, rate, metricx/y/z and
+// material dimensioned (n1, n2, n3, .) as the caller holds them, the box
+// [lo, lo + ext) in their 1-based indices.  Every product and sum in the
+// reference's order without contraction, so the rates equal a plain IEEE
+// evaluation of the same expressions.
+struct CartRhsArgs {
+  const double *field, *mx, *my, *mz, *mat;
+  double *rate;
+  int n1, n2, n3;
+  int lo[3], ext[3];
+  double cx[3], cy[3], cz[3];
+};
+
+__global__ void __launch_bounds__(256) k_trad_cart_rhs(CartRhsArgs a) {
+  const long long vol = (long long)a.n1 * a.n2 * a.n3;
+  const long long sy = a.n1, sz = (long long)a.n1 * a.n2;
+  const long long npts = (long long)a.ext[0] * a.ext[1] * a.ext[2];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npts;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = a.lo[0] + (int)(i % a.ext[0]);
+    const int y = a.lo[1] + (int)((i / a.ext[0]) % a.ext[1]);
+    const int z = a.lo[2] + (int)(i / ((long long)a.ext[0] * a.ext[1]));
+    const long long p = (long long)(x - 1) + sy * (y - 1) + sz * (z - 1);
+    const double mx = a.mx[p], my = a.my[vol + p], mz = a.mz[2 * vol + p];
+    double dfx[9], dfy[9], dfz[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) { dfx[c] = 0.0; dfy[c] = 0.0; dfz[c] = 0.0; }
+#pragma unroll
+    for (int s = 1; s <= 3; ++s) {
+      const double kx = __dmul_rn(mx, a.cx[s - 1]), ky = __dmul_rn(my, a.cy[s - 1]), kz = __dmul_rn(mz, a.cz[s - 1]);
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        const double *f = a.field + c * vol + p;
+        dfx[c] = __dadd_rn(dfx[c], __dmul_rn(kx, __dsub_rn(__ldg(f + s), __ldg(f - s))));
+        dfy[c] = __dadd_rn(dfy[c], __dmul_rn(ky, __dsub_rn(__ldg(f + s * sy), __ldg(f - s * sy))));
+        dfz[c] = __dadd_rn(dfz[c], __dmul_rn(kz, __dsub_rn(__ldg(f + s * sz), __ldg(f - s * sz))));
+      }
+    }
+    const double lam = a.mat[p], mu = a.mat[vol + p];
+    const double a1 = 1.0 / a.mat[2 * vol + p];
+    const double a2 = __dadd_rn(lam, __dmul_rn(2.0, mu)), a3 = lam, a4 = mu;
+    double *r = a.rate + p;
+    r[0] = __dadd_rn(r[0], __dmul_rn(a1, __dadd_rn(__dadd_rn(dfx[3], dfy[6]), dfz[7])));
+    r[vol] = __dadd_rn(r[vol], __dmul_rn(a1, __dadd_rn(__dadd_rn(dfx[6], dfy[4]), dfz[8])));
+    r[2 * vol] = __dadd_rn(r[2 * vol], __dmul_rn(a1, __dadd_rn(__dadd_rn(dfx[7], dfy[8]), dfz[5])));
+    r[3 * vol] = __dadd_rn(__dadd_rn(r[3 * vol], __dmul_rn(a2, dfx[0])), __dmul_rn(a3, __dadd_rn(dfy[1], dfz[2])));
+    r[4 * vol] = __dadd_rn(__dadd_rn(r[4 * vol], __dmul_rn(a2, dfy[1])), __dmul_rn(a3, __dadd_rn(dfx[0], dfz[2])));
+    r[5 * vol] = __dadd_rn(__dadd_rn(r[5 * vol], __dmul_rn(a2, dfz[2])), __dmul_rn(a3, __dadd_rn(dfx[0], dfy[1])));
+    r[6 * vol] = __dadd_rn(r[6 * vol], __dmul_rn(a4, __dadd_rn(dfy[0], dfx[1])));
+    r[7 * vol] = __dadd_rn(r[7 * vol], __dmul_rn(a4, __dadd_rn(dfz[0], dfx[2])));
+    r[8 * vol] = __dadd_rn(r[8 * vol], __dmul_rn(a4, __dadd_rn(dfz[1], dfy[2])));
+  }
+}
+
 template <typename T>
 __global__ void k_convert(const double *src, T *dst, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1570,6 +1626,34 @@ int wql3d_update_state_array(double *state, const double *rate, int64_t n, doubl
   return WQL3D_OK;
 }
 
+int wql3d_traditional_cartesian_rhs(const double *field, double *rate, const double *metricx, const double *metricy,
+                                    const double *metricz, const double *material, int32_t n1, int32_t n2, int32_t n3,
+                                    int32_t nm, int32_t nmat, int32_t xlo, int32_t xhi, int32_t ylo, int32_t yhi,
+                                    int32_t zlo, int32_t zhi, double hq, double hr, double hs, void *stream) {
+  if (!field || !rate || !metricx || !metricy || !metricz || !material) return fail(WQL3D_EINVAL, "rhs arrays");
+  if (n1 < 1 || n2 < 1 || n3 < 1 || nm < 3 || nmat < 3) return fail(WQL3D_EINVAL, "rhs array shape");
+  // the box must leave the three stencil points on each side inside the arrays
+  if (xlo < 4 || xhi > n1 - 3 || ylo < 4 || yhi > n2 - 3 || zlo < 4 || zhi > n3 - 3)
+    return fail(WQL3D_EINVAL, "rhs interior bounds");
+  if (xlo > xhi || ylo > yhi || zlo > zhi) return WQL3D_OK;
+  CartRhsArgs a;
+  a.field = field; a.rate = rate; a.mx = metricx; a.my = metricy; a.mz = metricz; a.mat = material;
+  a.n1 = n1; a.n2 = n2; a.n3 = n3;
+  a.lo[0] = xlo; a.lo[1] = ylo; a.lo[2] = zlo;
+  a.ext[0] = xhi - xlo + 1; a.ext[1] = yhi - ylo + 1; a.ext[2] = zhi - zlo + 1;
+  const double c[3] = {0.75, -0.15, 1.0 / 60.0};
+  for (int s = 0; s < 3; ++s) {
+    a.cx[s] = c[s] / hq;
+    a.cy[s] = c[s] / hr;
+    a.cz[s] = c[s] / hs;
+  }
+  const long long npts = (long long)a.ext[0] * a.ext[1] * a.ext[2];
+  const unsigned g = (unsigned)std::min<long long>((npts + 255) / 256, 148LL * 64);
+  k_trad_cart_rhs<<<g, 256, 0, (cudaStream_t)stream>>>(a);
+  CK(cudaGetLastError());
+  return WQL3D_OK;
+}
+
 int wql3d_get_seismograms(wql3d_domain *d, int bi, double *out, int32_t *nsamples) {
   DOM_CHECK(d, bi);
   DevTime h;
@@ -1921,6 +2005,8 @@ struct wql3d_batch {
   int fp32 = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev = nullptr;
+  cudaStream_t side = nullptr;               // the shells' stream (fork / join per stage)
+  cudaEvent_t fork = nullptr, join = nullptr;
   std::vector<wql3d_domain *> doms;
   Alloc mem;
   void *blks = nullptr;           // device array of Blk<T>
@@ -1991,7 +2077,8 @@ void batch_enqueue_step(wql3d_batch *bt, double dt, int w_stride) {
     a.Bdt = kRkB[st - 1] * dt;
     a.dt = dt;
     a.time = nullptr;
-    launch_batch_stage<T>(cl, ncl, a, bt->zchunk, bt->stream, &bt->launches);
+    launch_batch_stage<T>(cl, ncl, a, bt->zchunk, bt->stream, tuning().overlap ? bt->side : nullptr, bt->fork,
+                          bt->join, &bt->launches);
     bt->cur ^= 1;
   }
   launch_batch_advance<T>(bt->times, bt->n, dt, bt->stream, &bt->launches);
@@ -2083,18 +2170,27 @@ int wql3d_batch_create(wql3d_domain *const *domains, int32_t n, wql3d_batch **ou
   bt->fp32 = fp32;
   bt->doms.assign(domains, domains + n);
   bt->cur = domains[0]->cur;
+  auto drop = [](wql3d_batch *b) {
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+  };
   if (cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&bt->ev, cudaEventDisableTiming) != cudaSuccess) {
-    delete bt;
+      cudaEventCreateWithFlags(&bt->ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&bt->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&bt->join, cudaEventDisableTiming) != cudaSuccess) {
+    drop(bt);
     return fail(WQL3D_ECUDA, "batch stream");
   }
   bt->mem.stream = bt->stream;
   auto bad = [&](int code) {
     cudaStreamSynchronize(bt->stream);
     bt->mem.release();
-    cudaEventDestroy(bt->ev);
-    cudaStreamDestroy(bt->stream);
-    delete bt;
+    drop(bt);
     return code;
   };
   const size_t bsz = fp32 ? sizeof(Blk<float>) : sizeof(Blk<double>);
@@ -2189,8 +2285,12 @@ int wql3d_batch_synchronize(wql3d_batch *bt) {
 int wql3d_batch_destroy(wql3d_batch *bt) {
   if (!bt) return WQL3D_OK;
   cudaStreamSynchronize(bt->stream);
+  cudaStreamSynchronize(bt->side);
   if (bt->graph) cudaGraphExecDestroy(bt->graph);
   bt->mem.release();
+  cudaEventDestroy(bt->fork);
+  cudaEventDestroy(bt->join);
+  cudaStreamDestroy(bt->side);
   cudaEventDestroy(bt->ev);
   cudaStreamDestroy(bt->stream);
   delete bt;

@@ -21,9 +21,11 @@ struct BatchClass {
   DevTime *const *times;   // every shot's step time / sample counter (device)
 };
 
+// side != nullptr: the shells run on the side stream (fork / join events),
+// concurrently with the interior tiles
 template <typename T>
 void launch_batch_stage(const BatchClass<T> *classes, int ncls, const StageArgs &a, int zchunk, cudaStream_t s,
-                        int64_t *launches);
+                        cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, int64_t *launches);
 template <typename T>
 void launch_batch_sample(const Blk<T> *blks, DevTime *const *times, int nshots, int cur, int w_stride,
                          cudaStream_t s, int64_t *launches);
