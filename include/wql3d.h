@@ -347,11 +347,16 @@ int wql3d_adjoint_reset(wql3d_domain *d);
 int wql3d_adjoint_step(wql3d_domain *d, int n, double dt);
 int wql3d_adjoint_add_receivers(wql3d_domain *d, int block, const double *res);
 /* The same reversal without recomputing the stage inputs: wql3d_record_step
-   runs time step n like wql3d_time_step (one-block FP64 domain) and copies its
-   five stage inputs F^(0..4) into dev_out (5 x wql3d_field_volume doubles on
-   the device); wql3d_adjoint_step_recorded reverses step n from such a record
-   (t_n: the time at the start of step n).  A driver records a checkpoint
-   segment once and reverses it from the records. */
+   runs time step n like wql3d_time_step (one-block FP64 domain) and records
+   into dev_out (WQL3D_RECORD_FIELDS x wql3d_field_volume doubles on the
+   device) its five stage inputs F^(0..4) and, for a curvilinear block, the
+   derivative terms of each stage input that the material gradient needs (the
+   stage kernel writes them as it computes them: strain rates and stress-flux
+   sums, 9 components); wql3d_adjoint_step_recorded reverses step n from such
+   a record (t_n: the time at the start of step n) without re-deriving them.
+   A driver records a checkpoint segment once and reverses it from the
+   records. */
+#define WQL3D_RECORD_FIELDS 10
 int wql3d_record_step(wql3d_domain *d, double dt, int n, int w_stride, double *dev_out);
 int wql3d_adjoint_step_recorded(wql3d_domain *d, int n, double dt, double t_n, const double *dev_in);
 /* L^T R and (dL/d(lambda, mu, rho) F)^T R at the current fields, host arrays

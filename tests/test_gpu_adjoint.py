@@ -130,3 +130,36 @@ def test_autograd_function_and_checkpoint_interval(wql3d_lib):
     gmat, gM = ref.backward(ref.forward() - observed)
     assert rel_l2(grads[0][0], gmat) < 1e-13
     ref.close()
+
+
+def test_gradient_over_shots_sums_the_shots(wql3d_lib):
+    """gradient_over_shots in one process: the misfit and material gradient
+    are the sums of the shots' own adjoint solves, the moment gradients each
+    shot's own (the reduction path of the multi-GPU gradient configuration,
+    whose all-reduce the gloo test covers)."""
+    import copy
+    from waveqlab3d_q_gpu_b200.adjoint import AdjointSolver, gradient_over_shots
+    from waveqlab3d_q_gpu_b200.problem import Source
+    N = 16
+    shots = []
+    for i, (x, y) in enumerate(((0.9, 1.1), (1.2, 0.8))):
+        p = _problem("curvilinear")
+        p.blocks[0].sources = [Source("ricker", 8.0, 0.1, 1.0, 0.8, 1.2, 0.3, -0.2, 0.1, x, y, 1.05)]
+        sol = AdjointSolver(p, N)
+        obs = 0.9 * sol.forward()
+        sol.close()
+        shots.append((p, obs))
+    mat = copy.deepcopy(shots[0][0].blocks[0].material) * 1.01
+    chi, g, gms = gradient_over_shots(shots, mat)
+    chi_sum, g_sum = 0.0, np.zeros_like(mat)
+    for (p, obs), gM_got in zip(shots, gms):
+        sol = AdjointSolver(p, N)
+        sol.set_parameters(material=mat)
+        res = sol.forward() - obs
+        gm, gM = sol.backward(res)
+        sol.close()
+        chi_sum += 0.5 * float(np.sum(res * res))
+        g_sum += gm
+        assert np.array_equal(gM_got, gM)
+    assert chi == chi_sum
+    assert np.array_equal(g, g_sum)

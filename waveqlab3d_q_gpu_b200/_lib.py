@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libwql3d.so")
 
 ABI_VERSION = 4
+RECORD_FIELDS = 10   # WQL3D_RECORD_FIELDS: field volumes per recorded step
 OK = 0
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENONFINITE", -5: "ESTATE"}
 

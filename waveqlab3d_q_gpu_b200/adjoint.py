@@ -13,21 +13,24 @@ Kennedy-Carpenter (5,4) low-storage update (``wql3d_adjoint_*`` in
 include/wql3d.h).
 
 Memory: sqrt(N)-step checkpointing with recomputation.  The forward run
-stores the fields every K = ceil(sqrt(N)) steps on the device; the reverse
-sweep restores each checkpoint, recomputes its K steps once while recording
-every step's five stage inputs into a device segment buffer
-(``wql3d_record_step``), and reverses those steps from the records
-(``wql3d_adjoint_step_recorded``).  Device storage is ceil(N/K) + 5 K field
-states instead of 5 N; the forward work is done twice.  With
-``record_stages=False`` the segment holds one state per step and every
-adjoint step recomputes its four inner stages (ceil(N/K) + K states, the
-forward work done almost three times).
+stores the fields every K steps on the device; the reverse sweep restores
+each checkpoint, recomputes its K steps once while recording every step's
+five stage inputs and, for a curvilinear block, their derivative terms
+(written by the stage kernel as it computes them) into a device segment
+buffer (``wql3d_record_step``), and reverses those steps from the records
+(``wql3d_adjoint_step_recorded``), so that the adjoint pass does not re-derive
+the stage inputs for the material gradient.  Device storage is ceil(N/K) + 10 K
+field states (K = ceil(sqrt(N / 10)) by default, the minimum) instead of 10 N;
+the forward work is done twice.  With ``record_stages=False`` the segment
+holds one state per step and every adjoint step recomputes its four inner
+stages (ceil(N/K) + K states, K = ceil(sqrt(N)), the forward work done
+almost three times).
 """
 from __future__ import annotations
 
 import ctypes as C
 import math
-from typing import Optional
+from typing import Optional, Sequence
 
 import numpy as np
 import torch
@@ -46,7 +49,12 @@ class AdjointSolver:
             raise ValueError("the adjoint covers one elastic block")
         self.problem = problem
         self.nsteps = int(nsteps)
-        self.K = int(checkpoint_every) if checkpoint_every else max(1, math.ceil(math.sqrt(self.nsteps)))
+        # storage is ceil(N / K) checkpoints + K recorded steps of `per` field
+        # volumes each: K = sqrt(N / per) minimises it (every step is still
+        # recomputed exactly once in the reverse sweep, whatever K)
+        per = _lib.RECORD_FIELDS if record_stages else 1
+        self.K = (int(checkpoint_every) if checkpoint_every
+                  else max(1, math.ceil(math.sqrt(self.nsteps / per))))
         self.dt = problem.dt()
         self.domain = Domain(problem, precision="fp64", max_samples=self.nsteps + 2)
         L = _lib.load()
@@ -59,7 +67,6 @@ class AdjointSolver:
         self.ckpt = torch.empty((self.nchk, ne.value), dtype=torch.float64, device="cuda")
         self.record = bool(record_stages)
         self.ne = ne.value
-        per = 5 if self.record else 1
         self.seg = torch.empty((self.K, per * ne.value), dtype=torch.float64, device="cuda")
         blk = problem.blocks[0]
         self.nrec = 0 if blk.receivers is None else len(blk.receivers)
@@ -167,3 +174,57 @@ class WaveformMisfit(torch.autograd.Function):
 def waveform_misfit(material: torch.Tensor, moment: torch.Tensor, solver: AdjointSolver,
                     observed: np.ndarray) -> torch.Tensor:
     return WaveformMisfit.apply(material, moment, solver, observed)
+
+
+def _solve_shot(problem: Problem, observed: np.ndarray, material: np.ndarray, checkpoint_every=None):
+    """chi, d chi / d(lambda, mu, rho), d chi / dM of one shot on this GPU."""
+    sol = AdjointSolver(problem, observed.shape[0], checkpoint_every)
+    try:
+        sol.set_parameters(material=material)
+        seis = sol.forward()
+        res = seis - observed
+        gmat, gM = sol.backward(res)
+        return 0.5 * float(np.sum(res * res)), gmat, gM
+    finally:
+        sol.close()
+
+
+def gradient_over_shots(shots: Sequence, material: np.ndarray, *, group=None, solve=None):
+    """Misfit and gradients summed over the shots of a gradient
+    configuration, the shots dealt round-robin to the ranks of a
+    torch.distributed process group (one GPU each): rank r solves shots r,
+    r + W, ...; then one all-reduce (SUM) over the group of [chi, the material
+    gradient field, the stacked per-shot moment-tensor gradients] (NCCL on
+    device buffers, or gloo on host buffers).  shots: (problem, observed)
+    pairs, observed (N, nrec, 3); material (3, ns, nr, nq).  Returns (chi,
+    gradient (3, ns, nr, nq), [per-shot (nsrc, 6)]), the same on every rank.
+    solve(problem, observed, material) -> (chi, gmat, gM) stands in for the
+    per-shot forward + adjoint (tests on hosts without a GPU)."""
+    solve = solve or _solve_shot
+    try:
+        import torch.distributed as dist
+        dist_on = dist.is_available() and dist.is_initialized()
+    except ImportError:
+        dist_on = False
+    rank = dist.get_rank(group) if dist_on else 0
+    world = dist.get_world_size(group) if dist_on else 1
+    nsrc = [len(p.blocks[0].sources) for p, _ in shots]
+    offs = np.concatenate([[0], np.cumsum([6 * k for k in nsrc])]).astype(int)
+    nmat = int(np.prod(material.shape))
+    flat = np.zeros(1 + nmat + int(offs[-1]))
+    for i, (p, obs) in enumerate(shots):
+        if i % world != rank:
+            continue
+        chi, gmat, gM = solve(p, obs, material)
+        flat[0] += chi
+        flat[1:1 + nmat] += np.asarray(gmat, dtype=np.float64).ravel()
+        flat[1 + nmat + offs[i]:1 + nmat + offs[i + 1]] = np.asarray(gM, dtype=np.float64).ravel()
+    if world > 1:
+        backend = dist.get_backend(group)
+        t = torch.from_numpy(flat)
+        if backend == "nccl":
+            t = t.cuda()
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        flat = t.cpu().numpy()
+    gms = [flat[1 + nmat + offs[i]:1 + nmat + offs[i + 1]].reshape(nsrc[i], 6) for i in range(len(shots))]
+    return float(flat[0]), flat[1:1 + nmat].reshape(material.shape), gms

@@ -43,16 +43,26 @@ static void launch_curv_fused(Blk<T> &b, const StageCtx &c, const StageArgs &a) 
   ++*c.launches;
 }
 
+// the lean kernels keep one PML slab per axis: blocks whose two slabs on an
+// axis overlap (2 npml > n) take the generic update
+template <typename T>
+static bool pml_overlap(const Blk<T> &b) {
+  const int nax[3] = {b.nx, b.ny, b.nz};
+  for (int ax = 0; ax < 3; ++ax)
+    if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) return true;
+  return false;
+}
+
+template <typename T>
+bool curv_stage_fused(const Blk<T> &b) {
+  return tuning().curv_fused && tuning().lean && !pml_overlap(b);
+}
+
 template <typename T>
 void launch_curv_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
   const long long npts = (long long)b.nx * b.ny * b.nz;
-  // the lean kernels keep one PML slab per axis: blocks whose two slabs on
-  // an axis overlap (2 npml > n) take the generic update
-  bool overlap = false;
-  const int nax[3] = {b.nx, b.ny, b.nz};
-  for (int ax = 0; ax < 3; ++ax)
-    if (b.pml_on[2 * ax] && b.pml_on[2 * ax + 1] && 2 * b.npml > nax[ax]) overlap = true;
-  if (tuning().curv_fused && tuning().lean && !overlap) {
+  const bool overlap = pml_overlap(b);
+  if (curv_stage_fused(b)) {
     launch_curv_fused<T>(b, c, a);
     return;
   }
@@ -101,6 +111,7 @@ void launch_curv_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
 }
 
 template void launch_curv_stage<WQL3D_REAL>(Blk<WQL3D_REAL> &, const StageCtx &, const StageArgs &);
+template bool curv_stage_fused<WQL3D_REAL>(const Blk<WQL3D_REAL> &);
 int WQL3D_CAT(upload_tables_curv_, WQL3D_TAG)(const ConstTables &t) { return upload_tables_here(t); }
 
 }  // namespace wql3d

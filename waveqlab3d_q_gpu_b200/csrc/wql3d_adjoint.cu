@@ -15,7 +15,7 @@ namespace {
 //   g_mu     += 2 (R_xx v_x,x + R_yy v_y,y + R_zz v_z,z) + R_xy (v_x,y + v_y,x) + ...
 //   g_rho    += -1 / (rho^2 J) sum_f R_{v_f} (flux sum)_f
 __global__ void __launch_bounds__(128, 3) k_adj_pre(Blk<double> b, AdjBlk A, double Bdt, double As,
-                                                    const double *__restrict__ Sprev) {
+                                                    const double *__restrict__ Sprev, const double *__restrict__ E) {
   int x, y, z;
   if (!flat_point(b, x, y, z)) return;
   const long long p = pidx(b, x, y, z);
@@ -50,14 +50,26 @@ __global__ void __launch_bounds__(128, 3) k_adj_pre(Blk<double> b, AdjBlk A, dou
 #pragma unroll
     for (int f = 0; f < 3; ++f) ZY[(3 + a * 3 + f) * V] = X0 * W[0][f] + X1 * W[1][f] + X2 * W[2][f];
   }
-  double U[9], S[9];
-  curv_derivs<double>(b, Sprev, x, y, z, p, U, S);
-  const double tr = U[0] + U[4] + U[8];
+  // derivative terms of the stage input: recorded by the forward pass, or
+  // recomputed (e: normal and shear strain rates, fs: stress-flux sums)
+  double e[6], fs[3];
+  if (E) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) e[c] = E[c * V + p];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) fs[c] = E[(6 + c) * V + p];
+  } else {
+    double U[9], S[9];
+    curv_derivs<double>(b, Sprev, x, y, z, p, U, S);
+    e[0] = U[0]; e[1] = U[4]; e[2] = U[8];
+    e[3] = U[3] + U[1]; e[4] = U[6] + U[2]; e[5] = U[7] + U[5];
+    fs[0] = S[0] + S[3] + S[6]; fs[1] = S[1] + S[4] + S[7]; fs[2] = S[2] + S[5] + S[8];
+  }
+  const double tr = e[0] + e[1] + e[2];
   double *g = A.g + p;
   g[0] += (R[3] + R[4] + R[5]) * tr;
-  g[V] += 2.0 * (R[3] * U[0] + R[4] * U[4] + R[5] * U[8]) + R[6] * (U[3] + U[1]) + R[7] * (U[6] + U[2]) +
-          R[8] * (U[7] + U[5]);
-  g[2 * V] += -a1 / rho * (R[0] * (S[0] + S[3] + S[6]) + R[1] * (S[1] + S[4] + S[7]) + R[2] * (S[2] + S[5] + S[8]));
+  g[V] += 2.0 * (R[3] * e[0] + R[4] * e[1] + R[5] * e[2]) + R[6] * e[3] + R[7] * e[4] + R[8] * e[5];
+  g[2 * V] += -a1 / rho * (R[0] * fs[0] + R[1] * fs[1] + R[2] * fs[2]);
 }
 
 // Gather pass: Fbar_v += sum_a (1/h_a) D_a^T Y_a, Fbar_sigma += J sum_a X_a (1/h_a) D_a^T Z
@@ -237,7 +249,7 @@ void adj_launch_stage(const Blk<double> &b, const AdjBlk &A, int stage, double B
                       int64_t *launches) {
   const long long npts = (long long)b.nx * b.ny * b.nz;
   const unsigned gr = (unsigned)((npts + 127) / 128);
-  k_adj_pre<<<gr, 128, 0, s>>>(b, A, Bdt, A_s, A.S[stage - 1]);
+  k_adj_pre<<<gr, 128, 0, s>>>(b, A, Bdt, A_s, A.S[stage - 1], A.E[stage - 1]);
   ++*launches;
   for (int f = 0; f < 6; ++f) {
     if (b.bc[f] <= 0) continue;

@@ -34,6 +34,7 @@ struct AdjBlk {
   double *g;              // material gradient: lambda, mu, rho (3 comps)
   double *gM;             // moment-tensor gradient, nsrc x 6 (mxx myy mzz mxy mxz myz)
   double *S[5];           // stage inputs F^(0..4) of the step being reversed (9 comps each)
+  const double *E[5];     // their derivative terms recorded by k_curv_fused (StageArgs::rec), or null
   const int *toff[3];     // transposed derivative rows per axis: [n][ADJ_TW] offsets
   const double *tc[3];    // ... and coefficients (0 pads)
   const double *res;      // receiver residuals of one sample, nrec x 3

@@ -965,10 +965,11 @@ void launch_stage(wql3d_domain *d, int bi, const StageArgs &a, bool fused = fals
 }
 
 template <typename T>
-int enqueue_stage(wql3d_domain *d, int stage, double dt, int flags) {
+int enqueue_stage(wql3d_domain *d, int stage, double dt, int flags, void *rec = nullptr) {
   StageArgs a;
   a.cur = d->cur;
   a.flags = flags;
+  a.rec = rec;
   a.stage = stage;
   a.A = kRkA[stage - 1];
   a.Bdt = kRkB[stage - 1] * dt;
@@ -1722,6 +1723,13 @@ void transposed_rows(int n, int lit, std::vector<int> &off, std::vector<double> 
   }
 }
 
+// recorded steps carry the stage inputs' derivative terms when the block's
+// stages run the fused curvilinear kernel (the Cartesian kernels do not write
+// them; the adjoint then recomputes them)
+bool record_terms(wql3d_domain *d) {
+  return d->hb[0].mesh == WQL3D_MESH_CURVILINEAR && !tuning().generic && curv_stage_fused(d->bd[0]);
+}
+
 int adjoint_supported(wql3d_domain *d) {
   if (d->fp32 || d->nblocks != 1 || d->response != WQL3D_ELASTIC || d->slab || d->desc.remote_side || d->desc.mms)
     return fail(WQL3D_EINVAL, "the adjoint covers one FP64 elastic block (no interface, slab or MMS)");
@@ -1825,10 +1833,13 @@ int wql3d_record_step(wql3d_domain *d, double dt, int n, int w_stride, double *d
   h.n = n;
   CK(cudaMemcpyAsync(d->time, &h, sizeof(h), cudaMemcpyHostToDevice, d->stream));
   if (int rc = enqueue_sample<double>(d, w_stride)) return rc;
+  // stage inputs, then (blocks on the fused curvilinear kernel) the stage
+  // inputs' derivative terms written by the stage kernel itself
+  const bool terms = record_terms(d);
   for (int s = 1; s <= 5; ++s) {
     CK(cudaMemcpyAsync(dev_out + (s - 1) * ne, d->cur ? b.F1 : b.F0, sizeof(double) * ne, cudaMemcpyDeviceToDevice,
                        d->stream));
-    if (int rc = enqueue_stage<double>(d, s, dt, F_ALL)) return rc;
+    if (int rc = enqueue_stage<double>(d, s, dt, F_ALL, terms ? (void *)(dev_out + (4 + s) * ne) : nullptr)) return rc;
   }
   k_advance<<<1, 32, 0, d->stream>>>(d->time, dt);
   d->launches++;
@@ -1843,7 +1854,11 @@ int wql3d_adjoint_step_recorded(wql3d_domain *d, int n, double dt, double t_n, c
   Blk<double> &b = d->bd[0];
   AdjBlk A = d->adj;
   const size_t ne = (size_t)9 * b.vol;
-  for (int s = 0; s < 5; ++s) A.S[s] = const_cast<double *>(dev_in) + s * ne;
+  const bool terms = record_terms(d);
+  for (int s = 0; s < 5; ++s) {
+    A.S[s] = const_cast<double *>(dev_in) + s * ne;
+    A.E[s] = terms ? dev_in + (5 + s) * ne : nullptr;
+  }
   for (int s = 5; s >= 1; --s) {
     adj_launch_stage(b, A, s, kRkB[s - 1] * dt, kRkA[s - 1], d->stream, &d->launches);
     adj_launch_moment(b, A, t_n + kRkC[s - 1] * dt, d->stream, &d->launches);

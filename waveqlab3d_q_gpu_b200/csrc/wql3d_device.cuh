@@ -149,6 +149,11 @@ struct StageArgs {
   double A, Bdt, dt;
   const DevTime *time;
   int pf = 0;           // k_curv_fused: 1 = L2 prefetch of the memory variables on entry
+  // k_curv_fused: when set, every point writes the derivative terms of the
+  // stage input the adjoint's material gradient needs (9 components, field
+  // layout): e = (U0, U4, U8, U3 + U1, U6 + U2, U7 + U5) and the stress-flux
+  // sums (S0 + S3 + S6, S1 + S4 + S7, S2 + S5 + S8)
+  void *rec = nullptr;
 };
 
 template <typename T>
@@ -1883,6 +1888,12 @@ __global__ void __launch_bounds__(128, MINB) k_curv_fused(Blk<T> b, StageArgs a)
   const bool in_pml = sx.in() || sy.in() || sz.in();
   T U[9], S[9];
   if (rhs) curv_derivs<T>(b, F, x, y, z, p, U, S);
+  if (rhs && a.rec) {
+    T *E = reinterpret_cast<T *>(a.rec) + p;
+    E[0] = U[0]; E[V] = U[4]; E[2 * V] = U[8];
+    E[3 * V] = U[3] + U[1]; E[4 * V] = U[6] + U[2]; E[5 * V] = U[7] + U[5];
+    E[6 * V] = S[0] + S[3] + S[6]; E[7 * V] = S[1] + S[4] + S[7]; E[8 * V] = S[2] + S[5] + S[8];
+  }
   T df[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) {

@@ -80,6 +80,10 @@ void launch_cart_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a);
 // curvilinear split stage: derivative pass, memory variables, face SATs, point update
 template <typename T>
 void launch_curv_stage(Blk<T> &b, const StageCtx &c, const StageArgs &a);
+// true when the block's full curvilinear stages run k_curv_fused (which can
+// record the adjoint's derivative terms, StageArgs::rec)
+template <typename T>
+bool curv_stage_fused(const Blk<T> &b);
 // generic per-point kernel (any flags, MMS, both meshes)
 template <typename T>
 void launch_generic_stage(Blk<T> &b, int mesh, const StageCtx &c, const StageArgs &a);
