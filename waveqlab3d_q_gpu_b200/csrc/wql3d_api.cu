@@ -180,6 +180,9 @@ struct wql3d_domain {
   // plane extraction (wql3d_get_plane): largest plane x 9 components
   double *plane = nullptr;
   long long plane_cap = 0;
+  // host <-> device staging: 9 components of the largest block with 3 ghost layers
+  double *xfer = nullptr;
+  long long xfer_cap = 0;
 };
 
 namespace {
@@ -241,10 +244,64 @@ int copy_component(wql3d_domain *d, const HostBlock &h, void *dev, size_t esz, v
   return WQL3D_OK;
 }
 
+// Host arrays move through a contiguous device staging buffer: one copy of
+// up to 9 components at the link's full rate, then a kernel that scatters
+// them into (or gathers them from) the padded device layout, converting to
+// the storage precision on the device.  (A 3-D strided copy moves one host
+// row, a few hundred bytes, per DMA transfer.)
+struct XferGeom {
+  int nq, nr, ns, hnb;          // interior extents and the host array's ghost width
+  long long PX, PY, XOFF, NBZ;  // padded device layout: x pitch, y pitch, x / y-z offsets
+  long long vol;                // device component stride
+};
+
+template <typename T>
+__global__ void k_xfer(XferGeom g, double *stage, T *dev, int nc, int to_dev) {
+  const long long hq = g.nq + 2 * g.hnb, hr = g.nr + 2 * g.hnb, hs = g.ns + 2 * g.hnb;
+  const long long hn = hq * hr * hs;
+  const long long n = (long long)g.nq * g.nr * g.ns;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * nc;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long c = i / n, k = i - c * n;
+    const long long x = k % g.nq, y = (k / g.nq) % g.nr, z = k / ((long long)g.nq * g.nr);
+    const long long hi = c * hn + (x + g.hnb) + hq * ((y + g.hnb) + hr * (z + g.hnb));
+    const long long di = c * g.vol + (g.XOFF + x) + g.PX * ((g.NBZ + y) + g.PY * (g.NBZ + z));
+    if (to_dev) dev[di] = (T)stage[hi];
+    else stage[hi] = (double)dev[di];
+  }
+}
+
+template <typename T>
+int xfer_array(wql3d_domain *d, const HostBlock &h, T *dev, int ncomp, double *host, int hnb, bool to_dev) {
+  const long long hn = (long long)(h.nq + 2 * hnb) * (h.nr + 2 * hnb) * (h.ns + 2 * hnb);
+  XferGeom g{h.nq, h.nr, h.ns, hnb, h.PX, h.PY, h.XOFF, NB, h.vol};
+  for (int c0 = 0; c0 < ncomp; c0 += 9) {
+    const int nc = std::min(9, ncomp - c0);
+    const size_t bytes = sizeof(double) * (size_t)(hn * nc);
+    double *hp = host + (long long)c0 * hn;
+    const long long n = (long long)h.nq * h.nr * h.ns * nc;
+    const unsigned gr = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 32);
+    if (to_dev) {
+      CK(cudaMemcpyAsync(d->xfer, hp, bytes, cudaMemcpyHostToDevice, d->stream));
+      k_xfer<T><<<gr, 256, 0, d->stream>>>(g, d->xfer, dev + (long long)c0 * h.vol, nc, 1);
+    } else {
+      if (hnb > 0) CK(cudaMemsetAsync(d->xfer, 0, bytes, d->stream));
+      k_xfer<T><<<gr, 256, 0, d->stream>>>(g, d->xfer, const_cast<T *>(dev) + (long long)c0 * h.vol, nc, 0);
+      CK(cudaMemcpyAsync(hp, d->xfer, bytes, cudaMemcpyDeviceToHost, d->stream));
+    }
+    CK(cudaGetLastError());
+    // the staging buffer is reused by the next chunk and the host data must
+    // be complete (or consumed) on return
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  return WQL3D_OK;
+}
+
 // double host data -> device storage type (FP32 path converts on the host)
 template <typename T>
 int put_array(wql3d_domain *d, const HostBlock &h, T *dev, int ncomp, const double *host, int hnb) {
   long long hn = (long long)(h.nq + 2 * hnb) * (h.nr + 2 * hnb) * (h.ns + 2 * hnb);
+  if (d->xfer && hn * 9 <= d->xfer_cap) return xfer_array<T>(d, h, dev, ncomp, const_cast<double *>(host), hnb, true);
   for (int c = 0; c < ncomp; ++c) {
     const double *src = host + (long long)c * hn;
     if (sizeof(T) == sizeof(double)) {
@@ -264,6 +321,7 @@ int put_array(wql3d_domain *d, const HostBlock &h, T *dev, int ncomp, const doub
 template <typename T>
 int get_array(wql3d_domain *d, const HostBlock &h, const T *dev, int ncomp, double *host, int hnb) {
   long long hn = (long long)(h.nq + 2 * hnb) * (h.nr + 2 * hnb) * (h.ns + 2 * hnb);
+  if (d->xfer && hn * 9 <= d->xfer_cap) return xfer_array<T>(d, h, const_cast<T *>(dev), ncomp, host, hnb, false);
   for (int c = 0; c < ncomp; ++c) {
     double *dst = host + (long long)c * hn;
     if (sizeof(T) == sizeof(double)) {
@@ -1168,6 +1226,12 @@ int wql3d_domain_create(const wql3d_domain_desc *desc, wql3d_domain **out) {
   }
   if (d->mem.get(&d->plane, (size_t)d->plane_cap, false) != cudaSuccess)
     return cleanup(fail(WQL3D_ENOMEM, "plane buffer"));
+  for (int i = 0; i < desc->nblocks; ++i) {
+    const long long nq = desc->block[i].nq + 6, nr = desc->block[i].nr + 6, ns = desc->block[i].ns + 6;
+    d->xfer_cap = std::max(d->xfer_cap, 9 * nq * nr * ns);
+  }
+  if (d->mem.get(&d->xfer, (size_t)d->xfer_cap, false) != cudaSuccess)
+    return cleanup(fail(WQL3D_ENOMEM, "transfer staging buffer"));
   for (int i = 0; i < desc->nblocks; ++i) {
     const int fd = desc->block[i].fd_operator;
     if (fd < WQL3D_FD_TRADITIONAL6 || fd > WQL3D_FD_UPWIND_DRP6)
