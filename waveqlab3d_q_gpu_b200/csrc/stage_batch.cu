@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(128, 3) k_batch_shell(BatchClass<T> C, StageAr
   shell_decode(sb, (int)idx, x, y, z);
   StageArgs la = a;
   la.time = C.times[s_shot];
-  point_update<T, MESH_CART, RESP, SEP>(sb, la, x, y, z);
+  point_update<T, MESH_CART, RESP, SEP, false, true>(sb, la, x, y, z);
 }
 
 // stage-1 station samples of every shot: one CTA per shot
