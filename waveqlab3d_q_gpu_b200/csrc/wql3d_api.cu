@@ -2031,6 +2031,7 @@ int wql3d_check_status(wql3d_domain *d, int32_t *bad_step) {
   CK(cudaStreamSynchronize(d->stream));
   CK(cudaGetLastError());
   if (bad_step) *bad_step = h.bad;
+  if (h.stall) return fail(WQL3D_ECUDA, "a bounded wait in a stage kernel gave up: the fields are void");
   if (h.bad) return fail(WQL3D_ENONFINITE, "non-finite station value at step " + std::to_string(h.bad) +
                                                 " (RUN-STATION-001)");
   return WQL3D_OK;

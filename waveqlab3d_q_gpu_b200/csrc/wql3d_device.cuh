@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace wql3d {
@@ -61,7 +62,7 @@ struct DevTime {
   int n;           // current step number (1-based)
   int nsamp;       // receiver samples taken
   int bad;         // first step whose station sample held a non-finite value (0: none)
-  int pad;
+  int stall;       // nonzero: a bounded wait in a stage kernel gave up (the stage's results are void)
 };
 
 template <typename T>
@@ -182,6 +183,49 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gsrc, bool 
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
+// Tensor-memory-accelerator (TMA) tile loads, cp.async.bulk.tensor, completing
+// on an mbarrier in shared memory.  No cluster multicast: every tensor map
+// covers this GPU's own field arrays.  Rules the callers keep: the innermost
+// coordinate times the element size is a multiple of 16 bytes, the shared
+// destination is 128-byte aligned, and every wait is bounded.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// makes the initialised barriers visible to the async (TMA) proxy
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// the calling thread's arrival, announcing `bytes` of transfers to come
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// wait for phase `parity` of a barrier, giving up after `limit` polls
+// (each poll may suspend the thread for a while); false when it gave up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int limit) {
+  for (int k = 0; k < limit; ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// one box of a 4-D tensor map (coordinates innermost first) into shared memory
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
+}
 
 // central (interior) SBP row at 1-based i of n points on axis a: 7 <= i <= n-6,
 // or up to an open face of a slab
@@ -2085,32 +2129,53 @@ __global__ void __launch_bounds__(128, 3) k_shell(Blk<T> b, StageArgs a, int cou
 // nine outputs of a point are split: warps of group V (velocity rates)
 // need z-derivatives of s_xz, s_yz, s_zz, warps of group S (stress rates) of
 // v_x, v_y, v_z, so each thread's seven-plane z-queue is three fields and
-// lives in registers.  Shared memory holds only the double-buffered haloed
-// x-y plane, filled one plane ahead with 16-byte cp.async.
+// lives in registers.  Shared memory holds the double-buffered haloed x-y
+// plane of eight fields, filled one plane ahead either by the tensor memory
+// accelerator (TMA = true: one thread issues eight 4-D box loads of W x H
+// points, x, y, z, component, completing on the buffer's mbarrier) or by
+// 16-byte cp.async from every thread.
 // ---------------------------------------------------------------------------
-template <typename T, int TY>
+// smallest width >= w (a multiple of vec) whose h-row field plane is a whole
+// number of 128-byte lines, so that every field's plane can be a TMA destination
+constexpr int tma_plane_width(int w, int h, int esz, int vec) {
+  while ((h * w * esz) % 128) w += vec;
+  return w;
+}
+
+template <typename T, int TY, int NBUF = 2>
 struct SplitSmem {
   static constexpr int VEC = 16 / (int)sizeof(T);
-  static constexpr int W = ((38 + VEC - 1 + VEC - 1) / VEC) * VEC;
-  static constexpr int H = TY + 6, NP = 32 * TY, CH = W / VEC;
+  static constexpr int H = TY + 6, NP = 32 * TY;
+  static constexpr int W = tma_plane_width(((38 + VEC - 1 + VEC - 1) / VEC) * VEC, H, (int)sizeof(T), VEC);
+  static constexpr int CH = W / VEC;
   static constexpr size_t plane_elems = (size_t)8 * H * W;
-  // after the two planes: the strain rates of the tile's points (6 x NP) and
-  // the velocity group's memory-variable sums (3 x NP), anelastic blocks
-  static constexpr size_t bytes = sizeof(T) * (2 * plane_elems + 9 * (size_t)NP);
+  // after the NBUF planes: the strain rates of the tile's points (6 x NP) and
+  // the velocity group's memory-variable sums (3 x NP), anelastic blocks;
+  // then the planes' mbarriers (TMA fills)
+  static constexpr size_t bar_off = sizeof(T) * (NBUF * plane_elems + 9 * (size_t)NP);
+  static constexpr size_t bytes = bar_off + NBUF * sizeof(uint64_t);
 };
 
+// polls of a TMA plane wait before the tile gives up (about a second)
+constexpr int kTmaWaitLimit = 1 << 20;
+
 // one 32 x TY column tile (tile indices bx, by, bz) of the strict interior;
-// smraw is the planes' dynamic shared memory
-template <typename T, int RESP, int TY>
+// smraw is the planes' dynamic shared memory (1024-byte aligned for TMA);
+// tm: the tensor map of the field buffer the stencil reads (TMA = true);
+// NBUF plane buffers (cp.async: 2, filled one plane ahead; TMA: filled
+// NBUF - 1 planes ahead)
+template <typename T, int RESP, int TY, bool TMA = false, int NBUF = 2>
 __device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const StageArgs &a, int zchunk, int bx, int by,
-                                                    int bz, unsigned char *smraw) {
-  using SM = SplitSmem<T, TY>;
+                                                    int bz, unsigned char *smraw, const CUtensorMap *tm = nullptr) {
+  static_assert(TMA || NBUF == 2, "cp.async fills use two plane buffers");
+  using SM = SplitSmem<T, TY, NBUF>;
   constexpr int W = SM::W, H = SM::H, NP = SM::NP, VEC = SM::VEC, CH = SM::CH;
   constexpr int NT = 2 * NP;                                 // threads per block
   constexpr int NPOS = H * CH, PPT = (NPOS + NT - 1) / NT;
   T (*S)[8][H][W] = reinterpret_cast<T (*)[8][H][W]>(smraw);
-  T *eb = reinterpret_cast<T *>(smraw) + 2 * SM::plane_elems;   // strain rates, 6 x NP
+  T *eb = reinterpret_cast<T *>(smraw) + NBUF * SM::plane_elems;   // strain rates, 6 x NP
   T *sb = eb + 6 * NP;                                           // memory-variable sums 3-5, 3 x NP
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smraw + SM::bar_off);
   const int tid = threadIdx.x;
   const bool gS = tid >= NP;                                 // stress-rate group
   const int lt = gS ? tid - NP : tid;
@@ -2144,15 +2209,40 @@ __device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const Stage
     long long inrow = base0 - rowstart0 + (long long)ch * VEC;
     gok[k] = pos < NPOS && (y0 - 3 + yy) <= b.ny + 3 && inrow + VEC <= b.sy;
   }
+  bool stalled = false;
+  if constexpr (TMA) {
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < NBUF; ++k) mbar_init(&bars[k], 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
   auto fill = [&](int zz, int buf) {
     const long long plane0 = base0 + (long long)(zz - zs) * b.sz;
     T *dst = &S[buf][0][0][0];
+    if constexpr (TMA) {
+      // box origin (x, y, z, component) of the plane in the padded array;
+      // base0 is 16-byte aligned and the row / plane pitches are multiples of
+      // 128 bytes, so x is too; a violated rule issues no copy and the
+      // bounded wait records the stall
+      if (tid == 0) {
+        const long long rem = plane0 % b.sz;
+        const int cx = (int)(rem % b.sy), cy = (int)(rem / b.sy), cz = (int)(plane0 / b.sz);
+        if ((cx % VEC) == 0 && (smem_u32(dst) & 127u) == 0) {
+          mbar_expect_tx(&bars[buf], (unsigned)(8 * H * W * sizeof(T)));
 #pragma unroll
-    for (int f = 0; f < 8; ++f) {
-      const T *srcf = F + c_smf[f] * V + plane0;
+          for (int f = 0; f < 8; ++f) tma_load_4d(dst + f * H * W, tm, cx, cy, cz, c_smf[f], &bars[buf]);
+        }
+      }
+    } else {
 #pragma unroll
-      for (int k = 0; k < PPT; ++k)
-        if (tid + k * NT < NPOS) cp_async<16>(dst + f * H * W + soff[k], gok[k] ? srcf + goff[k] : F, gok[k]);
+      for (int f = 0; f < 8; ++f) {
+        const T *srcf = F + c_smf[f] * V + plane0;
+#pragma unroll
+        for (int k = 0; k < PPT; ++k)
+          if (tid + k * NT < NPOS) cp_async<16>(dst + f * H * W + soff[k], gok[k] ? srcf + goff[k] : F, gok[k]);
+      }
     }
   };
   // z-queue fields: group V -> s_zz, s_xz, s_yz (F 5, 7, 8); group S -> v_x, v_y, v_z (F 0, 1, 2)
@@ -2169,7 +2259,13 @@ __device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const Stage
   q[1][6] = ld(F + q1 * V + pc + 3 * b.sz);
   q[2][6] = ld(F + q2 * V + pc + 3 * b.sz);
   fill(zs, 0);
-  cp_async_commit();
+  if constexpr (TMA) {
+#pragma unroll
+    for (int k = 1; k < NBUF - 1; ++k)
+      if (zs + k <= ze) fill(zs + k, k);
+  } else {
+    cp_async_commit();
+  }
   // this group's rates and material, one step ahead
   const int nd = gS ? 6 : 3, d0 = gS ? 3 : 0;
   // FP32 (compensated) path: the update's global operands -- the compensation
@@ -2196,12 +2292,23 @@ __device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const Stage
 
   for (int z = zs; z <= ze; ++z) {
     const int i = z - zs;
-    const int buf = i & 1;
+    const int buf = TMA ? i % NBUF : (i & 1);
     const long long p = pc + (long long)i * b.sz;
-    cp_async_wait_all();
+    if constexpr (TMA) {
+      // the plane of this iteration: buffer buf's (i / NBUF)-th fill (after a
+      // wait that gave up, the tile no longer waits)
+      if (!stalled && !mbar_wait_bounded(&bars[buf], (unsigned)((i / NBUF) & 1), kTmaWaitLimit)) stalled = true;
+    } else {
+      cp_async_wait_all();
+    }
     __syncthreads();
-    if (z + 1 <= ze) fill(z + 1, buf ^ 1);
-    cp_async_commit();
+    if constexpr (TMA) {
+      // the buffer of iteration i - 1, which every thread has left
+      if (z + NBUF - 1 <= ze) fill(z + NBUF - 1, (i + NBUF - 1) % NBUF);
+    } else {
+      if (z + 1 <= ze) fill(z + 1, buf ^ 1);
+      cp_async_commit();
+    }
     T qn0 = 0, qn1 = 0, qn2 = 0, dfn[6], mn0 = 0, mn1 = 0, fcn[NPRE], szn = 0;
     if (z + 1 <= ze) {
       const long long pn = p + 4 * b.sz;
@@ -2370,13 +2477,15 @@ __device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const Stage
     }
     m0 = mn0; m1 = mn1;
   }
-  cp_async_wait_all();
+  if constexpr (!TMA) cp_async_wait_all();
+  if (stalled && a.time) atomicOr(const_cast<int *>(&a.time->stall), 1);
 }
 
-template <typename T, int RESP, int TY>
-__global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1)) k_interior_split(Blk<T> b, StageArgs a, int zchunk) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  interior_split_tile<T, RESP, TY>(b, a, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
+template <typename T, int RESP, int TY, bool TMA, int NBUF>
+__global__ void __launch_bounds__(64 * TY, (TY == 4 ? 2 : 1))
+    k_interior_split(Blk<T> b, StageArgs a, int zchunk, const __grid_constant__ CUtensorMap tm) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  interior_split_tile<T, RESP, TY, TMA, NBUF>(b, a, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smraw, &tm);
 }
 
 // F <- F + dt*DF over every interior point (update_fields, split path): in place

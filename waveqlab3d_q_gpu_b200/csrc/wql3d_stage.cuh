@@ -44,6 +44,7 @@ struct Tuning {
   int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default), 2 or 4 in FP64; 4 (default), 5 or 6 in FP32
   int mvpf = -1;      // k_curv_fused: L2 prefetch of the memory variables on entry (-1: FP32 only)
   int overlap = 1;    // Cartesian stage: shell on the side stream, concurrent with the interior
+  int tma = 0;        // Cartesian interior: 1 = planes filled by TMA box loads (default: cp.async, measured faster)
 };
 
 inline Tuning tuning() {
@@ -53,6 +54,7 @@ inline Tuning tuning() {
     if (const char *e = getenv("WQL3D_FUSED_MINB")) r.fused_minb = atoi(e);
     if (const char *e = getenv("WQL3D_MV_PREFETCH")) r.mvpf = atoi(e);
     if (const char *e = getenv("WQL3D_SHELL_OVERLAP")) r.overlap = atoi(e);
+    if (const char *e = getenv("WQL3D_TMA")) r.tma = atoi(e);
     if (const char *e = getenv("WQL3D_KERNEL")) {
       r.generic = strcmp(e, "generic") == 0;
       if (strcmp(e, "curv_generic_update") == 0) r.lean = 0;
