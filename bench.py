@@ -207,15 +207,38 @@ def oracle_steps(problem, steps, warmup, budget_s):
     return npts * n / el / 1e9, n, el, int(os.environ["OMP_NUM_THREADS"])
 
 
+STEPS_OF_CONFIG = {"hill": 1500, "cartesian": 500, "planar": 2000}
+
+
+def workload_config(args, name, npts, nblocks, world):
+    """The line's ``config``: what the workload is and how it is spread over the
+    N processes, identical in both arms (the timing details sit outside it)."""
+    if world > 1 and world % 2 == 0 and args.workload == "hill":
+        return {"workload": name, "points_per_copy": npts, "copies": world // 2,
+                "parallelism": f"blocks2x{world // 2}", "backend": args.dist_backend,
+                "exchange": "interface face trace every RK stage, NCCL send/recv into the library's receive buffer"}
+    return {"workload": name, "points": npts, "blocks": nblocks, "rk_stages_per_step": 5,
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (126 MB) at every step"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     p, name = make_problem(args, max(args.steps, 1), cpu_sample=True)
+    if args.workload == "planar":
+        # the configuration is the full-size one (two blocks of n/2 x n x 3n/4);
+        # the CPU times its 128 x 128 x 96 instance
+        n = args.n or 512
+        cfg = workload_config(args, f"planar-fault-2block-{n}x{n}x{3 * n // 4}-fq8-vonkarman-slipweakening",
+                              n * n * (3 * n // 4), 2, world)
+    else:
+        cfg = workload_config(args, name, sum(b.npoints for b in p.blocks), len(p.blocks), world)
     value, n, el, cores = oracle_steps(p, args.steps, min(args.warmup, 1), 150.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n,
         "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": name},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{n} RK time steps of the workload in {el:.1f} s (CPU restatement of the "
                                    f"reference solver, OpenMP over z; the Fortran reference needs gfortran + MPI, "
@@ -388,10 +411,9 @@ def main():
             "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": r64["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": name, "points": npts, "blocks": nb, "rk_stages_per_step": 5,
-                       "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (%.1f GB on the device per precision run)" % (r64["bytes"] / 1e9),
-                       "timed_steps_of_run": f"{K} of the configuration's 1500"},
+            "config": workload_config(args, name, npts, nb, world),
+            "device_bytes": r64["bytes"],
+            "timed_steps_of_run": f"{K} of the configuration's {STEPS_OF_CONFIG.get(args.workload, '?')}",
             "e2e": e2e,
             "gpu_launches": r64["launches"],
             "roofline": {"bound": "hbm", "achieved": r64["achieved"], "peak": peak, "unit": "GB/s",
@@ -479,10 +501,7 @@ def pairs_main(args, rank, world, local, barrier, max_over_ranks, p, name):
         line = {"metric": METRIC, "value": copies * npts * K / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
                 "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": name, "points_per_copy": npts, "copies": copies,
-                           "parallelism": f"blocks2x{copies}", "backend": args.dist_backend,
-                           "exchange": "interface face trace every RK stage, NCCL send/recv into the library's "
-                                       "receive buffer"},
+                "config": workload_config(args, name, npts, len(p.blocks), world),
                 "e2e": {"value": copies * npts * K / e2e_s / 1e9, "unit": UNIT,
                         "h2d_bytes_per_step": world * host.nbytes / K,
                         "d2h_bytes_per_step": world * (host.nbytes + seis.nbytes) / K,
