@@ -290,8 +290,10 @@ int wql3d_get_seismograms(wql3d_domain *d, int block, double *out, int32_t *nsam
 int wql3d_reset_samples(wql3d_domain *d);
 /* run status: waits for the domain's queued work and returns WQL3D_ENONFINITE
    when a station sample of any step so far held a non-finite value (the
-   reference stops such a run, src/seismogram.f90:516-524, RUN-STATION-001);
-   bad_step (optional) receives the first such step, 0 if none */
+   reference stops such a run, src/seismogram.f90:516-524, RUN-STATION-001),
+   and WQL3D_ECUDA when a bounded device wait of a stage kernel gave up (the
+   fields are then void); bad_step (optional) receives the first non-finite
+   step, 0 if none */
 int wql3d_check_status(wql3d_domain *d, int32_t *bad_step);
 int wql3d_receiver_index(wql3d_domain *d, int block, int32_t *idx);
 

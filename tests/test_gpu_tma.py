@@ -56,3 +56,36 @@ def test_tma_planes_equal_cp_async_planes(wql3d_lib, tmp_path, response, prec):
     for k in a.files:
         assert np.array_equal(a[k], b[k]), (k, np.abs(a[k] - b[k]).max())
     assert np.abs(a["F"]).max() > 0.0
+
+
+STALL = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+from cases import small_case
+from waveqlab3d_q_gpu_b200.domain import Domain
+from waveqlab3d_q_gpu_b200._lib import Wql3dError
+p = small_case(mesh="cartesian", response="elastic", n=(45, 31, 29))
+g = Domain(p, nsteps_hint=2)
+g.time_step_RK()
+try:
+    g.check_status()
+    print("NO-STALL")
+except Wql3dError as e:
+    print("STALL", e)
+F = g.fields(0)
+print("READ", F.shape)
+g.close()
+"""
+
+
+def test_tma_wait_limit_reports_stall(wql3d_lib):
+    """WQL3D_TMA=2 issues no copies: every plane wait runs out (bounded, about a
+    second per tile), the tile carries on, the domain status reports the stall
+    and the context stays usable."""
+    env = dict(os.environ)
+    env["WQL3D_TMA"] = "2"
+    env["PYTHONPATH"] = os.path.dirname(ROOT) + os.pathsep + env.get("PYTHONPATH", "")
+    r = subprocess.run([sys.executable, "-c", STALL, ROOT], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert "STALL" in r.stdout and "bounded wait" in r.stdout, r.stdout
+    assert "READ (9, 29, 31, 45)" in r.stdout, r.stdout

@@ -53,8 +53,10 @@ static void launch_interior(Blk<T> &b, const StageCtx &c, const StageArgs &a) {
   memset(&tm, 0, sizeof(tm));
   if (tuning().tma && plane_tensor_map<T>(b, a.cur ? b.F1 : b.F0, &tm)) {
     const size_t sm = SplitSmem<T, 4>::bytes;
+    StageArgs ta = a;
+    ta.nofill = tuning().tma == 2;
     cudaFuncSetAttribute(k_interior_split<T, RESP, 4, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_interior_split<T, RESP, 4, true, 2><<<gr, 256, sm, c.stream>>>(b, a, zchunk, tm);
+    k_interior_split<T, RESP, 4, true, 2><<<gr, 256, sm, c.stream>>>(b, ta, zchunk, tm);
   } else {
     const size_t sm = SplitSmem<T, 4>::bytes;
     cudaFuncSetAttribute(k_interior_split<T, RESP, 4, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

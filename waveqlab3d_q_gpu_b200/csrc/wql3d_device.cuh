@@ -155,6 +155,9 @@ struct StageArgs {
   // layout): e = (U0, U4, U8, U3 + U1, U6 + U2, U7 + U5) and the stress-flux
   // sums (S0 + S3 + S6, S1 + S4 + S7, S2 + S5 + S8)
   void *rec = nullptr;
+  // Cartesian interior, TMA fills: 1 = issue no copies (test of the bounded
+  // plane waits: they run out and the domain status reports the stall)
+  int nofill = 0;
 };
 
 template <typename T>
@@ -2229,7 +2232,7 @@ __device__ __forceinline__ void interior_split_tile(const Blk<T> &b, const Stage
       if (tid == 0) {
         const long long rem = plane0 % b.sz;
         const int cx = (int)(rem % b.sy), cy = (int)(rem / b.sy), cz = (int)(plane0 / b.sz);
-        if ((cx % VEC) == 0 && (smem_u32(dst) & 127u) == 0) {
+        if ((cx % VEC) == 0 && (smem_u32(dst) & 127u) == 0 && !a.nofill) {
           mbar_expect_tx(&bars[buf], (unsigned)(8 * H * W * sizeof(T)));
 #pragma unroll
           for (int f = 0; f < 8; ++f) tma_load_4d(dst + f * H * W, tm, cx, cy, cz, c_smf[f], &bars[buf]);

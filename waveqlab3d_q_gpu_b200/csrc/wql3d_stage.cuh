@@ -44,7 +44,8 @@ struct Tuning {
   int fused_minb = 0; // k_curv_fused resident 128-thread blocks per SM: 3 (default), 2 or 4 in FP64; 4 (default), 5 or 6 in FP32
   int mvpf = -1;      // k_curv_fused: L2 prefetch of the memory variables on entry (-1: FP32 only)
   int overlap = 1;    // Cartesian stage: shell on the side stream, concurrent with the interior
-  int tma = 0;        // Cartesian interior: 1 = planes filled by TMA box loads (default: cp.async, measured faster)
+  int tma = 0;        // Cartesian interior: 1 = planes filled by TMA box loads (default: cp.async, measured faster);
+                      // 2 = TMA waits with no copies issued (test of the bounded waits and the stall status)
 };
 
 inline Tuning tuning() {

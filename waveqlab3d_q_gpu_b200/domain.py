@@ -253,7 +253,8 @@ class Domain:
 
     def check_status(self) -> int:
         """Waits for the queued work; raises Wql3dError (ENONFINITE) when a station
-        sample so far was not finite (src/seismogram.f90:516-524)."""
+        sample so far was not finite (src/seismogram.f90:516-524), or (ECUDA)
+        when a bounded device wait of a stage kernel gave up."""
         bad = C.c_int32()
         _lib.check(_lib.load().wql3d_check_status(self.handle, C.byref(bad)), "wql3d_check_status")
         return bad.value
