@@ -20,12 +20,17 @@ __global__ void __launch_bounds__(128, 3) k_adj_pre(Blk<double> b, AdjBlk A, dou
   if (!flat_point(b, x, y, z)) return;
   const long long p = pidx(b, x, y, z);
   const long long V = b.vol;
+  // R is kept in memory only where a later pass of the stage reads it: the
+  // face points (k_adj_face) and the sources' support box (k_adj_moment)
+  const bool keepR = x == 1 || x == b.nx || y == 1 || y == b.ny || z == 1 || z == b.nz ||
+                     (x >= b.sbox[0] && x <= b.sbox[1] && y >= b.sbox[2] && y <= b.sbox[3] && z >= b.sbox[4] &&
+                      z <= b.sbox[5]);
   double R[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) {
     const double r = A.DFb[c * V + p] + Bdt * A.Fb[c * V + p];
     R[c] = r;
-    A.R[c * V + p] = r;
+    if (keepR) A.R[c * V + p] = r;
     A.DFb[c * V + p] = As * r;
   }
   const double lam = b.M[p], mu = b.M[V + p], rho = b.M[2 * V + p];
