@@ -2,7 +2,8 @@
 slip-weakening interface, von Karman medium, overstressed nucleation
 patch) at reduced size on the CUDA path against the CPU oracle: both blocks'
 fields, the memory variables and the fault outputs after 8 steps of
-rupture (1e-11), and the FP32 path within 1e-3 of FP64."""
+rupture (1e-11), and the FP32 path within 1e-6 of FP64 (measured 4.8e-8
+on the fields, 3.7e-8 on the slip)."""
 import numpy as np
 import pytest
 
@@ -41,5 +42,5 @@ def test_planar_fault_fp32(wql3d_lib):
     a.run(8)
     b.run(8)
     for k in (0, 1):
-        assert rel_l2(b.fields(k), a.fields(k)) < 1e-3
-    assert rel_l2(b.fault("S"), a.fault("S")) < 1e-3
+        assert rel_l2(b.fields(k), a.fields(k)) < 1e-6
+    assert rel_l2(b.fault("S"), a.fault("S")) < 1e-6

@@ -86,8 +86,9 @@ def test_rate_state_curvilinear_q8_pml(wql3d_lib, oracle_lib):
 
 
 def test_fp32_rate_state_tracks_fp64(wql3d_lib):
-    """The FP32 path through the nucleation (60 steps): fields and slip rate
-    within 1e-3 of FP64 (the law and the slip run in FP64 on both paths)."""
+    """The FP32 path through the nucleation (60 steps): fields within 1e-6 and
+    the slip rate within 1e-8 of FP64 (measured 4.1e-8 and 5.1e-10; the law and
+    the slip run in FP64 on both paths)."""
     from waveqlab3d_q_gpu_b200.domain import Domain
     p = tpv101_case(t_final=1.0)
     a = Domain(p, nsteps_hint=60)
@@ -95,9 +96,9 @@ def test_fp32_rate_state_tracks_fp64(wql3d_lib):
     a.run(60)
     b.run(60)
     for k in (0, 1):
-        assert rel_l2(b.fields(k), a.fields(k)) < 1e-3, (k, rel_l2(b.fields(k), a.fields(k)))
-    assert rel_l2(b.fault("Svel"), a.fault("Svel")) < 1e-3, rel_l2(b.fault("Svel"), a.fault("Svel"))
-    assert rel_l2(b.fault("state"), a.fault("state")) < 1e-6
+        assert rel_l2(b.fields(k), a.fields(k)) < 1e-6, (k, rel_l2(b.fields(k), a.fields(k)))
+    assert rel_l2(b.fault("Svel"), a.fault("Svel")) < 1e-8, rel_l2(b.fault("Svel"), a.fault("Svel"))
+    assert rel_l2(b.fault("state"), a.fault("state")) < 1e-12
 
 
 def test_tpv101_nucleation_matches_oracle(wql3d_lib, oracle_lib):

@@ -62,6 +62,6 @@ def test_fp32_batch_tracks_fp64(wql3d_lib):
     b32.run(40)
     for s64, s32 in zip(b64.seismograms(), b32.seismograms()):
         assert np.abs(s64[:, :, 1:]).max() > 0
-        assert rel_l2(s32[:, :, 1:], s64[:, :, 1:]) < 1e-4
+        assert rel_l2(s32[:, :, 1:], s64[:, :, 1:]) < 1e-5   # measured 3.9e-7 .. 6.4e-7
     b64.close()
     b32.close()
