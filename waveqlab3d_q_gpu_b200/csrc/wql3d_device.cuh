@@ -189,8 +189,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // ---------------------------------------------------------------------------
 // Tensor-memory-accelerator (TMA) tile loads, cp.async.bulk.tensor, completing
-// on an mbarrier in shared memory.  No cluster multicast: every tensor map
-// covers this GPU's own field arrays.  Rules the callers keep: the innermost
+// on an mbarrier in shared memory.  Each copy lands in the issuing CTA's own
+// shared memory only, and every tensor map covers this GPU's own field
+// arrays.  Rules the callers keep: the innermost
 // coordinate times the element size is a multiple of 16 bytes, the shared
 // destination is 128-byte aligned, and every wait is bounded.
 // ---------------------------------------------------------------------------
